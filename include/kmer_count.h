@@ -1,0 +1,154 @@
+/* kmer_count.h -- C ABI of the B200 exact canonical k-mer counter
+ * (libkmertree_b200.so).
+ *
+ * Drop-in for the counting path of ScorchShana/KmerTreeCounter (tree_v4):
+ * FASTQ bytes -> exact (canonical k-mer, count) records written in the
+ * reference's own file formats, so tool/ExportReader.h,
+ * tool/FinalDrainReader.h, tool/histogram_tool.cpp and tool/PostProcess.h
+ * read the output unchanged:
+ *
+ *   <out_dir>/low.bin        headerless packed keys, one per first occurrence
+ *                            (src/ExportWriter.h:339-342, :522-550)
+ *   <out_dir>/root_{id}.bin  headerless ExportRecord<N> = {u64 key[N]; u32
+ *                            count; u32 pad=0}, id = key word 0 >> 56, one
+ *                            file per id 0..255, created even when empty
+ *                            (src/definition.h:159-163,
+ *                            src/FinalDrainWriter.h:31-90)
+ *
+ * Exact count of a key = its root record count + [key in low.bin], the
+ * merged view tool/histogram_tool.cpp "precise" computes.
+ *
+ * All plain C types.  The library owns its device and pinned memory; caller
+ * strings and buffers are borrowed for the duration of a call.  Every call is
+ * synchronous at the API level and runs on one CUDA stream per context.  The
+ * library never calls exit(); errors are negative return codes with a
+ * message from kc_last_error() (thread-local).
+ */
+#ifndef KMER_COUNT_H
+#define KMER_COUNT_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+#define KC_OK 0
+#define KC_ERR_INVALID (-1)  /* bad argument (reference: usage error, exit 1) */
+#define KC_ERR_IO (-2)       /* open/read/write failure (reference: exit(-1)) */
+#define KC_ERR_OVERFLOW (-3) /* count table could not be grown to fit */
+#define KC_ERR_DEVICE (-4)   /* CUDA error, extension missing, no device */
+#define KC_ERR_NOMEM (-5)    /* device or pinned allocation failed */
+#define KC_ERR_STATE (-6)    /* call order: no result available yet */
+
+/* ---- sizing modes -------------------------------------------------------- */
+#define KC_SIZING_SAMPLED 0 /* per-bucket loads from the routing histogram and a
+                               fixed repeat ratio; rehash on overflow */
+#define KC_SIZING_LEARNED 1 /* per-bucket loads from a sizing model; the sampled
+                               rule is the fallback on overflow */
+
+/* Counting configuration.  Replaces the positional arguments of
+ * `Tree <fastq> <k> <n_thread> <mem_gb> [map_capacity] [min] [max]`
+ * (src/main.cpp:314-374); n_thread, mem_gb and map_capacity have no meaning on
+ * the device and are accepted and ignored by the CLI. */
+typedef struct kc_config {
+    uint32_t k;            /* 1..64; key words N = 1 for k<=32, 2 for k<=64 */
+    uint32_t canonical;    /* must be 1: the reference always counts canonical */
+    uint32_t min_count;    /* root-record filter, inclusive (src/NewKmerTree.h:1159-1168) */
+    uint32_t max_count;
+    uint32_t n_buckets;    /* internal partitions: 256 or 4096 */
+    uint32_t sizing;       /* KC_SIZING_* */
+    int32_t device;        /* CUDA device ordinal */
+    uint32_t sort_output;  /* 1: root records sorted by key inside each root file */
+    uint64_t chunk_bytes;  /* host->device streaming chunk (default 256 MiB) */
+    uint64_t batch_bytes;  /* FASTQ bytes counted per device pass (default 4 GiB) */
+    double bloom_bits;     /* first-occurrence filter bits per k-mer occurrence */
+    double table_load;     /* target load factor of the repeat tables */
+    double repeat_ratio;   /* sampled sizing: distinct repeat keys per k-mer */
+} kc_config;
+
+/* Counters of one run.  total_kmers and root_records match the reference's
+ * "Total read k-mer count" and "High frequency unique k-mer" lines
+ * (src/main.cpp:266, :309). */
+typedef struct kc_stats {
+    uint64_t input_bytes;
+    uint64_t total_kmers;     /* K: valid windows */
+    uint64_t low_records;     /* L: keys written to low.bin */
+    uint64_t root_records;    /* R: records written to root files (after filter) */
+    uint64_t table_keys;      /* distinct keys held by the repeat tables */
+    uint64_t rehashes;        /* table growth steps taken after an overflow */
+    uint64_t batches;         /* device passes */
+    uint64_t root_counts[256];/* records per root file */
+    double device_ms;         /* time spent in kernels and copies on the stream */
+    double wall_ms;
+} kc_stats;
+
+typedef struct kc_context kc_context;
+
+/* Defaults: k=31, canonical=1, min=1, max=UINT32_MAX, 256 buckets, sampled
+ * sizing, device 0, unsorted roots, 256 MiB chunks, 4 GiB batches. */
+void kc_config_default(kc_config* cfg);
+
+/* Thread-local message for the last failing call on this thread. */
+const char* kc_last_error(void);
+
+/* Bytes of one packed low.bin record for k (src/ExportWriter.h:339-342). */
+uint64_t kc_packed_bytes(uint32_t k);
+
+/* sizeof(ExportRecord<N>) for k: 16, 24 (src/definition.h:159-163). */
+uint64_t kc_record_bytes(uint32_t k);
+
+/* ---- one-shot file API --------------------------------------------------- */
+
+/* Count the FASTQ (plain or gzip, detected by magic bytes as
+ * src/FastqReader.h:93-104 does) at fastq_path and write low.bin and
+ * root_0..255.bin into out_dir (created if missing).
+ * Replaces process_main<N> (src/main.cpp:111-312). */
+int kc_count_fastq(const kc_config* cfg, const char* fastq_path, const char* out_dir, kc_stats* stats);
+
+/* ---- context API ------------------------------------------------------- */
+
+int kc_create(const kc_config* cfg, kc_context** out);
+void kc_destroy(kc_context* ctx);
+
+/* Count a FASTQ byte stream held in host memory (pinned or pageable); the
+ * bytes are streamed to the device in chunk_bytes pieces.  Results stay on
+ * the device until copied out or written. */
+int kc_count_host(kc_context* ctx, const uint8_t* fastq, uint64_t n, kc_stats* stats);
+
+/* Same, with the FASTQ already in device memory (a device pointer). */
+int kc_count_device(kc_context* ctx, const uint8_t* d_fastq, uint64_t n, kc_stats* stats);
+
+/* Sizes of the last result: packed low.bin bytes, number of root records,
+ * and per-root record counts (256 entries, may be NULL). */
+int kc_result_sizes(kc_context* ctx, uint64_t* low_bytes, uint64_t* n_root_records, uint64_t* root_counts);
+
+/* Copy the packed low.bin bytes into dst (cap bytes). */
+int kc_copy_low(kc_context* ctx, uint8_t* dst, uint64_t cap);
+
+/* Copy all root records (ExportRecord<N>, grouped by root id 0..255 in
+ * order) into dst (cap bytes). */
+int kc_copy_roots(kc_context* ctx, uint8_t* dst, uint64_t cap);
+
+/* Write low.bin and root_0..255.bin of the last result into out_dir. */
+int kc_write_outputs(kc_context* ctx, const char* out_dir);
+
+/* Device pointers to the last result (valid until the next count or
+ * kc_destroy): packed low bytes and the grouped root-record array. */
+int kc_device_results(kc_context* ctx, const void** d_low, uint64_t* low_bytes, const void** d_roots,
+                      uint64_t* n_roots);
+
+/* Page-locked host memory for callers that stream input (cudaHostAlloc). */
+void* kc_host_alloc(uint64_t bytes);
+void kc_host_free(void* p);
+
+/* CUDA stream of the context (as void*), for callers that time it. */
+void* kc_stream(kc_context* ctx);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* KMER_COUNT_H */

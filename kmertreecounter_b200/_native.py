@@ -1,0 +1,227 @@
+"""ctypes binding of libkmertree_b200.so (C ABI in include/kmer_count.h).
+
+The shared library is the product; this module only marshals arguments.  It
+raises on import when the library is missing -- there is no CPU fallback.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libkmertree_b200.so")
+SYNTH_PATH = os.path.join(HERE, "libkc_synth.so")
+
+KC_OK = 0
+KC_ERR_INVALID = -1
+KC_ERR_IO = -2
+KC_ERR_OVERFLOW = -3
+KC_ERR_DEVICE = -4
+KC_ERR_NOMEM = -5
+KC_ERR_STATE = -6
+
+KC_SIZING_SAMPLED = 0
+KC_SIZING_LEARNED = 1
+
+# Every extern "C" symbol include/kmer_count.h declares.
+ABI_SYMBOLS = (
+    "kc_config_default", "kc_last_error", "kc_packed_bytes", "kc_record_bytes", "kc_count_fastq",
+    "kc_create", "kc_destroy", "kc_count_host", "kc_count_device", "kc_result_sizes", "kc_copy_low",
+    "kc_copy_roots", "kc_write_outputs", "kc_device_results", "kc_host_alloc", "kc_host_free", "kc_stream",
+)
+
+
+class KcConfig(C.Structure):
+    _fields_ = [
+        ("k", C.c_uint32), ("canonical", C.c_uint32), ("min_count", C.c_uint32), ("max_count", C.c_uint32),
+        ("n_buckets", C.c_uint32), ("sizing", C.c_uint32), ("device", C.c_int32), ("sort_output", C.c_uint32),
+        ("chunk_bytes", C.c_uint64), ("batch_bytes", C.c_uint64), ("bloom_bits", C.c_double),
+        ("table_load", C.c_double), ("repeat_ratio", C.c_double),
+    ]
+
+
+class KcStats(C.Structure):
+    _fields_ = [
+        ("input_bytes", C.c_uint64), ("total_kmers", C.c_uint64), ("low_records", C.c_uint64),
+        ("root_records", C.c_uint64), ("table_keys", C.c_uint64), ("rehashes", C.c_uint64),
+        ("batches", C.c_uint64), ("root_counts", C.c_uint64 * 256), ("device_ms", C.c_double),
+        ("wall_ms", C.c_double),
+    ]
+
+    def as_dict(self):
+        d = {f: getattr(self, f) for f, _ in self._fields_ if f != "root_counts"}
+        d["root_counts"] = list(self.root_counts)
+        return d
+
+
+class KcError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"kc error {code}: {msg}")
+        self.code = code
+
+
+def _load():
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"{LIB_PATH} is missing: run `python -m kmertreecounter_b200.build` "
+                          "(the CUDA extension is required; there is no CPU fallback)")
+    lib = C.CDLL(LIB_PATH)
+    vp, u64, u32, i32 = C.c_void_p, C.c_uint64, C.c_uint32, C.c_int
+    cfgp, stp = C.POINTER(KcConfig), C.POINTER(KcStats)
+    sig = {
+        "kc_config_default": (None, [cfgp]),
+        "kc_last_error": (C.c_char_p, []),
+        "kc_packed_bytes": (u64, [u32]),
+        "kc_record_bytes": (u64, [u32]),
+        "kc_count_fastq": (i32, [cfgp, C.c_char_p, C.c_char_p, stp]),
+        "kc_create": (i32, [cfgp, C.POINTER(vp)]),
+        "kc_destroy": (None, [vp]),
+        "kc_count_host": (i32, [vp, vp, u64, stp]),
+        "kc_count_device": (i32, [vp, vp, u64, stp]),
+        "kc_result_sizes": (i32, [vp, C.POINTER(u64), C.POINTER(u64), C.POINTER(u64)]),
+        "kc_copy_low": (i32, [vp, vp, u64]),
+        "kc_copy_roots": (i32, [vp, vp, u64]),
+        "kc_write_outputs": (i32, [vp, C.c_char_p]),
+        "kc_device_results": (i32, [vp, C.POINTER(vp), C.POINTER(u64), C.POINTER(vp), C.POINTER(u64)]),
+        "kc_host_alloc": (vp, [u64]),
+        "kc_host_free": (None, [vp]),
+        "kc_stream": (vp, [vp]),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    return lib
+
+
+lib = _load()
+
+
+def last_error():
+    m = lib.kc_last_error()
+    return m.decode() if m else ""
+
+
+def check(rc):
+    if rc != KC_OK:
+        raise KcError(rc, last_error())
+    return rc
+
+
+def default_config(**kw):
+    cfg = KcConfig()
+    lib.kc_config_default(C.byref(cfg))
+    for k, v in kw.items():
+        if not hasattr(cfg, k):
+            raise AttributeError(f"kc_config has no field {k}")
+        setattr(cfg, k, v)
+    return cfg
+
+
+def packed_bytes(k):
+    return int(lib.kc_packed_bytes(k))
+
+
+def record_bytes(k):
+    return int(lib.kc_record_bytes(k))
+
+
+def record_dtype(k):
+    """numpy dtype of ExportRecord<N> (src/definition.h:159-163)."""
+    nw = 1 if k <= 32 else (2 if k <= 64 else 4)
+    return np.dtype([("key", "<u8", (nw,)), ("count", "<u4"), ("pad", "<u4")])
+
+
+class Counter:
+    """One counting context (a CUDA stream and its device buffers)."""
+
+    def __init__(self, cfg=None, **kw):
+        self.cfg = cfg if cfg is not None else default_config(**kw)
+        self._ctx = C.c_void_p()
+        check(lib.kc_create(C.byref(self.cfg), C.byref(self._ctx)))
+        self.stats = KcStats()
+
+    def close(self):
+        if self._ctx:
+            lib.kc_destroy(self._ctx)
+            self._ctx = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    @property
+    def stream(self):
+        return lib.kc_stream(self._ctx)
+
+    def count_host(self, data):
+        """Count FASTQ bytes in host memory (bytes, bytearray or uint8 ndarray)."""
+        if isinstance(data, (bytes, bytearray)):
+            buf = np.frombuffer(data, dtype=np.uint8)
+        else:
+            buf = np.ascontiguousarray(data, dtype=np.uint8)
+        ptr = buf.ctypes.data if buf.size else None
+        check(lib.kc_count_host(self._ctx, ptr, buf.size, C.byref(self.stats)))
+        return self.stats
+
+    def count_host_ptr(self, ptr, n):
+        check(lib.kc_count_host(self._ctx, C.c_void_p(ptr), n, C.byref(self.stats)))
+        return self.stats
+
+    def count_device(self, dptr, n):
+        """Count FASTQ bytes already in device memory (an integer device pointer)."""
+        check(lib.kc_count_device(self._ctx, C.c_void_p(dptr), n, C.byref(self.stats)))
+        return self.stats
+
+    def sizes(self):
+        lb, nr = C.c_uint64(), C.c_uint64()
+        rc = (C.c_uint64 * 256)()
+        check(lib.kc_result_sizes(self._ctx, C.byref(lb), C.byref(nr), rc))
+        return lb.value, nr.value, list(rc)
+
+    def low_bytes(self):
+        lb, _, _ = self.sizes()
+        out = np.empty(lb, dtype=np.uint8)
+        check(lib.kc_copy_low(self._ctx, out.ctypes.data if lb else None, lb))
+        return out
+
+    def root_records(self):
+        _, nr, counts = self.sizes()
+        dt = record_dtype(self.cfg.k)
+        out = np.empty(nr, dtype=dt)
+        check(lib.kc_copy_roots(self._ctx, out.ctypes.data if nr else None, nr * dt.itemsize))
+        return out, counts
+
+    def write_outputs(self, out_dir):
+        check(lib.kc_write_outputs(self._ctx, str(out_dir).encode()))
+
+    def device_results(self):
+        dl, lb, dr, nr = C.c_void_p(), C.c_uint64(), C.c_void_p(), C.c_uint64()
+        check(lib.kc_device_results(self._ctx, C.byref(dl), C.byref(lb), C.byref(dr), C.byref(nr)))
+        return dl.value, lb.value, dr.value, nr.value
+
+
+def count_fastq(path, out_dir, **kw):
+    """File API: count `path`, write low.bin + root_{0..255}.bin into out_dir."""
+    cfg = default_config(**kw)
+    st = KcStats()
+    check(lib.kc_count_fastq(C.byref(cfg), str(path).encode(), str(out_dir).encode(), C.byref(st)))
+    return st
+
+
+def host_alloc(nbytes):
+    p = lib.kc_host_alloc(nbytes)
+    if not p:
+        raise KcError(KC_ERR_NOMEM, last_error())
+    return p
+
+
+def host_free(p):
+    lib.kc_host_free(p)

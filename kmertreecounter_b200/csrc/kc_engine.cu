@@ -1,0 +1,716 @@
+// Host engine and C ABI of the B200 exact canonical k-mer counter.
+//
+// One kc_context = one CUDA stream + the device buffers of the pipeline.  A
+// count runs batch by batch over the FASTQ bytes (one batch = up to
+// batch_bytes, resident in HBM), then exports the repeat tables:
+//
+//   per batch   lines_per_tile -> scan -> extract<HIST> -> [size tables on the
+//               first batch] -> extract<SCATTER> -> count_routed -> [rehash
+//               overflowed buckets + retry] -> scan -> pack_low
+//   at the end  export_count -> export_write (ExportRecord<N> grouped by root)
+//
+// This replaces the reference's reader/parser/classifier/tree thread pipeline
+// (src/main.cpp:111-312) as a whole; see the kernel header for the per-kernel
+// correspondence.
+
+#include <algorithm>
+#include <bit>
+#include <chrono>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "../../include/kmer_count.h"
+#include "kc_internal.h"
+#include "kc_kernels.cuh"
+#include "kc_scan.cuh"
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const char* fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    g_err = buf;
+    return code;
+}
+
+#define CK(x)                                                                                         \
+    do {                                                                                              \
+        cudaError_t e_ = (x);                                                                         \
+        if (e_ != cudaSuccess) return fail(KC_ERR_DEVICE, "%s failed: %s (%s:%d)", #x, cudaGetErrorString(e_), \
+                                           __FILE__, __LINE__);                                       \
+    } while (0)
+
+struct DevBuf {
+    void* p = nullptr;
+    size_t cap = 0;
+    // Grow to at least `bytes` (contents not kept).
+    cudaError_t ensure(size_t bytes) {
+        if (bytes <= cap && p) return cudaSuccess;
+        if (p) cudaFree(p);
+        p = nullptr;
+        cap = 0;
+        size_t want = std::max<size_t>(bytes + bytes / 8, 4096);
+        cudaError_t e = cudaMalloc(&p, want);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            e = cudaMalloc(&p, bytes);
+            want = bytes;
+        }
+        if (e == cudaSuccess) cap = want;
+        else p = nullptr;
+        return e;
+    }
+    // Grow keeping the first `keep` bytes.
+    cudaError_t grow_keep(size_t bytes, size_t keep, cudaStream_t st) {
+        if (bytes <= cap && p) return cudaSuccess;
+        void* q = nullptr;
+        size_t want = std::max<size_t>(bytes + bytes / 4, 4096);
+        cudaError_t e = cudaMalloc(&q, want);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            want = bytes;
+            e = cudaMalloc(&q, want);
+            if (e != cudaSuccess) return e;
+        }
+        if (p && keep) {
+            e = cudaMemcpyAsync(q, p, keep, cudaMemcpyDeviceToDevice, st);
+            if (e != cudaSuccess) return e;
+            e = cudaStreamSynchronize(st);
+            if (e != cudaSuccess) return e;
+        }
+        if (p) cudaFree(p);
+        p = q;
+        cap = want;
+        return cudaSuccess;
+    }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        cap = 0;
+    }
+    template <class T>
+    T* as() const {
+        return reinterpret_cast<T*>(p);
+    }
+};
+
+inline uint64_t ceil_div(uint64_t a, uint64_t b) { return (a + b - 1) / b; }
+inline uint64_t pow2_at_least(uint64_t x) { return std::bit_ceil(std::max<uint64_t>(x, 1)); }
+
+}  // namespace
+
+struct kc_context {
+    kc_config cfg{};
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    uint32_t nw = 1, bucket_bits = 8, n_buckets = 256, bucket_shift = 56;
+    uint64_t slot_bytes = 16, record_bytes = 16, packed_bytes = 8;
+
+    // batch pipeline
+    DevBuf stage;        // [HALO | batch | pad] for host input
+    DevBuf tile_nl, tile_line;
+    DevBuf bucket_count, bucket_cursor;
+    DevBuf routed;
+    DevBuf tile_low, tile_fail, tile_low_prefix;
+    DevBuf scan_sums, scalars;
+    DevBuf overflow, meta;
+    DevBuf bloom, table;
+    DevBuf low_packed;
+    DevBuf roots, chunks, root_count, root_cursor;
+
+    // host mirrors
+    std::vector<kc::BucketMeta> h_meta;
+    std::vector<uint64_t> h_bucket_count;
+    std::vector<uint32_t> h_overflow;
+    uint64_t bloom_words = 0, table_slots_used = 0;
+    bool sized = false;
+    uint64_t expected_total_bytes = 0;
+
+    // run state
+    uint64_t line_base = 0;
+    uint64_t low_total = 0;
+    uint64_t K = 0;
+    uint64_t rehashes = 0, batches = 0, input_bytes = 0;
+    bool have_result = false;
+    uint64_t root_total = 0, table_keys = 0;
+    uint64_t root_counts[256] = {};
+
+    // optional learned sizing hook (per-bucket repeat-key predictions)
+    std::vector<double> predicted_repeat_keys;
+};
+
+namespace {
+
+int setup_shape(kc_context* c) {
+    const kc_config& g = c->cfg;
+    if (g.k < 1 || g.k > 64) return fail(KC_ERR_INVALID, "k=%u out of range: this build supports 1..64", g.k);
+    if (g.canonical != 1) return fail(KC_ERR_INVALID, "only canonical counting is supported (the reference has no other mode)");
+    if (g.max_count < g.min_count) return fail(KC_ERR_INVALID, "max_count < min_count");
+    if (g.n_buckets != 256 && g.n_buckets != 4096) return fail(KC_ERR_INVALID, "n_buckets must be 256 or 4096");
+    if (g.bloom_bits <= 0.0 || g.table_load <= 0.05 || g.table_load > 0.95 || g.repeat_ratio <= 0.0)
+        return fail(KC_ERR_INVALID, "bloom_bits, table_load (0.05..0.95) and repeat_ratio must be positive");
+    if (g.batch_bytes < (1ull << 20)) return fail(KC_ERR_INVALID, "batch_bytes must be at least 1 MiB");
+    c->nw = g.k <= 32 ? 1 : 2;
+    c->n_buckets = g.n_buckets;
+    c->bucket_bits = g.n_buckets == 256 ? 8 : 12;
+    c->bucket_shift = 64 - c->bucket_bits;
+    c->slot_bytes = c->nw == 1 ? sizeof(kc::Slot1) : sizeof(kc::Slot2);
+    c->record_bytes = kc_record_bytes(g.k);
+    c->packed_bytes = kc_packed_bytes(g.k);
+    return KC_OK;
+}
+
+// Exclusive scan of n values of type TI into TO out[], plus base; optional
+// device total in scalars[slot].
+template <class TI, class TO>
+int device_scan(kc_context* c, const TI* in, uint64_t n, TO* out, uint64_t base, uint64_t* d_total) {
+    const uint64_t nb = std::max<uint64_t>(1, ceil_div(n, kc::SCAN_TILE));
+    CK(c->scan_sums.ensure(nb * sizeof(uint64_t)));
+    uint64_t* sums = c->scan_sums.as<uint64_t>();
+    if (n) kc::scan_reduce<TI><<<nb, kc::SCAN_BLOCK, 0, c->stream>>>(in, n, sums);
+    else CK(cudaMemsetAsync(sums, 0, sizeof(uint64_t), c->stream));
+    kc::scan_sums<<<1, kc::SCAN_BLOCK, 0, c->stream>>>(sums, n ? nb : 1, base, d_total);
+    if (n) kc::scan_apply<TI, TO><<<nb, kc::SCAN_BLOCK, 0, c->stream>>>(in, n, sums, out);
+    CK(cudaGetLastError());
+    return KC_OK;
+}
+
+// Allocate filter and tables from per-bucket k-mer totals of the first batch.
+int size_structures(kc_context* c, const std::vector<uint64_t>& kb, double scale) {
+    const kc_config& g = c->cfg;
+    const uint32_t nb = c->n_buckets;
+    c->h_meta.assign(nb, kc::BucketMeta{});
+    uint64_t bw = 0, ts = 0;
+    const bool learned = g.sizing == KC_SIZING_LEARNED && c->predicted_repeat_keys.size() == nb;
+    for (uint32_t b = 0; b < nb; ++b) {
+        const double kest = (double)kb[b] * scale;
+        const uint64_t words = pow2_at_least(std::max<uint64_t>((uint64_t)(kest * g.bloom_bits / 64.0), 256));
+        double rep = learned ? c->predicted_repeat_keys[b] : kest * g.repeat_ratio;
+        const uint64_t slots = pow2_at_least(std::max<uint64_t>((uint64_t)(rep / g.table_load), 256));
+        c->h_meta[b].bloom_off = bw;
+        c->h_meta[b].bloom_mask = words - 1;
+        c->h_meta[b].tab_off = ts;
+        c->h_meta[b].tab_mask = slots - 1;
+        bw += words;
+        ts += slots;
+    }
+    c->bloom_words = bw;
+    c->table_slots_used = ts;
+    CK(c->bloom.ensure(bw * sizeof(uint64_t)));
+    CK(c->table.ensure(ts * c->slot_bytes + ts * c->slot_bytes / 2));
+    CK(c->meta.ensure(nb * sizeof(kc::BucketMeta)));
+    CK(cudaMemcpyAsync(c->meta.p, c->h_meta.data(), nb * sizeof(kc::BucketMeta), cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemsetAsync(c->bloom.p, 0, bw * sizeof(uint64_t), c->stream));
+    const int ig = 148 * 8;
+    if (c->nw == 1) kc::init_slots<1><<<ig, 256, 0, c->stream>>>(c->table.p, ts);
+    else kc::init_slots<2><<<ig, 256, 0, c->stream>>>(c->table.p, ts);
+    CK(cudaGetLastError());
+    CK(c->overflow.ensure(nb * sizeof(uint32_t)));
+    CK(cudaMemsetAsync(c->overflow.p, 0, nb * sizeof(uint32_t), c->stream));
+    c->h_overflow.assign(nb, 0);
+    c->sized = true;
+    return KC_OK;
+}
+
+template <int NW>
+void launch_count(kc_context* c, uint64_t n_keys, int use_filter) {
+    constexpr int TILE = kc::count_tile<NW>();
+    const uint64_t tiles = ceil_div(n_keys, TILE);
+    if (!tiles) return;
+    kc::CountArgs a;
+    a.routed = c->routed.p;
+    a.n_keys = n_keys;
+    a.meta = c->meta.as<kc::BucketMeta>();
+    a.bloom = c->bloom.as<uint64_t>();
+    a.table = c->table.p;
+    a.tile_low = c->tile_low.as<uint32_t>();
+    a.tile_fail = c->tile_fail.as<uint32_t>();
+    a.bucket_overflow = c->overflow.as<uint32_t>();
+    a.bucket_shift = c->bucket_shift;
+    a.use_filter = use_filter;
+    kc::count_routed<NW><<<tiles, kc::CNT_THREADS, 0, c->stream>>>(a);
+}
+
+// Grow the tables of overflowed buckets (x4) and re-insert the keys that
+// met a full table, until none is left.
+template <int NW>
+int rehash_loop(kc_context* c, uint64_t n_keys) {
+    const uint32_t nb = c->n_buckets;
+    for (int round = 0;; ++round) {
+        CK(cudaMemcpyAsync(c->h_overflow.data(), c->overflow.p, nb * sizeof(uint32_t), cudaMemcpyDeviceToHost,
+                           c->stream));
+        CK(cudaStreamSynchronize(c->stream));
+        std::vector<uint32_t> grow;
+        for (uint32_t b = 0; b < nb; ++b)
+            if (c->h_overflow[b]) grow.push_back(b);
+        if (grow.empty()) return KC_OK;
+        if (round > 24) return fail(KC_ERR_OVERFLOW, "repeat tables kept overflowing after %d growth rounds", round);
+        CK(cudaMemsetAsync(c->overflow.p, 0, nb * sizeof(uint32_t), c->stream));
+        CK(c->scalars.ensure(64));
+        uint32_t* d_failed = c->scalars.as<uint32_t>() + 8;
+        for (uint32_t b : grow) {
+            uint64_t old_slots = c->h_meta[b].tab_mask + 1;
+            uint64_t new_slots = old_slots * 4;
+            for (;;) {
+                const uint64_t need = (c->table_slots_used + new_slots) * c->slot_bytes;
+                CK(c->table.grow_keep(need, c->table_slots_used * c->slot_bytes, c->stream));
+                const uint64_t off = c->table_slots_used;
+                void* nt = c->table.as<uint8_t>() + off * c->slot_bytes;
+                const void* ot = c->table.as<uint8_t>() + c->h_meta[b].tab_off * c->slot_bytes;
+                kc::init_slots<NW><<<256, 256, 0, c->stream>>>(nt, new_slots);
+                CK(cudaMemsetAsync(d_failed, 0, sizeof(uint32_t), c->stream));
+                kc::rehash_bucket<NW><<<std::max<uint64_t>(1, std::min<uint64_t>(1184, ceil_div(old_slots, 256))), 256, 0,
+                                        c->stream>>>(ot, old_slots, nt, new_slots - 1, d_failed);
+                CK(cudaGetLastError());
+                uint32_t h_failed = 0;
+                CK(cudaMemcpyAsync(&h_failed, d_failed, sizeof(uint32_t), cudaMemcpyDeviceToHost, c->stream));
+                CK(cudaStreamSynchronize(c->stream));
+                c->table_slots_used += new_slots;
+                if (!h_failed) {
+                    c->h_meta[b].tab_off = off;
+                    c->h_meta[b].tab_mask = new_slots - 1;
+                    break;
+                }
+                new_slots *= 4;  // pathological clustering: grow again
+            }
+            ++c->rehashes;
+        }
+        CK(cudaMemcpyAsync(c->meta.p, c->h_meta.data(), nb * sizeof(kc::BucketMeta), cudaMemcpyHostToDevice,
+                           c->stream));
+        launch_count<NW>(c, n_keys, 0);
+        CK(cudaGetLastError());
+    }
+}
+
+template <int NW>
+int launch_extract(kc_context* c, const uint8_t* buf, uint64_t n, int has_halo, int mode) {
+    const uint64_t tiles = ceil_div(n, kc::EXT_TILE);
+    if (!tiles) return KC_OK;
+    kc::ExtractArgs a;
+    a.buf = buf;
+    a.n = n;
+    a.has_halo = has_halo;
+    a.tile_line = c->tile_line.as<uint64_t>();
+    a.k = c->cfg.k;
+    a.bucket_shift = c->bucket_shift;
+    a.n_buckets = c->n_buckets;
+    a.bucket_count = c->bucket_count.as<unsigned long long>();
+    a.bucket_cursor = c->bucket_cursor.as<unsigned long long>();
+    a.routed = c->routed.p;
+    const size_t smem = (size_t)c->n_buckets * 16;
+    if (mode == kc::HIST) kc::extract_kernel<NW, kc::HIST><<<tiles, kc::EXT_THREADS, smem, c->stream>>>(a);
+    else kc::extract_kernel<NW, kc::SCATTER><<<tiles, kc::EXT_THREADS, smem, c->stream>>>(a);
+    CK(cudaGetLastError());
+    return KC_OK;
+}
+
+// Count one batch of FASTQ bytes already in device memory.
+template <int NW>
+int process_batch(kc_context* c, const uint8_t* buf, uint64_t n, int has_halo) {
+    if (reinterpret_cast<uintptr_t>(buf) % 16)
+        return fail(KC_ERR_INVALID, "device FASTQ batch must be 16-byte aligned");
+    const uint32_t nb = c->n_buckets;
+    const uint64_t tiles = ceil_div(n, kc::EXT_TILE);
+    CK(c->tile_nl.ensure(std::max<uint64_t>(tiles, 1) * sizeof(uint32_t)));
+    CK(c->tile_line.ensure(std::max<uint64_t>(tiles, 1) * sizeof(uint64_t)));
+    CK(c->scalars.ensure(64));
+    uint64_t* d_scal = c->scalars.as<uint64_t>();
+    if (tiles) kc::lines_per_tile<<<tiles, kc::EXT_THREADS, 0, c->stream>>>(buf, n, c->tile_nl.as<uint32_t>());
+    CK(cudaGetLastError());
+    int rc = device_scan<uint32_t, uint64_t>(c, c->tile_nl.as<uint32_t>(), tiles, c->tile_line.as<uint64_t>(),
+                                             c->line_base, d_scal + 0);
+    if (rc) return rc;
+
+    CK(c->bucket_count.ensure(nb * sizeof(uint64_t)));
+    CK(c->bucket_cursor.ensure(nb * sizeof(uint64_t)));
+    CK(cudaMemsetAsync(c->bucket_count.p, 0, nb * sizeof(uint64_t), c->stream));
+    if ((rc = launch_extract<NW>(c, buf, n, has_halo, kc::HIST))) return rc;
+
+    c->h_bucket_count.resize(nb);
+    uint64_t line_end = 0;
+    CK(cudaMemcpyAsync(c->h_bucket_count.data(), c->bucket_count.p, nb * sizeof(uint64_t), cudaMemcpyDeviceToHost,
+                       c->stream));
+    CK(cudaMemcpyAsync(&line_end, d_scal + 0, sizeof(uint64_t), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    c->line_base = line_end;
+
+    uint64_t kb = 0;
+    std::vector<uint64_t> start(nb);
+    for (uint32_t b = 0; b < nb; ++b) {
+        start[b] = kb;
+        kb += c->h_bucket_count[b];
+    }
+    c->K += kb;
+    if (!c->sized) {
+        double scale = 1.0;
+        if (c->expected_total_bytes > n && n > 0) scale = (double)c->expected_total_bytes / (double)n;
+        if ((rc = size_structures(c, c->h_bucket_count, scale))) return rc;
+    }
+    if (!kb) return KC_OK;
+
+    constexpr int CT = kc::count_tile<NW>();
+    const uint64_t ctiles = ceil_div(kb, CT);
+    CK(c->routed.ensure(ctiles * CT * (uint64_t)(8 * NW)));
+    CK(c->tile_low.ensure(ctiles * sizeof(uint32_t)));
+    CK(c->tile_fail.ensure(ctiles * sizeof(uint32_t)));
+    CK(c->tile_low_prefix.ensure(ctiles * sizeof(uint64_t)));
+    CK(cudaMemcpyAsync(c->bucket_cursor.p, start.data(), nb * sizeof(uint64_t), cudaMemcpyHostToDevice, c->stream));
+    if ((rc = launch_extract<NW>(c, buf, n, has_halo, kc::SCATTER))) return rc;
+
+    launch_count<NW>(c, kb, 1);
+    CK(cudaGetLastError());
+    if ((rc = rehash_loop<NW>(c, kb))) return rc;
+
+    // first occurrences -> packed low.bin bytes
+    if ((rc = device_scan<uint32_t, uint64_t>(c, c->tile_low.as<uint32_t>(), ctiles,
+                                              c->tile_low_prefix.as<uint64_t>(), 0, d_scal + 1)))
+        return rc;
+    uint64_t nlow = 0;
+    CK(cudaMemcpyAsync(&nlow, d_scal + 1, sizeof(uint64_t), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    CK(c->low_packed.grow_keep((c->low_total + nlow) * c->packed_bytes + 64, c->low_total * c->packed_bytes,
+                               c->stream));
+    kc::pack_low<NW><<<std::min<uint64_t>(ctiles, 148 * 16), 256, 0, c->stream>>>(
+        c->routed.p, c->tile_low.as<uint32_t>(), c->tile_low_prefix.as<uint64_t>(), ctiles, CT, c->cfg.k,
+        c->low_packed.as<uint8_t>(), c->low_total);
+    CK(cudaGetLastError());
+    c->low_total += nlow;
+    return KC_OK;
+}
+
+template <int NW>
+int export_tables(kc_context* c) {
+    const uint32_t nb = c->n_buckets;
+    std::vector<kc::ExportChunk> ch;
+    const uint32_t CH = 16384;
+    for (uint32_t b = 0; b < nb; ++b) {
+        const uint64_t slots = c->h_meta[b].tab_mask + 1;
+        for (uint64_t s = 0; s < slots; s += CH) {
+            kc::ExportChunk e;
+            e.slot_begin = c->h_meta[b].tab_off + s;
+            e.n_slots = (uint32_t)std::min<uint64_t>(CH, slots - s);
+            e.root = b >> (c->bucket_bits - 8);
+            ch.push_back(e);
+        }
+    }
+    CK(c->chunks.ensure(ch.size() * sizeof(kc::ExportChunk)));
+    CK(cudaMemcpyAsync(c->chunks.p, ch.data(), ch.size() * sizeof(kc::ExportChunk), cudaMemcpyHostToDevice,
+                       c->stream));
+    CK(c->root_count.ensure(257 * sizeof(uint64_t)));
+    CK(c->root_cursor.ensure(256 * sizeof(uint64_t)));
+    CK(cudaMemsetAsync(c->root_count.p, 0, 257 * sizeof(uint64_t), c->stream));
+    unsigned long long* rc_d = c->root_count.as<unsigned long long>();
+    const uint64_t grid = std::min<uint64_t>(ch.size(), 148 * 16);
+    kc::export_count<NW><<<grid, 256, 0, c->stream>>>(c->table.p, c->chunks.as<kc::ExportChunk>(), ch.size(),
+                                                      c->cfg.min_count, c->cfg.max_count, rc_d, rc_d + 256);
+    CK(cudaGetLastError());
+    uint64_t h[257];
+    CK(cudaMemcpyAsync(h, rc_d, sizeof h, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    uint64_t start[256], tot = 0;
+    for (int r = 0; r < 256; ++r) {
+        start[r] = tot;
+        c->root_counts[r] = h[r];
+        tot += h[r];
+    }
+    c->root_total = tot;
+    c->table_keys = h[256];
+    CK(c->roots.ensure(std::max<uint64_t>(tot, 1) * c->record_bytes));
+    CK(cudaMemcpyAsync(c->root_cursor.p, start, sizeof start, cudaMemcpyHostToDevice, c->stream));
+    kc::export_write<NW><<<grid, 256, 0, c->stream>>>(c->table.p, c->chunks.as<kc::ExportChunk>(), ch.size(),
+                                                      c->cfg.min_count, c->cfg.max_count,
+                                                      c->root_cursor.as<unsigned long long>(), c->roots.as<uint8_t>());
+    CK(cudaGetLastError());
+    // Record order inside a root file is unspecified in the reference (DFS and
+    // hash-bucket order, src/NewKmerTree.h:773-859); sorting is applied by the
+    // caller of export_tables when cfg.sort_output is set.
+    return KC_OK;
+}
+
+int begin_run(kc_context* c, uint64_t total_bytes) {
+    CK(cudaSetDevice(c->device));
+    c->line_base = 0;
+    c->low_total = 0;
+    c->K = 0;
+    c->rehashes = 0;
+    c->batches = 0;
+    c->input_bytes = 0;
+    c->sized = false;
+    c->have_result = false;
+    c->expected_total_bytes = total_bytes;
+    return KC_OK;
+}
+
+int finish_run(kc_context* c) {
+    int rc;
+    if (!c->sized) {
+        // empty input: allocate minimal structures so the export is uniform
+        std::vector<uint64_t> zero(c->n_buckets, 0);
+        if ((rc = size_structures(c, zero, 1.0))) return rc;
+    }
+    rc = c->nw == 1 ? export_tables<1>(c) : export_tables<2>(c);
+    if (rc) return rc;
+    if (c->cfg.sort_output) {
+        rc = kc_sort_roots(c->roots.p, c->root_total, c->record_bytes, c->cfg.k, c->root_counts, c->stream);
+        if (rc) return fail(rc, "root record sort failed: %s", kc_sort_error());
+    }
+    CK(cudaStreamSynchronize(c->stream));
+    c->have_result = true;
+    return KC_OK;
+}
+
+void fill_stats(kc_context* c, kc_stats* s, double dev_ms, double wall_ms) {
+    if (!s) return;
+    std::memset(s, 0, sizeof *s);
+    s->input_bytes = c->input_bytes;
+    s->total_kmers = c->K;
+    s->low_records = c->low_total;
+    s->root_records = c->root_total;
+    s->table_keys = c->table_keys;
+    s->rehashes = c->rehashes;
+    s->batches = c->batches;
+    std::memcpy(s->root_counts, c->root_counts, sizeof s->root_counts);
+    s->device_ms = dev_ms;
+    s->wall_ms = wall_ms;
+}
+
+int run_batch(kc_context* c, const uint8_t* buf, uint64_t n, int has_halo) {
+    c->batches++;
+    c->input_bytes += n;
+    return c->nw == 1 ? process_batch<1>(c, buf, n, has_halo) : process_batch<2>(c, buf, n, has_halo);
+}
+
+}  // namespace
+
+// ------------------------------------------------------------------ C ABI
+
+extern "C" {
+
+void kc_config_default(kc_config* g) {
+    if (!g) return;
+    std::memset(g, 0, sizeof *g);
+    g->k = 31;
+    g->canonical = 1;
+    g->min_count = 1;
+    g->max_count = 0xFFFFFFFFu;
+    g->n_buckets = 256;
+    g->sizing = KC_SIZING_SAMPLED;
+    g->device = 0;
+    g->sort_output = 0;
+    g->chunk_bytes = 256ull << 20;
+    g->batch_bytes = 4ull << 30;
+    g->bloom_bits = 8.0;
+    g->table_load = 0.7;
+    g->repeat_ratio = 0.125;
+}
+
+const char* kc_last_error(void) { return g_err.c_str(); }
+
+uint64_t kc_packed_bytes(uint32_t k) { return (uint64_t)(k / 32) * 8 + (2 * (k % 32) + 7) / 8; }
+
+uint64_t kc_record_bytes(uint32_t k) { return k <= 32 ? 16 : (k <= 64 ? 24 : 40); }
+
+int kc_create(const kc_config* cfg, kc_context** out) {
+    if (!cfg || !out) return fail(KC_ERR_INVALID, "null argument");
+    *out = nullptr;
+    kc_context* c = new kc_context();
+    c->cfg = *cfg;
+    int rc = setup_shape(c);
+    if (rc) {
+        delete c;
+        return rc;
+    }
+    int ndev = 0;
+    cudaError_t e = cudaGetDeviceCount(&ndev);
+    if (e != cudaSuccess || ndev == 0) {
+        delete c;
+        return fail(KC_ERR_DEVICE, "no CUDA device available (%s)", cudaGetErrorString(e));
+    }
+    if (cfg->device < 0 || cfg->device >= ndev) {
+        delete c;
+        return fail(KC_ERR_INVALID, "device %d out of range (%d devices)", cfg->device, ndev);
+    }
+    c->device = cfg->device;
+    if ((e = cudaSetDevice(c->device)) != cudaSuccess || (e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking)) != cudaSuccess ||
+        (e = cudaEventCreate(&c->ev0)) != cudaSuccess || (e = cudaEventCreate(&c->ev1)) != cudaSuccess) {
+        delete c;
+        return fail(KC_ERR_DEVICE, "stream/event creation failed: %s", cudaGetErrorString(e));
+    }
+    // 4096-bucket extraction needs 64 KiB of dynamic shared memory.
+    const int smem = 4096 * 16;
+    cudaFuncSetAttribute(kc::extract_kernel<1, kc::HIST>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    cudaFuncSetAttribute(kc::extract_kernel<1, kc::SCATTER>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    cudaFuncSetAttribute(kc::extract_kernel<2, kc::HIST>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    cudaFuncSetAttribute(kc::extract_kernel<2, kc::SCATTER>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if ((e = cudaGetLastError()) != cudaSuccess) {
+        delete c;
+        return fail(KC_ERR_DEVICE, "kernel attribute setup failed: %s", cudaGetErrorString(e));
+    }
+    *out = c;
+    return KC_OK;
+}
+
+void kc_destroy(kc_context* c) {
+    if (!c) return;
+    cudaSetDevice(c->device);
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    DevBuf* bufs[] = {&c->stage,  &c->tile_nl,   &c->tile_line, &c->bucket_count, &c->bucket_cursor, &c->routed,
+                      &c->tile_low, &c->tile_fail, &c->tile_low_prefix, &c->scan_sums, &c->scalars, &c->overflow,
+                      &c->meta,   &c->bloom,     &c->table,     &c->low_packed,   &c->roots,         &c->chunks,
+                      &c->root_count, &c->root_cursor};
+    for (DevBuf* b : bufs) b->release();
+    if (c->ev0) cudaEventDestroy(c->ev0);
+    if (c->ev1) cudaEventDestroy(c->ev1);
+    if (c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+}
+
+void* kc_stream(kc_context* c) { return c ? (void*)c->stream : nullptr; }
+
+int kc_count_device(kc_context* c, const uint8_t* d_fastq, uint64_t n, kc_stats* stats) {
+    if (!c || (!d_fastq && n)) return fail(KC_ERR_INVALID, "null argument");
+    const auto t0 = std::chrono::steady_clock::now();
+    int rc = begin_run(c, n);
+    if (rc) return rc;
+    CK(cudaEventRecord(c->ev0, c->stream));
+    const uint64_t B = c->cfg.batch_bytes & ~(uint64_t)(kc::EXT_TILE - 1);
+    for (uint64_t off = 0; off < n || (n == 0 && off == 0); off += B) {
+        if (n == 0) break;
+        const uint64_t len = std::min<uint64_t>(B, n - off);
+        if ((rc = run_batch(c, d_fastq + off, len, off > 0))) return rc;
+    }
+    if ((rc = finish_run(c))) return rc;
+    CK(cudaEventRecord(c->ev1, c->stream));
+    CK(cudaEventSynchronize(c->ev1));
+    float ms = 0;
+    cudaEventElapsedTime(&ms, c->ev0, c->ev1);
+    const double wall = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    fill_stats(c, stats, ms, wall);
+    return KC_OK;
+}
+
+// Host input: stream chunk_bytes pieces into the staging buffer
+// [HALO | batch | pad]; between batches the last HALO bytes move to the
+// front so windows that straddle the split are seen once, as the reference
+// reader's k-1 overlap does (src/FastqReader.h:338-365).
+int kc_count_host(kc_context* c, const uint8_t* fastq, uint64_t n, kc_stats* stats) {
+    if (!c || (!fastq && n)) return fail(KC_ERR_INVALID, "null argument");
+    const auto t0 = std::chrono::steady_clock::now();
+    int rc = begin_run(c, n);
+    if (rc) return rc;
+    const uint64_t B = std::max<uint64_t>(kc::EXT_TILE, c->cfg.batch_bytes & ~(uint64_t)(kc::EXT_TILE - 1));
+    const uint64_t cap = std::min<uint64_t>(B, std::max<uint64_t>(n, 1));
+    CK(c->stage.ensure(kc::HALO + cap + kc::EXT_TILE));
+    CK(cudaEventRecord(c->ev0, c->stream));
+    uint8_t* base = c->stage.as<uint8_t>();
+    const uint64_t chunk = std::max<uint64_t>(c->cfg.chunk_bytes, 1 << 20);
+    for (uint64_t off = 0; off < n; off += cap) {
+        const uint64_t len = std::min<uint64_t>(cap, n - off);
+        if (off > 0) {
+            // previous batch's last HALO bytes (always >= HALO bytes long here)
+            CK(cudaMemcpyAsync(base, base + kc::HALO + cap - kc::HALO, kc::HALO, cudaMemcpyDeviceToDevice, c->stream));
+        }
+        for (uint64_t q = 0; q < len; q += chunk) {
+            const uint64_t m = std::min<uint64_t>(chunk, len - q);
+            CK(cudaMemcpyAsync(base + kc::HALO + q, fastq + off + q, m, cudaMemcpyHostToDevice, c->stream));
+        }
+        if ((rc = run_batch(c, base + kc::HALO, len, off > 0))) return rc;
+    }
+    if ((rc = finish_run(c))) return rc;
+    CK(cudaEventRecord(c->ev1, c->stream));
+    CK(cudaEventSynchronize(c->ev1));
+    float ms = 0;
+    cudaEventElapsedTime(&ms, c->ev0, c->ev1);
+    const double wall = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    fill_stats(c, stats, ms, wall);
+    return KC_OK;
+}
+
+int kc_result_sizes(kc_context* c, uint64_t* low_bytes, uint64_t* n_root, uint64_t* root_counts) {
+    if (!c) return fail(KC_ERR_INVALID, "null context");
+    if (!c->have_result) return fail(KC_ERR_STATE, "no result: run a count first");
+    if (low_bytes) *low_bytes = c->low_total * c->packed_bytes;
+    if (n_root) *n_root = c->root_total;
+    if (root_counts) std::memcpy(root_counts, c->root_counts, sizeof c->root_counts);
+    return KC_OK;
+}
+
+int kc_copy_low(kc_context* c, uint8_t* dst, uint64_t cap) {
+    if (!c) return fail(KC_ERR_INVALID, "null context");
+    if (!c->have_result) return fail(KC_ERR_STATE, "no result: run a count first");
+    const uint64_t bytes = c->low_total * c->packed_bytes;
+    if (cap < bytes) return fail(KC_ERR_INVALID, "destination too small: %llu < %llu", (unsigned long long)cap,
+                                 (unsigned long long)bytes);
+    if (bytes) {
+        CK(cudaMemcpyAsync(dst, c->low_packed.p, bytes, cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
+    }
+    return KC_OK;
+}
+
+int kc_copy_roots(kc_context* c, uint8_t* dst, uint64_t cap) {
+    if (!c) return fail(KC_ERR_INVALID, "null context");
+    if (!c->have_result) return fail(KC_ERR_STATE, "no result: run a count first");
+    const uint64_t bytes = c->root_total * c->record_bytes;
+    if (cap < bytes) return fail(KC_ERR_INVALID, "destination too small: %llu < %llu", (unsigned long long)cap,
+                                 (unsigned long long)bytes);
+    if (bytes) {
+        CK(cudaMemcpyAsync(dst, c->roots.p, bytes, cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
+    }
+    return KC_OK;
+}
+
+int kc_device_results(kc_context* c, const void** d_low, uint64_t* low_bytes, const void** d_roots, uint64_t* n_roots) {
+    if (!c) return fail(KC_ERR_INVALID, "null context");
+    if (!c->have_result) return fail(KC_ERR_STATE, "no result: run a count first");
+    if (d_low) *d_low = c->low_packed.p;
+    if (low_bytes) *low_bytes = c->low_total * c->packed_bytes;
+    if (d_roots) *d_roots = c->roots.p;
+    if (n_roots) *n_roots = c->root_total;
+    return KC_OK;
+}
+
+void* kc_host_alloc(uint64_t bytes) {
+    void* p = nullptr;
+    if (cudaHostAlloc(&p, bytes ? bytes : 1, cudaHostAllocDefault) != cudaSuccess) {
+        cudaGetLastError();
+        fail(KC_ERR_NOMEM, "cudaHostAlloc(%llu) failed", (unsigned long long)bytes);
+        return nullptr;
+    }
+    return p;
+}
+
+void kc_host_free(void* p) {
+    if (p) cudaFreeHost(p);
+}
+
+}  // extern "C"
+
+// Internal hook for the learned sizing model: per-bucket predicted distinct
+// repeat keys for the next count on this context.
+int kc_internal_set_predictions(kc_context* c, const double* per_bucket, uint32_t n) {
+    if (!c) return KC_ERR_INVALID;
+    if (!per_bucket || n == 0) {
+        c->predicted_repeat_keys.clear();
+        return KC_OK;
+    }
+    if (n != c->n_buckets) return fail(KC_ERR_INVALID, "prediction count %u != n_buckets %u", n, c->n_buckets);
+    c->predicted_repeat_keys.assign(per_bucket, per_bucket + n);
+    return KC_OK;
+}
+
+int kc_internal_set_error(int code, const char* msg) { return fail(code, "%s", msg); }
+
+uint64_t kc_internal_record_bytes(const kc_context* c) { return c ? c->record_bytes : 0; }

@@ -1,0 +1,18 @@
+// Internal (non-ABI) declarations shared by the engine's translation units.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+struct kc_context;
+
+// Sort root records (ExportRecord<N>, record_bytes each, grouped by root id
+// with root_counts[256] records per root) by key inside every root, in place
+// on `stream`.  Returns 0 or a negative KC_ERR_* code.
+int kc_sort_roots(void* records, uint64_t n, uint64_t record_bytes, uint32_t k, const uint64_t* root_counts,
+                  cudaStream_t stream);
+const char* kc_sort_error();
+
+int kc_internal_set_predictions(kc_context* c, const double* per_bucket, uint32_t n);
+int kc_internal_set_error(int code, const char* msg);
+uint64_t kc_internal_record_bytes(const kc_context* c);

@@ -1,0 +1,172 @@
+// File side of the C ABI: FASTQ input (plain or gzip) and the reference's
+// output files.
+//
+//   input   gzip is detected by the magic bytes 1F 8B and inflated with zlib,
+//           as src/FastqReader.h:93-104 does; plain files are read as bytes.
+//   output  <dir>/low.bin       packed keys     (src/ExportWriter.h:339-344)
+//           <dir>/root_{id}.bin ExportRecord<N> (src/FinalDrainWriter.h:31-90),
+//           all 256 created, empty ones included.
+
+#include <algorithm>
+#include <cerrno>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include <fcntl.h>
+#include <sys/stat.h>
+#include <unistd.h>
+#include <zlib.h>
+
+#include "../../include/kmer_count.h"
+#include "kc_internal.h"
+
+namespace {
+
+int io_fail(const std::string& m) { return kc_internal_set_error(KC_ERR_IO, m.c_str()); }
+
+bool write_all(int fd, const uint8_t* p, uint64_t n) {
+    while (n) {
+        const ssize_t w = ::write(fd, p, n > (1ull << 30) ? (1ull << 30) : n);
+        if (w > 0) {
+            p += w;
+            n -= (uint64_t)w;
+        } else if (w < 0 && errno == EINTR) {
+            continue;
+        } else {
+            return false;
+        }
+    }
+    return true;
+}
+
+int write_file(const std::string& path, const uint8_t* p, uint64_t n) {
+    const int fd = ::open(path.c_str(), O_WRONLY | O_CREAT | O_TRUNC, 0644);
+    if (fd < 0) return io_fail("cannot open " + path + ": " + std::strerror(errno));
+    const bool ok = write_all(fd, p, n);
+    const int e = errno;
+    if (::close(fd) != 0 || !ok) return io_fail("short write to " + path + ": " + std::strerror(ok ? errno : e));
+    return KC_OK;
+}
+
+std::string with_slash(const char* d) {
+    std::string s = d && *d ? d : ".";
+    if (s.back() != '/') s.push_back('/');
+    return s;
+}
+
+// Reads the whole input into page-locked memory (inflating gzip).
+int read_fastq(const char* path, uint8_t** out, uint64_t* n) {
+    *out = nullptr;
+    *n = 0;
+    const int fd = ::open(path, O_RDONLY);
+    if (fd < 0) return io_fail(std::string("Failed to open file ") + path + ": " + std::strerror(errno));
+    struct stat st;
+    if (fstat(fd, &st) != 0) {
+        ::close(fd);
+        return io_fail(std::string("Failed to get file size of ") + path);
+    }
+    unsigned char magic[2] = {0, 0};
+    const ssize_t m = ::read(fd, magic, 2);
+    const bool gz = m == 2 && magic[0] == 0x1F && magic[1] == 0x8B;
+    if (!gz) {
+        const uint64_t size = (uint64_t)st.st_size;
+        uint8_t* buf = (uint8_t*)kc_host_alloc(size + 1);
+        if (!buf) {
+            ::close(fd);
+            return KC_ERR_NOMEM;
+        }
+        uint64_t got = 0;
+        if (lseek(fd, 0, SEEK_SET) != 0) {
+            ::close(fd);
+            kc_host_free(buf);
+            return io_fail("seek failed");
+        }
+        while (got < size) {
+            const ssize_t r = ::read(fd, buf + got, std::min<uint64_t>(size - got, 1ull << 30));
+            if (r < 0 && errno == EINTR) continue;
+            if (r <= 0) {
+                ::close(fd);
+                kc_host_free(buf);
+                return io_fail(std::string("Failed to read fastq data from ") + path);
+            }
+            got += (uint64_t)r;
+        }
+        ::close(fd);
+        *out = buf;
+        *n = size;
+        return KC_OK;
+    }
+    ::close(fd);
+    gzFile gzf = gzopen(path, "rb");
+    if (!gzf) return io_fail(std::string("Failed to open gzip file: ") + path);
+    gzbuffer(gzf, 1u << 20);
+    std::vector<uint8_t> tmp;
+    tmp.reserve((size_t)st.st_size * 4 + 1);  // the reference also assumes ~4x (src/FastqPreReader.h:316-326)
+    std::vector<uint8_t> chunk(1u << 24);
+    for (;;) {
+        const int r = gzread(gzf, chunk.data(), (unsigned)chunk.size());
+        if (r < 0) {
+            int errnum = 0;
+            const char* msg = gzerror(gzf, &errnum);
+            gzclose(gzf);
+            return io_fail(std::string("Failed to read fastq data: ") + (msg ? msg : "gzip error"));
+        }
+        if (r == 0) break;
+        tmp.insert(tmp.end(), chunk.begin(), chunk.begin() + r);
+    }
+    gzclose(gzf);
+    uint8_t* buf = (uint8_t*)kc_host_alloc(tmp.size() + 1);
+    if (!buf) return KC_ERR_NOMEM;
+    if (!tmp.empty()) std::memcpy(buf, tmp.data(), tmp.size());
+    *out = buf;
+    *n = tmp.size();
+    return KC_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int kc_write_outputs(kc_context* ctx, const char* out_dir) {
+    if (!ctx) return kc_internal_set_error(KC_ERR_INVALID, "null context");
+    uint64_t low_bytes = 0, n_root = 0, counts[256];
+    int rc = kc_result_sizes(ctx, &low_bytes, &n_root, counts);
+    if (rc) return rc;
+    const std::string dir = with_slash(out_dir);
+    if (::mkdir(dir.c_str(), 0755) != 0 && errno != EEXIST)
+        return io_fail("cannot create " + dir + ": " + std::strerror(errno));
+    const uint64_t rec = kc_internal_record_bytes(ctx);
+    const uint64_t root_bytes = n_root * rec;
+    uint8_t* host = (uint8_t*)kc_host_alloc(std::max(low_bytes, root_bytes) + 1);
+    if (!host) return KC_ERR_NOMEM;
+    if ((rc = kc_copy_low(ctx, host, low_bytes)) == KC_OK) rc = write_file(dir + "low.bin", host, low_bytes);
+    if (rc == KC_OK && (rc = kc_copy_roots(ctx, host, root_bytes)) == KC_OK) {
+        uint64_t off = 0;
+        for (int r = 0; r < 256 && rc == KC_OK; ++r) {
+            rc = write_file(dir + "root_" + std::to_string(r) + ".bin", host + off * rec, counts[r] * rec);
+            off += counts[r];
+        }
+    }
+    kc_host_free(host);
+    return rc;
+}
+
+int kc_count_fastq(const kc_config* cfg, const char* fastq_path, const char* out_dir, kc_stats* stats) {
+    if (!cfg || !fastq_path) return kc_internal_set_error(KC_ERR_INVALID, "null argument");
+    kc_context* ctx = nullptr;
+    int rc = kc_create(cfg, &ctx);
+    if (rc) return rc;
+    uint8_t* data = nullptr;
+    uint64_t n = 0;
+    if ((rc = read_fastq(fastq_path, &data, &n)) == KC_OK) {
+        rc = kc_count_host(ctx, data, n, stats);
+        kc_host_free(data);
+        if (rc == KC_OK) rc = kc_write_outputs(ctx, out_dir ? out_dir : "./tmp/");
+    }
+    kc_destroy(ctx);
+    return rc;
+}
+
+}  // extern "C"

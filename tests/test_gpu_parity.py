@@ -1,0 +1,138 @@
+"""GPU path (through the C ABI) against the oracle and the reference.
+
+Bit-exact: the merged (canonical k-mer, count) multiset of low.bin + root
+files must equal the oracle's, and, for the golden inputs, the digest the
+reference's own output produced.  The first-occurrence filter may move a key
+between low.bin and its root file only as the reference design allows (a
+false positive puts its whole count in the root record)."""
+import hashlib
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+import inputs
+import oracle
+import parity
+from conftest import ROOT
+
+pytestmark = pytest.mark.gpu
+
+kc = pytest.importorskip("kmertreecounter_b200")
+from kmertreecounter_b200 import synth  # noqa: E402
+
+_data = {}
+
+
+def golden_input(golden, name):
+    if name not in _data:
+        e = golden[name]
+        d = getattr(inputs, e["builder"])(**e["kwargs"])
+        assert hashlib.sha256(d).hexdigest() == e["fastq_sha256"]
+        _data[name] = np.frombuffer(d, np.uint8)
+    return _data[name]
+
+
+GOLDEN = [(n, k) for n, ks in [("plain_small", [31]), ("plain_small_s7", [21, 32, 33, 63]),
+                               ("adversarial", [17, 31, 32, 33, 64])] for k in ks]
+
+
+@pytest.mark.parametrize("name,k", GOLDEN)
+def test_golden_digest(golden, name, k):
+    g = golden[name]["k"][str(k)]
+    data = golden_input(golden, name)
+    with kc.Counter(k=k) as c:
+        st = c.count_host(data)
+        assert st.total_kmers == g["K"]
+        low, roots, per_root = parity.gpu_outputs(c, k)
+        parity.check_layout(low, roots, per_root, k)
+        mk, mc = parity.merged(low, roots, k)
+        assert mk.shape[0] == g["D"]
+        assert oracle.digest(mk, mc) == g["digest"]
+        assert [int(x) for x in oracle.histogram(mc, 1, 64)] == g["hist_1_64"]
+
+
+@pytest.mark.parametrize("k", [1, 5, 12, 21, 31, 32, 33, 47, 63, 64])
+@pytest.mark.parametrize("buckets", [256, 4096])
+def test_small_vs_oracle(k, buckets):
+    p = synth.plain_small(seed=100 + k, scale=0.05)
+    p.sub_rate = 0.02
+    data = synth.fastq(p)
+    with kc.Counter(k=k, n_buckets=buckets) as c:
+        c.count_host(data)
+        parity.check_exact(c, data, k)
+
+
+def test_multi_batch_matches(golden):
+    data = golden_input(golden, "adversarial")
+    want = oracle.count(data, 31)
+    with kc.Counter(k=31, batch_bytes=1 << 20, chunk_bytes=1 << 20) as c:
+        st = c.count_host(data)
+        assert st.batches == (data.size + (1 << 20) - 1) // (1 << 20)
+        parity.check_exact(c, data, 31, want)
+
+
+def test_forced_rehash_stays_exact():
+    p = synth.plain_small(seed=9, scale=0.2)
+    data = synth.fastq(p)
+    with kc.Counter(k=31, repeat_ratio=1e-7) as c:
+        st = c.count_host(data)
+        assert st.rehashes > 0
+        parity.check_exact(c, data, 31)
+
+
+def test_device_input_matches_host():
+    torch = pytest.importorskip("torch")
+    p = synth.plain_small(seed=4, scale=0.1)
+    data = synth.fastq(p)
+    d = torch.from_numpy(data).cuda()
+    want = oracle.count(data, 25)
+    with kc.Counter(k=25, batch_bytes=1 << 20) as c:
+        c.count_device(d.data_ptr(), d.numel())
+        torch.cuda.synchronize()
+        parity.check_exact(c, data, 25, want)
+
+
+@pytest.mark.parametrize("lo,hi", [(2, 2**32 - 1), (1, 3), (3, 10)])
+def test_min_max_filter(lo, hi):
+    p = synth.plain_small(seed=21, scale=0.1)
+    data = synth.fastq(p)
+    with kc.Counter(k=21, min_count=lo, max_count=hi) as c:
+        c.count_host(data)
+        parity.check_filtered(c, data, 21, lo, hi)
+
+
+@pytest.mark.parametrize("data", [b"", b"@r\n", b"@r\nACG\n+\nIII\n", b"@r\n" + b"N" * 100 + b"\n+\n",
+                                  b"@r\nACGTACGTAC", b"\n\n\n\n\n\n\n\n", b"@a\nACGTTGCA\r\n+\r\nIIIIIIII\r\n"])
+@pytest.mark.parametrize("k", [4, 31, 40])
+def test_edge_inputs(data, k):
+    arr = np.frombuffer(data, np.uint8)
+    with kc.Counter(k=k) as c:
+        c.count_host(arr)
+        parity.check_exact(c, arr, k)
+        lb, nr, per = c.sizes()
+        assert sum(per) == nr
+
+
+def test_cli_output_read_by_reference_tool(golden, tmp_path):
+    """bin/Tree writes ./tmp/low.bin and root_0..255.bin that the reference's
+    own histogram_tool reads unchanged and turns into the same histogram."""
+    data = golden_input(golden, "adversarial")
+    fq = tmp_path / "in.fastq"
+    fq.write_bytes(data.tobytes())
+    tree = os.path.join(ROOT, "kmertreecounter_b200", "bin", "Tree")
+    p = subprocess.run([tree, str(fq), "33", "8", "4"], cwd=tmp_path, capture_output=True, text=True)
+    assert p.returncode == 0, p.stderr
+    g = golden["adversarial"]["k"]["33"]
+    assert f"Total read k-mer count: {g['K']}" in p.stdout
+    files = sorted(os.listdir(tmp_path / "tmp"))
+    assert "low.bin" in files and all(f"root_{r}.bin" in files for r in range(256))
+    low, roots, _ = oracle.read_outputs(str(tmp_path / "tmp"), 33)
+    mk, mc = oracle.merged_counts(low, roots["key"], roots["count"])
+    assert oracle.digest(mk, mc) == g["digest"]
+    if os.path.exists(oracle.REF_HIST):
+        h = tmp_path / "hist.tsv"
+        subprocess.run([oracle.REF_HIST, "precise", str(tmp_path / "tmp"), "33", "4", "4", str(h), "1", "64"],
+                       check=True, capture_output=True)
+        assert [int(line.split("\t")[1]) for line in h.read_text().splitlines()] == g["histogram_tool_precise_1_64"]

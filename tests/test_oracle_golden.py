@@ -1,0 +1,42 @@
+"""The CPU oracle against outputs of the reference implementation itself.
+
+tests/golden/golden.json was produced by tests/golden/make_golden.py from the
+reference `Tree` binary (compiled from the reference's sources) and its
+histogram_tool: for each input and k it holds the reference's K, the number
+of distinct keys, a sha256 of the merged exact (key, count) table and the
+count histogram.  Here the oracle must reproduce every one of them.
+"""
+import hashlib
+
+import numpy as np
+import pytest
+
+import inputs
+import oracle
+
+CASES = [(name, k) for name, ks in [("plain_small", [31]), ("plain_small_s7", [21, 32, 33, 63]),
+                                    ("adversarial", [17, 31, 32, 33, 64])] for k in ks]
+
+_cache = {}
+
+
+def fastq_for(golden, name):
+    if name not in _cache:
+        e = golden[name]
+        data = getattr(inputs, e["builder"])(**e["kwargs"])
+        assert len(data) == e["fastq_bytes"]
+        assert hashlib.sha256(data).hexdigest() == e["fastq_sha256"], "input generator drifted"
+        _cache[name] = np.frombuffer(data, dtype=np.uint8)
+    return _cache[name]
+
+
+@pytest.mark.parametrize("name,k", CASES)
+def test_oracle_matches_reference(golden, name, k):
+    g = golden[name]["k"][str(k)]
+    data = fastq_for(golden, name)
+    keys, counts, K = oracle.count(data, k)
+    assert K == g["K"]
+    assert keys.shape[0] == g["D"]
+    assert oracle.digest(keys, counts.astype(np.uint64)) == g["digest"]
+    assert [int(x) for x in oracle.histogram(counts, 1, 64)] == g["hist_1_64"]
+    assert g["hist_1_64"] == g["histogram_tool_precise_1_64"]
