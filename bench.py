@@ -1,0 +1,371 @@
+"""Benchmark: FASTQ Gbases/s to exact canonical k-mer counts on B200.
+
+Workload (default): the genome-scale shape -- seeded 100 Mbp genome, 45% GC,
+20% repeat families, 30x coverage of 150 bp reads (20M reads, 3 Gbases,
+~6.3 GB FASTQ), canonical k=31 with 64-bit keys.  A step counts the whole
+FASTQ once: extraction, routing, first-occurrence filter, repeat tables,
+low.bin packing and root-record export, all on the device.
+
+  value   FASTQ resident in HBM, outputs left in HBM (kc_count_device)
+  e2e     the C ABI on HOST buffers: pinned FASTQ -> H2D -> count -> packed
+          low.bin + root records copied back into pinned host buffers
+          (kc_count_host + kc_copy_low + kc_copy_roots)
+
+`--impl reference` times the reference's own CPU implementation (the `Tree`
+binary built from the reference sources into oracle/_ref, else the oracle
+port) on a bounded sample of the same workload, with all host threads.
+
+Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+Multi-GPU: one process per GPU under torch.distributed.run; each rank counts
+its own copy of the workload (weak scaling, no data-path collective).
+"""
+import argparse
+import ctypes
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+import numpy as np  # noqa: E402
+
+WORKLOADS = {
+    # name: (synth preset, k, n_buckets)
+    "genome_scale": ("genome_scale", 31, 256),
+    "plain_small": ("plain_small", 31, 256),
+    "large_long": ("large_long", 63, 4096),
+}
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="genome_scale", choices=sorted(WORKLOADS))
+    ap.add_argument("--scale", type=float, default=1.0, help="shrink genome and reads together")
+    ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--sample-scale", type=float, default=0.05, help="CPU sample size, fraction of the workload")
+    return ap.parse_args()
+
+
+def dist_env():
+    return int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("LOCAL_RANK", "0"))
+
+
+# --------------------------------------------------------------- clocks
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# --------------------------------------------------------------- workload
+
+def make_workload(name, scale):
+    from kmertreecounter_b200 import synth
+    preset, k, buckets = WORKLOADS[name]
+    p = getattr(synth, preset)(scale=scale)
+    bases = int(p.n_reads) * int(p.read_len_min) if p.read_len_min == p.read_len_max else None
+    return p, k, buckets, bases
+
+
+def cpu_sample(name, sample_scale, workdir):
+    """Write a bounded sample of the workload (same shape, shrunken) to disk."""
+    from kmertreecounter_b200 import synth
+    preset, k, _ = WORKLOADS[name]
+    p = getattr(synth, preset)(scale=sample_scale)
+    data = synth.fastq(p)
+    path = os.path.join(workdir, "sample.fastq")
+    data.tofile(path)
+    return path, data, k, int(p.n_reads) * int(p.read_len_min), p
+
+
+def time_reference(path, data, k, bases, runs, workdir):
+    """Reference `Tree` (or the oracle port) on the sample: list of
+    (Gbases/s, seconds), kind, cores."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    cores = os.cpu_count() or 1
+    K_expected = oracle.extract(data, k).shape[0]
+    out = []
+    if os.path.exists(oracle.REF_TREE):
+        kind = "reference"
+        mem = max(4, int(os.sysconf("SC_PAGE_SIZE") * os.sysconf("SC_PHYS_PAGES") / 2**30 * 0.7))
+        for _ in range(runs):
+            for attempt in range(3):
+                t = time.perf_counter()
+                stdout, rc = oracle.run_reference(path, k, workdir, threads=max(6, cores), mem_gb=mem)
+                dt = time.perf_counter() - t
+                if rc == 0 and oracle.reference_total(stdout) == K_expected:
+                    out.append((bases / dt / 1e9, dt))
+                    break
+        if not out:
+            kind = "port"
+    else:
+        kind = "port"
+    if kind == "port":
+        cores = 1
+        for _ in range(runs):
+            t = time.perf_counter()
+            oracle.count(data, k)
+            dt = time.perf_counter() - t
+            out.append((bases / dt / 1e9, dt))
+    return out, kind, cores
+
+
+# --------------------------------------------------------------- our arm
+
+def run_ours(args):
+    import torch
+    import kmertreecounter_b200 as kc
+    from kmertreecounter_b200 import synth
+
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+
+    p, k, buckets, bases = make_workload(args.workload, args.scale)
+    g = synth.genome(p)
+    n = synth.fastq_bytes(p)
+    host_ptr = kc.host_alloc(n)  # pinned FASTQ for the e2e leg
+    synth.fastq(p, g, out=host_ptr)
+    del g
+    host = np.ctypeslib.as_array((ctypes.c_uint8 * n).from_address(host_ptr))
+    dev = torch.empty(n, dtype=torch.uint8, device="cuda")
+    dev.copy_(torch.from_numpy(host))
+    torch.cuda.synchronize()
+
+    cfg = kc.default_config(k=k, n_buckets=buckets, device=local)
+    counter = kc.Counter(cfg)
+    stream = torch.cuda.ExternalStream(counter.stream)
+
+    def barrier():
+        if world > 1:
+            import torch.distributed as dist
+            dist.barrier()
+
+    # warm-up (also sizes every buffer)
+    for _ in range(max(args.warmup, 0)):
+        counter.count_device(dev.data_ptr(), n)
+
+    # --- device-resident timed region
+    counter.set_profiling(True)
+    stage_ms, stage_launch = {}, {}
+    clocks = ClockSampler(local)
+    barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        st = counter.count_device(dev.data_ptr(), n)
+        for name, (ms, ln) in counter.stage_times().items():
+            stage_ms[name] = stage_ms.get(name, 0.0) + ms
+            stage_launch[name] = stage_launch.get(name, 0) + ln
+    e1.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    clk = clocks.stop()
+    total_ms = e0.elapsed_time(e1)
+    if world > 1:
+        import torch.distributed as dist
+        t = torch.tensor([total_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+    ms_step = total_ms / args.steps
+    stats = st.as_dict()
+    stats.pop("root_counts", None)
+    gpu_launches = int(sum(stage_launch.values()))
+
+    # --- end to end through the C ABI with host buffers
+    lb, nr, _ = counter.sizes()
+    rec = kc.record_bytes(k)
+    out_low = kc.host_alloc(lb + (1 << 26))
+    out_roots = kc.host_alloc(nr * rec + (1 << 26))
+    e2e_ms = []
+    counter.set_profiling(False)
+    for i in range(max(1, args.e2e_steps) + 1):
+        torch.cuda.synchronize()
+        barrier()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        counter.count_host_ptr(host_ptr, n)
+        lb2, nr2, _ = counter.sizes()
+        counter.copy_low_into(out_low, lb2)
+        counter.copy_roots_into(out_roots, nr2 * rec)
+        b.record(stream)
+        torch.cuda.synchronize()
+        if i > 0:  # first call is a warm-up of the host path
+            e2e_ms.append(a.elapsed_time(b))
+    e2e_step = statistics.median(e2e_ms)
+    if world > 1:
+        import torch.distributed as dist
+        t = torch.tensor([e2e_step], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_step = float(t.item())
+
+    # --- roofline of the dominant kernel (count_routed), SURVEY 8(d) units:
+    # 64 B per k-mer (one 32 B filter sector read + write) and 64 B per
+    # repeat occurrence (one table sector read + write).
+    from measured import peaks
+    pk = peaks()
+    K, L = stats["total_kmers"], stats["low_records"]
+    alg_bytes = 64 * K + 64 * (K - L)
+    count_ms = stage_ms.get("count", 0.0) / args.steps
+    achieved = alg_bytes / (count_ms / 1e3) / 1e9 if count_ms > 0 else None
+    dominant = max(stage_ms, key=lambda s: stage_ms[s]) if stage_ms else None
+
+    line = {
+        "metric": "FASTQ Gbases/s to exact k-mer counts on 1 B200",
+        "value": bases * world / (ms_step / 1e3) / 1e9,
+        "unit": "Gbases/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": ms_step,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "u64",
+        "data": "synthetic (seeded generator, reference benchmark shape)",
+        "config": {"workload": f"{args.workload}: 100 Mbp genome 45% GC 20% repeats, 30x 150 bp (20M reads), k=31"
+                   if args.workload == "genome_scale" and args.scale == 1.0 else f"{args.workload} scale={args.scale}",
+                   "k": k, "n_buckets": buckets, "fastq_bytes": n, "bases": bases, "reads": int(p.n_reads),
+                   "l2": "inputs larger than L2 (FASTQ %.1f GB)" % (n / 1e9), "parallelism": f"replica x{world}"},
+        "distinct_kmers_per_s": None,
+        "stats": stats,
+        "stages_ms_per_step": {s: v / args.steps for s, v in stage_ms.items()},
+        "gpu_launches": gpu_launches,
+        "e2e": {"value": bases * world / (e2e_step / 1e3) / 1e9, "unit": "Gbases/s", "ms_per_step": e2e_step,
+                "h2d_bytes_per_step": n, "d2h_bytes_per_step": lb + nr * rec},
+        "roofline": {"bound": "hbm", "kernel": "count_routed", "achieved": achieved, "peak": pk["hbm_gbs"],
+                     "unit": "GB/s", "frac": (achieved / pk["hbm_gbs"]) if achieved else None,
+                     "peak_source": pk["source"], "alg_bytes_per_launch": alg_bytes, "traffic": None,
+                     "dominant_stage": dominant},
+        "clocks": clk,
+    }
+    kc.host_free(out_low)
+    kc.host_free(out_roots)
+    del dev
+    counter.close()
+    kc.host_free(host_ptr)
+
+    if rank == 0 and not args.no_cpu_baseline:
+        with tempfile.TemporaryDirectory() as wd:
+            path, data, kk, sbases, sp = cpu_sample(args.workload, args.sample_scale, wd)
+            res, kind, cores = time_reference(path, data, kk, sbases, 2, wd)
+            best = max(r[0] for r in res)
+            line["cpu_baseline"] = {"value": best, "unit": "Gbases/s", "cores": cores, "kind": kind,
+                                    "sample": f"{args.workload} at scale {args.sample_scale}: {int(sp.n_reads)} reads, "
+                                              f"{data.size} FASTQ bytes, best of {len(res)} runs"}
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+# --------------------------------------------------------------- reference arm
+
+def run_reference(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return
+    with tempfile.TemporaryDirectory() as wd:
+        path, data, k, bases, sp = cpu_sample(args.workload, args.sample_scale, wd)
+        res, kind, cores = time_reference(path, data, k, bases, max(args.warmup, 0) + args.steps, wd)
+        timed = res[max(args.warmup, 0):] or res
+        secs = sum(r[1] for r in timed)
+        value = bases * len(timed) / secs / 1e9
+        line = {
+            "metric": "FASTQ Gbases/s to exact k-mer counts on 1 B200",
+            "impl": "reference",
+            "value": value,
+            "unit": "Gbases/s",
+            "n_gpus": world,
+            "steps": len(timed),
+            "warmup": args.warmup,
+            "ms_per_step": secs / len(timed) * 1e3,
+            "higher_is_better": True,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "u64",
+            "data": "synthetic (seeded generator, reference benchmark shape)",
+            "config": {"workload": f"{args.workload} sample at scale {args.sample_scale}", "k": k,
+                       "fastq_bytes": int(data.size), "bases": bases},
+            "cpu_baseline": {"value": value, "unit": "Gbases/s", "cores": cores, "kind": kind,
+                             "sample": f"{args.workload} at scale {args.sample_scale}: {int(sp.n_reads)} reads per step"},
+            "e2e": {"value": value, "unit": "Gbases/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        }
+        print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -147,6 +147,30 @@ void kc_host_free(void* p);
 /* CUDA stream of the context (as void*), for callers that time it. */
 void* kc_stream(kc_context* ctx);
 
+/* ---- diagnostics ----------------------------------------------------------
+ * The reference prints per-stage timers and, with TEST_MODE, cycle counters
+ * (src/main.cpp:270-309, src/definition.h:4).  Here: with profiling on, every
+ * stage of a count is bracketed by CUDA events on the context's stream. */
+#define KC_STAGE_LINES 0
+#define KC_STAGE_SCAN 1
+#define KC_STAGE_EXTRACT_HIST 2
+#define KC_STAGE_EXTRACT_SCATTER 3
+#define KC_STAGE_COUNT_ROUTED 4
+#define KC_STAGE_REHASH 5
+#define KC_STAGE_PACK_LOW 6
+#define KC_STAGE_EXPORT 7
+#define KC_STAGE_SORT 8
+#define KC_STAGE_INIT 9
+#define KC_STAGE_COUNT 10
+
+int kc_set_profiling(kc_context* ctx, int enable);
+
+/* Device milliseconds and kernel launches per stage of the last count
+ * (arrays of `cap` entries; either may be NULL).  Returns KC_STAGE_COUNT. */
+int kc_stage_times(kc_context* ctx, double* ms, uint64_t* launches, int cap);
+
+const char* kc_stage_name(int stage);
+
 #ifdef __cplusplus
 }
 #endif

@@ -28,7 +28,9 @@ ABI_SYMBOLS = (
     "kc_config_default", "kc_last_error", "kc_packed_bytes", "kc_record_bytes", "kc_count_fastq",
     "kc_create", "kc_destroy", "kc_count_host", "kc_count_device", "kc_result_sizes", "kc_copy_low",
     "kc_copy_roots", "kc_write_outputs", "kc_device_results", "kc_host_alloc", "kc_host_free", "kc_stream",
+    "kc_set_profiling", "kc_stage_times", "kc_stage_name",
 )
+STAGE_COUNT = 10
 
 
 class KcConfig(C.Structure):
@@ -85,6 +87,9 @@ def _load():
         "kc_host_alloc": (vp, [u64]),
         "kc_host_free": (None, [vp]),
         "kc_stream": (vp, [vp]),
+        "kc_set_profiling": (i32, [vp, i32]),
+        "kc_stage_times": (i32, [vp, C.POINTER(C.c_double), C.POINTER(u64), i32]),
+        "kc_stage_name": (C.c_char_p, [i32]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -198,6 +203,22 @@ class Counter:
         out = np.empty(nr, dtype=dt)
         check(lib.kc_copy_roots(self._ctx, out.ctypes.data if nr else None, nr * dt.itemsize))
         return out, counts
+
+    def set_profiling(self, on=True):
+        check(lib.kc_set_profiling(self._ctx, 1 if on else 0))
+
+    def stage_times(self):
+        """{stage: (device ms, kernel launches)} of the last count."""
+        ms = (C.c_double * STAGE_COUNT)()
+        ln = (C.c_uint64 * STAGE_COUNT)()
+        n = lib.kc_stage_times(self._ctx, ms, ln, STAGE_COUNT)
+        return {lib.kc_stage_name(i).decode(): (ms[i], ln[i]) for i in range(n)}
+
+    def copy_low_into(self, addr, cap):
+        check(lib.kc_copy_low(self._ctx, C.c_void_p(addr), cap))
+
+    def copy_roots_into(self, addr, cap):
+        check(lib.kc_copy_roots(self._ctx, C.c_void_p(addr), cap))
 
     def write_outputs(self, out_dir):
         check(lib.kc_write_outputs(self._ctx, str(out_dir).encode()))

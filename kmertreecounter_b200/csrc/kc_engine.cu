@@ -148,9 +148,48 @@ struct kc_context {
 
     // optional learned sizing hook (per-bucket repeat-key predictions)
     std::vector<double> predicted_repeat_keys;
+
+    // stage profiling: CUDA event pairs recorded on `stream` around each stage
+    bool profiling = false;
+    std::vector<cudaEvent_t> ev_pool;
+    size_t ev_used = 0;
+    std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> spans;
+    uint64_t launches[KC_STAGE_COUNT] = {};
+    double stage_ms[KC_STAGE_COUNT] = {};
 };
 
 namespace {
+
+const char* const kStageNames[KC_STAGE_COUNT] = {"lines", "scan", "extract_hist", "extract_scatter", "count",
+                                                  "rehash", "pack_low", "export", "sort", "init"};
+
+cudaEvent_t next_event(kc_context* c) {
+    if (c->ev_used == c->ev_pool.size()) {
+        cudaEvent_t e = nullptr;
+        if (cudaEventCreate(&e) != cudaSuccess) return nullptr;
+        c->ev_pool.push_back(e);
+    }
+    return c->ev_pool[c->ev_used++];
+}
+
+// RAII span: records start/end events of a stage when profiling is on and
+// counts the launches issued inside it.
+struct Stage {
+    kc_context* c;
+    int id;
+    cudaEvent_t a = nullptr;
+    Stage(kc_context* ctx, int s, uint64_t n_launch = 1) : c(ctx), id(s) {
+        c->launches[s] += n_launch;
+        if (c->profiling && (a = next_event(c))) cudaEventRecord(a, c->stream);
+    }
+    ~Stage() {
+        if (!a) return;
+        cudaEvent_t b = next_event(c);
+        if (!b) return;
+        cudaEventRecord(b, c->stream);
+        c->spans.push_back({id, {a, b}});
+    }
+};
 
 int setup_shape(kc_context* c) {
     const kc_config& g = c->cfg;
@@ -177,6 +216,7 @@ template <class TI, class TO>
 int device_scan(kc_context* c, const TI* in, uint64_t n, TO* out, uint64_t base, uint64_t* d_total) {
     const uint64_t nb = std::max<uint64_t>(1, ceil_div(n, kc::SCAN_TILE));
     CK(c->scan_sums.ensure(nb * sizeof(uint64_t)));
+    Stage st(c, KC_STAGE_SCAN, n ? 3 : 1);
     uint64_t* sums = c->scan_sums.as<uint64_t>();
     if (n) kc::scan_reduce<TI><<<nb, kc::SCAN_BLOCK, 0, c->stream>>>(in, n, sums);
     else CK(cudaMemsetAsync(sums, 0, sizeof(uint64_t), c->stream));
@@ -211,11 +251,14 @@ int size_structures(kc_context* c, const std::vector<uint64_t>& kb, double scale
     CK(c->table.ensure(ts * c->slot_bytes + ts * c->slot_bytes / 2));
     CK(c->meta.ensure(nb * sizeof(kc::BucketMeta)));
     CK(cudaMemcpyAsync(c->meta.p, c->h_meta.data(), nb * sizeof(kc::BucketMeta), cudaMemcpyHostToDevice, c->stream));
-    CK(cudaMemsetAsync(c->bloom.p, 0, bw * sizeof(uint64_t), c->stream));
-    const int ig = 148 * 8;
-    if (c->nw == 1) kc::init_slots<1><<<ig, 256, 0, c->stream>>>(c->table.p, ts);
-    else kc::init_slots<2><<<ig, 256, 0, c->stream>>>(c->table.p, ts);
-    CK(cudaGetLastError());
+    {
+        Stage st(c, KC_STAGE_INIT, 1);
+        CK(cudaMemsetAsync(c->bloom.p, 0, bw * sizeof(uint64_t), c->stream));
+        const int ig = 148 * 8;
+        if (c->nw == 1) kc::init_slots<1><<<ig, 256, 0, c->stream>>>(c->table.p, ts);
+        else kc::init_slots<2><<<ig, 256, 0, c->stream>>>(c->table.p, ts);
+        CK(cudaGetLastError());
+    }
     CK(c->overflow.ensure(nb * sizeof(uint32_t)));
     CK(cudaMemsetAsync(c->overflow.p, 0, nb * sizeof(uint32_t), c->stream));
     c->h_overflow.assign(nb, 0);
@@ -226,7 +269,7 @@ int size_structures(kc_context* c, const std::vector<uint64_t>& kb, double scale
 template <int NW>
 void launch_count(kc_context* c, uint64_t n_keys, int use_filter) {
     constexpr int TILE = kc::count_tile<NW>();
-    const uint64_t tiles = ceil_div(n_keys, TILE);
+    const uint64_t tiles = ceil_div(n_keys, TILE);  // CTAs; each warp owns count_seg<NW>() keys
     if (!tiles) return;
     kc::CountArgs a;
     a.routed = c->routed.p;
@@ -234,11 +277,12 @@ void launch_count(kc_context* c, uint64_t n_keys, int use_filter) {
     a.meta = c->meta.as<kc::BucketMeta>();
     a.bloom = c->bloom.as<uint64_t>();
     a.table = c->table.p;
-    a.tile_low = c->tile_low.as<uint32_t>();
-    a.tile_fail = c->tile_fail.as<uint32_t>();
+    a.seg_low = c->tile_low.as<uint32_t>();
+    a.seg_fail = c->tile_fail.as<uint32_t>();
     a.bucket_overflow = c->overflow.as<uint32_t>();
     a.bucket_shift = c->bucket_shift;
     a.use_filter = use_filter;
+    Stage st(c, use_filter ? KC_STAGE_COUNT_ROUTED : KC_STAGE_REHASH);
     kc::count_routed<NW><<<tiles, kc::CNT_THREADS, 0, c->stream>>>(a);
 }
 
@@ -268,6 +312,7 @@ int rehash_loop(kc_context* c, uint64_t n_keys) {
                 const uint64_t off = c->table_slots_used;
                 void* nt = c->table.as<uint8_t>() + off * c->slot_bytes;
                 const void* ot = c->table.as<uint8_t>() + c->h_meta[b].tab_off * c->slot_bytes;
+                Stage st(c, KC_STAGE_REHASH, 2);
                 kc::init_slots<NW><<<256, 256, 0, c->stream>>>(nt, new_slots);
                 CK(cudaMemsetAsync(d_failed, 0, sizeof(uint32_t), c->stream));
                 kc::rehash_bucket<NW><<<std::max<uint64_t>(1, std::min<uint64_t>(1184, ceil_div(old_slots, 256))), 256, 0,
@@ -308,7 +353,9 @@ int launch_extract(kc_context* c, const uint8_t* buf, uint64_t n, int has_halo, 
     a.bucket_count = c->bucket_count.as<unsigned long long>();
     a.bucket_cursor = c->bucket_cursor.as<unsigned long long>();
     a.routed = c->routed.p;
+    a.error = c->scalars.as<uint32_t>() + 12;
     const size_t smem = (size_t)c->n_buckets * 16;
+    Stage st(c, mode == kc::HIST ? KC_STAGE_EXTRACT_HIST : KC_STAGE_EXTRACT_SCATTER);
     if (mode == kc::HIST) kc::extract_kernel<NW, kc::HIST><<<tiles, kc::EXT_THREADS, smem, c->stream>>>(a);
     else kc::extract_kernel<NW, kc::SCATTER><<<tiles, kc::EXT_THREADS, smem, c->stream>>>(a);
     CK(cudaGetLastError());
@@ -326,7 +373,11 @@ int process_batch(kc_context* c, const uint8_t* buf, uint64_t n, int has_halo) {
     CK(c->tile_line.ensure(std::max<uint64_t>(tiles, 1) * sizeof(uint64_t)));
     CK(c->scalars.ensure(64));
     uint64_t* d_scal = c->scalars.as<uint64_t>();
-    if (tiles) kc::lines_per_tile<<<tiles, kc::EXT_THREADS, 0, c->stream>>>(buf, n, c->tile_nl.as<uint32_t>());
+    CK(cudaMemsetAsync(c->scalars.as<uint32_t>() + 12, 0, sizeof(uint32_t), c->stream));
+    if (tiles) {
+        Stage st(c, KC_STAGE_LINES);
+        kc::lines_per_tile<<<tiles, kc::EXT_THREADS, 0, c->stream>>>(buf, n, c->tile_nl.as<uint32_t>());
+    }
     CK(cudaGetLastError());
     int rc = device_scan<uint32_t, uint64_t>(c, c->tile_nl.as<uint32_t>(), tiles, c->tile_line.as<uint64_t>(),
                                              c->line_base, d_scal + 0);
@@ -360,29 +411,35 @@ int process_batch(kc_context* c, const uint8_t* buf, uint64_t n, int has_halo) {
     if (!kb) return KC_OK;
 
     constexpr int CT = kc::count_tile<NW>();
+    constexpr int SEG = kc::count_seg<NW>();
     const uint64_t ctiles = ceil_div(kb, CT);
+    const uint64_t nsegs = ceil_div(kb, SEG);
     CK(c->routed.ensure(ctiles * CT * (uint64_t)(8 * NW)));
-    CK(c->tile_low.ensure(ctiles * sizeof(uint32_t)));
-    CK(c->tile_fail.ensure(ctiles * sizeof(uint32_t)));
-    CK(c->tile_low_prefix.ensure(ctiles * sizeof(uint64_t)));
+    CK(c->tile_low.ensure(ctiles * (CT / SEG) * sizeof(uint32_t)));
+    CK(c->tile_fail.ensure(ctiles * (CT / SEG) * sizeof(uint32_t)));
+    CK(c->tile_low_prefix.ensure(ctiles * (CT / SEG) * sizeof(uint64_t)));
     CK(cudaMemcpyAsync(c->bucket_cursor.p, start.data(), nb * sizeof(uint64_t), cudaMemcpyHostToDevice, c->stream));
     if ((rc = launch_extract<NW>(c, buf, n, has_halo, kc::SCATTER))) return rc;
+    uint32_t ext_err = 0;
+    CK(cudaMemcpyAsync(&ext_err, c->scalars.as<uint32_t>() + 12, sizeof(uint32_t), cudaMemcpyDeviceToHost, c->stream));
 
     launch_count<NW>(c, kb, 1);
     CK(cudaGetLastError());
     if ((rc = rehash_loop<NW>(c, kb))) return rc;
 
     // first occurrences -> packed low.bin bytes
-    if ((rc = device_scan<uint32_t, uint64_t>(c, c->tile_low.as<uint32_t>(), ctiles,
+    if ((rc = device_scan<uint32_t, uint64_t>(c, c->tile_low.as<uint32_t>(), nsegs,
                                               c->tile_low_prefix.as<uint64_t>(), 0, d_scal + 1)))
         return rc;
     uint64_t nlow = 0;
     CK(cudaMemcpyAsync(&nlow, d_scal + 1, sizeof(uint64_t), cudaMemcpyDeviceToHost, c->stream));
     CK(cudaStreamSynchronize(c->stream));
+    if (ext_err) return fail(KC_ERR_DEVICE, "internal error: routing bucket disagreed with its reservation");
     CK(c->low_packed.grow_keep((c->low_total + nlow) * c->packed_bytes + 64, c->low_total * c->packed_bytes,
                                c->stream));
-    kc::pack_low<NW><<<std::min<uint64_t>(ctiles, 148 * 16), 256, 0, c->stream>>>(
-        c->routed.p, c->tile_low.as<uint32_t>(), c->tile_low_prefix.as<uint64_t>(), ctiles, CT, c->cfg.k,
+    Stage st(c, KC_STAGE_PACK_LOW);
+    kc::pack_low<NW><<<std::min<uint64_t>(ceil_div(nsegs, 8), 148 * 16), 256, 0, c->stream>>>(
+        c->routed.p, c->tile_low.as<uint32_t>(), c->tile_low_prefix.as<uint64_t>(), nsegs, c->cfg.k,
         c->low_packed.as<uint8_t>(), c->low_total);
     CK(cudaGetLastError());
     c->low_total += nlow;
@@ -412,6 +469,7 @@ int export_tables(kc_context* c) {
     CK(cudaMemsetAsync(c->root_count.p, 0, 257 * sizeof(uint64_t), c->stream));
     unsigned long long* rc_d = c->root_count.as<unsigned long long>();
     const uint64_t grid = std::min<uint64_t>(ch.size(), 148 * 16);
+    Stage st1(c, KC_STAGE_EXPORT);
     kc::export_count<NW><<<grid, 256, 0, c->stream>>>(c->table.p, c->chunks.as<kc::ExportChunk>(), ch.size(),
                                                       c->cfg.min_count, c->cfg.max_count, rc_d, rc_d + 256);
     CK(cudaGetLastError());
@@ -428,6 +486,7 @@ int export_tables(kc_context* c) {
     c->table_keys = h[256];
     CK(c->roots.ensure(std::max<uint64_t>(tot, 1) * c->record_bytes));
     CK(cudaMemcpyAsync(c->root_cursor.p, start, sizeof start, cudaMemcpyHostToDevice, c->stream));
+    Stage st2(c, KC_STAGE_EXPORT);
     kc::export_write<NW><<<grid, 256, 0, c->stream>>>(c->table.p, c->chunks.as<kc::ExportChunk>(), ch.size(),
                                                       c->cfg.min_count, c->cfg.max_count,
                                                       c->root_cursor.as<unsigned long long>(), c->roots.as<uint8_t>());
@@ -449,7 +508,21 @@ int begin_run(kc_context* c, uint64_t total_bytes) {
     c->sized = false;
     c->have_result = false;
     c->expected_total_bytes = total_bytes;
+    c->ev_used = 0;
+    c->spans.clear();
+    std::memset(c->launches, 0, sizeof c->launches);
+    std::memset(c->stage_ms, 0, sizeof c->stage_ms);
     return KC_OK;
+}
+
+// After the final synchronize: fold event spans into per-stage totals.
+void collect_stage_times(kc_context* c) {
+    for (auto& sp : c->spans) {
+        float ms = 0;
+        if (cudaEventElapsedTime(&ms, sp.second.first, sp.second.second) == cudaSuccess) c->stage_ms[sp.first] += ms;
+    }
+    c->spans.clear();
+    c->ev_used = 0;
 }
 
 int finish_run(kc_context* c) {
@@ -462,6 +535,7 @@ int finish_run(kc_context* c) {
     rc = c->nw == 1 ? export_tables<1>(c) : export_tables<2>(c);
     if (rc) return rc;
     if (c->cfg.sort_output) {
+        Stage st(c, KC_STAGE_SORT, 0);
         rc = kc_sort_roots(c->roots.p, c->root_total, c->record_bytes, c->cfg.k, c->root_counts, c->stream);
         if (rc) return fail(rc, "root record sort failed: %s", kc_sort_error());
     }
@@ -570,6 +644,7 @@ void kc_destroy(kc_context* c) {
                       &c->meta,   &c->bloom,     &c->table,     &c->low_packed,   &c->roots,         &c->chunks,
                       &c->root_count, &c->root_cursor};
     for (DevBuf* b : bufs) b->release();
+    for (cudaEvent_t e : c->ev_pool) cudaEventDestroy(e);
     if (c->ev0) cudaEventDestroy(c->ev0);
     if (c->ev1) cudaEventDestroy(c->ev1);
     if (c->stream) cudaStreamDestroy(c->stream);
@@ -577,6 +652,25 @@ void kc_destroy(kc_context* c) {
 }
 
 void* kc_stream(kc_context* c) { return c ? (void*)c->stream : nullptr; }
+
+int kc_set_profiling(kc_context* c, int enable) {
+    if (!c) return fail(KC_ERR_INVALID, "null context");
+    c->profiling = enable != 0;
+    return KC_OK;
+}
+
+int kc_stage_times(kc_context* c, double* ms, uint64_t* launches, int cap) {
+    if (!c) return fail(KC_ERR_INVALID, "null context");
+    for (int i = 0; i < cap && i < KC_STAGE_COUNT; ++i) {
+        if (ms) ms[i] = c->stage_ms[i];
+        if (launches) launches[i] = c->launches[i];
+    }
+    return KC_STAGE_COUNT;
+}
+
+const char* kc_stage_name(int stage) {
+    return stage >= 0 && stage < KC_STAGE_COUNT ? kStageNames[stage] : "";
+}
 
 int kc_count_device(kc_context* c, const uint8_t* d_fastq, uint64_t n, kc_stats* stats) {
     if (!c || (!d_fastq && n)) return fail(KC_ERR_INVALID, "null argument");
@@ -593,6 +687,7 @@ int kc_count_device(kc_context* c, const uint8_t* d_fastq, uint64_t n, kc_stats*
     if ((rc = finish_run(c))) return rc;
     CK(cudaEventRecord(c->ev1, c->stream));
     CK(cudaEventSynchronize(c->ev1));
+    collect_stage_times(c);
     float ms = 0;
     cudaEventElapsedTime(&ms, c->ev0, c->ev1);
     const double wall = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
@@ -630,6 +725,7 @@ int kc_count_host(kc_context* c, const uint8_t* fastq, uint64_t n, kc_stats* sta
     if ((rc = finish_run(c))) return rc;
     CK(cudaEventRecord(c->ev1, c->stream));
     CK(cudaEventSynchronize(c->ev1));
+    collect_stage_times(c);
     float ms = 0;
     cudaEventElapsedTime(&ms, c->ev0, c->ev1);
     const double wall = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();

@@ -21,9 +21,32 @@
 #pragma once
 
 #include <cstdint>
+#include <type_traits>
 #include <cuda_runtime.h>
 
 namespace kc {
+
+#define KC_HD __host__ __device__ __forceinline__
+
+// Bit reversal usable from host code (unit tests) and device code.
+KC_HD uint32_t brev32(uint32_t x) {
+#ifdef __CUDA_ARCH__
+    return __brev(x);
+#else
+    x = ((x >> 1) & 0x55555555u) | ((x & 0x55555555u) << 1);
+    x = ((x >> 2) & 0x33333333u) | ((x & 0x33333333u) << 2);
+    x = ((x >> 4) & 0x0F0F0F0Fu) | ((x & 0x0F0F0F0Fu) << 4);
+    x = ((x >> 8) & 0x00FF00FFu) | ((x & 0x00FF00FFu) << 8);
+    return (x >> 16) | (x << 16);
+#endif
+}
+KC_HD uint64_t brev64(uint64_t x) {
+#ifdef __CUDA_ARCH__
+    return __brevll(x);
+#else
+    return ((uint64_t)brev32((uint32_t)x) << 32) | brev32((uint32_t)(x >> 32));
+#endif
+}
 
 constexpr int EXT_THREADS = 256;                     // extraction CTA
 constexpr int EXT_BPT = 32;                          // bytes per thread
@@ -77,8 +100,8 @@ __device__ __forceinline__ uint64_t hash_key(const Key2& k) {
 }
 
 // Reverse the order of the 32 two-bit bases of a word (base p -> 31-p).
-__device__ __forceinline__ uint64_t rev_bases(uint64_t x) {
-    x = __brevll(x);
+KC_HD uint64_t rev_bases(uint64_t x) {
+    x = brev64(x);
     return ((x >> 1) & 0x5555555555555555ull) | ((x & 0x5555555555555555ull) << 1);
 }
 
@@ -112,12 +135,12 @@ __device__ __forceinline__ uint64_t key_hi(const Key2& k) { return k.w0; }
 // and emits min(F, C) compared word by word (src/GetKmer.h:181-207).  With W
 // as defined here F = rev_bases(W) (left-aligned by the reversal itself) and
 // C = (~W masked to 2k bits) << (64N - 2k).
-__device__ __forceinline__ uint64_t canonical1(uint64_t W, uint32_t k) {
+KC_HD uint64_t canonical1(uint64_t W, uint32_t k) {
     const uint64_t F = rev_bases(W);
     const uint64_t C = (k == 32) ? ~W : ((~W) << (64 - 2 * k));
     return F < C ? F : C;
 }
-__device__ __forceinline__ Key2 canonical2(uint64_t Whi, uint64_t Wlo, uint32_t k) {
+KC_HD Key2 canonical2(uint64_t Whi, uint64_t Wlo, uint32_t k) {
     // F = base-reverse of the 128-bit (Whi:Wlo); the window occupies the low
     // 2k bits so the reversal lands it left-aligned.
     Key2 F{rev_bases(Wlo), rev_bases(Whi)};
@@ -204,20 +227,32 @@ struct Seg {
     uint32_t nls;    // bit j set: byte j is '\n'
 };
 
+// Four bytes at a time: base test by SIMD byte compares, 2-bit code by the
+// ((c >> 1) ^ (c >> 2)) & 3 identity (A=0 C=1 G=2 T/U=3, either case).
 __device__ __forceinline__ Seg classify(const uint32_t (&w)[8], uint64_t valid_bytes) {
     Seg s{0, 0, 0};
 #pragma unroll
     for (int i = 0; i < 8; ++i) {
-#pragma unroll
-        for (int b = 0; b < 4; ++b) {
-            const int j = 4 * i + b;
-            const uint32_t c = (w[i] >> (8 * b)) & 0xFFu;
-            const bool in = (uint64_t)j < valid_bytes;
-            const bool base = in && is_base(c);
-            s.codes = (s.codes << 2) | (base ? base_code(c) : 0u);
-            s.bases |= (base ? 1u : 0u) << j;
-            s.nls |= ((in && c == '\n') ? 1u : 0u) << j;
-        }
+        const uint32_t x = w[i];
+        const uint32_t u = x & 0xDFDFDFDFu;
+        const uint32_t isb = __vcmpeq4(u, 0x41414141u) | __vcmpeq4(u, 0x43434343u) | __vcmpeq4(u, 0x47474747u) |
+                             __vcmpeq4(u, 0x54545454u) | __vcmpeq4(u, 0x55555555u);
+        const uint32_t isn = __vcmpeq4(x, 0x0A0A0A0Au);
+        const uint32_t code4 = ((x >> 1) ^ (x >> 2)) & 0x03030303u;
+        // gather one bit per byte (bit 7 of each compare byte) into 4 bits
+        const uint32_t bm = ((isb >> 7) & 1u) | ((isb >> 14) & 2u) | ((isb >> 21) & 4u) | ((isb >> 28) & 8u);
+        const uint32_t nm = ((isn >> 7) & 1u) | ((isn >> 14) & 2u) | ((isn >> 21) & 4u) | ((isn >> 28) & 8u);
+        s.bases |= bm << (4 * i);
+        s.nls |= nm << (4 * i);
+        // codes of bytes 4i..4i+3 -> 8 bits, byte 4i in the high pair
+        const uint32_t c8 = ((code4 & 3u) << 6) | (((code4 >> 8) & 3u) << 4) | (((code4 >> 16) & 3u) << 2) |
+                            ((code4 >> 24) & 3u);
+        s.codes |= (uint64_t)c8 << (56 - 8 * i);
+    }
+    if (valid_bytes < 32) {
+        const uint32_t keep = valid_bytes ? (0xFFFFFFFFu >> (32 - (uint32_t)valid_bytes)) : 0u;
+        s.bases &= keep;
+        s.nls &= keep;
     }
     return s;
 }
@@ -237,8 +272,60 @@ __device__ __forceinline__ void load32(const uint8_t* p, uint64_t avail, uint32_
     }
 }
 
-// Length of the run of bases at the END of a 32-byte segment.
-__device__ __forceinline__ uint32_t tail_run(uint32_t bases) { return __clz(~bases); }
+typedef unsigned __int128 u128;
+
+// Bit i of the result: bits [i-k+1, i] of X are all set (bits below 0 read
+// as clear).  Shift-AND doubling: R_2m = R_m & (R_m << m), then one
+// overlapping step to reach k exactly.
+__device__ __forceinline__ u128 runs_at_least(u128 X, uint32_t k) {
+    u128 R = X;
+    uint32_t have = 1;
+    while (2 * have <= k) {
+        R &= R << have;
+        have *= 2;
+    }
+    if (have < k) R &= R << (k - have);
+    return R;
+}
+
+// Bits of the 32 bytes that lie on sequence lines (line index = 1 mod 4),
+// line0 = line index of byte 0, nls = newline bits.
+__device__ __forceinline__ uint32_t sequence_mask(uint32_t line0, uint32_t nls) {
+    uint32_t seq = 0, start = 0, line = line0, m = nls;
+    for (;;) {
+        const uint32_t end = m ? (uint32_t)__ffs(m) : 32u;  // bytes [start, end) share `line`
+        if ((line & 3u) == 1u && end > start) {
+            const uint32_t hi = end >= 32 ? 0xFFFFFFFFu : ((1u << end) - 1u);
+            seq |= hi & ~((1u << start) - 1u);
+        }
+        if (!m) break;
+        start = end;
+        m &= m - 1;
+        ++line;
+    }
+    return seq;
+}
+
+// Reverse the order of the nb two-bit bases in the low 2*nb bits of x.
+KC_HD uint32_t rev_small(uint32_t x, uint32_t nb) {
+    uint32_t r = brev32(x);
+    r = ((r >> 1) & 0x55555555u) | ((r & 0x55555555u) << 1);
+    return r >> (32 - 2 * nb);
+}
+
+// Window of the last k bases ending at byte j of segment s2 (segments s0,
+// s1 precede it): low 64 bits and, for k > 32, the next 64 bits.
+KC_HD void window_at(uint64_t s0, uint64_t s1, uint64_t s2, uint32_t j, uint64_t& lo,
+                                          uint64_t& hi) {
+    const uint32_t sh = 2 * (31 - j);  // 0..62
+    if (sh == 0) {
+        lo = s2;
+        hi = s1;
+    } else {
+        lo = (s2 >> sh) | (s1 << (64 - sh));
+        hi = (s1 >> sh) | (s0 << (64 - sh));
+    }
+}
 
 struct ExtractArgs {
     const uint8_t* buf;      // batch start (16-byte aligned)
@@ -251,7 +338,30 @@ struct ExtractArgs {
     unsigned long long* bucket_count;  // HIST: per-bucket totals (accumulated)
     unsigned long long* bucket_cursor; // SCATTER: next free index per bucket
     void* routed;            // SCATTER: routed key array
+    uint32_t* error;         // set when a key's bucket disagrees with its reservation
 };
+
+// Bucket of the canonical key of window (hi:lo) without building the key:
+// the top B bits of min(F, C) equal min(top B bits of F, top B bits of C).
+// top(F) = the newest B/2 bases reversed; top(C) = the oldest B/2 bases
+// complemented.
+KC_HD uint32_t bucket_of_window(uint64_t lo, uint64_t hi, uint32_t k, uint32_t B) {
+    const uint32_t nb = B / 2;
+    const uint32_t mask = (1u << B) - 1u;
+    const uint32_t topF = k >= nb ? rev_small((uint32_t)lo & mask, nb) : (rev_small((uint32_t)lo & ((1u << (2 * k)) - 1u), k) << (B - 2 * k));
+    uint32_t topC;
+    const uint32_t lo_bit = 2 * k >= B ? 2 * k - B : 0;  // lowest bit of the oldest B/2 bases
+    if (2 * k < B) {
+        topC = ((~(uint32_t)lo) & ((1u << (2 * k)) - 1u)) << (B - 2 * k);
+    } else if (lo_bit + B <= 64) {
+        topC = (uint32_t)(~lo >> lo_bit) & mask;
+    } else if (lo_bit >= 64) {
+        topC = (uint32_t)(~hi >> (lo_bit - 64)) & mask;
+    } else {
+        topC = (uint32_t)(((~lo) >> lo_bit) | ((~hi) << (64 - lo_bit))) & mask;
+    }
+    return topF < topC ? topF : topC;
+}
 
 // Canonical k-mer extraction over one 8 KiB tile per CTA.
 //
@@ -261,131 +371,130 @@ struct ExtractArgs {
 // the file) and the k bytes ending at p are all bases.  A window never
 // crosses '\n' because '\n' is not a base, so only p's line matters.
 //
-// Each thread owns 32 consecutive bytes.  The k-1 <= 63 bases before its
-// first byte come from the two preceding segments, passed by warp shuffles
-// (smem for lanes 0/1, whose predecessors sit in the previous warp or, for
-// warp 0, in the 64-byte halo before the tile).
+// Phase A, per thread (32 bytes): classify, then a bit-parallel emit mask:
+//   run of >= k bases ending at byte j (shift-AND doubling over the bases
+//   of this and the two preceding segments) AND byte j on a sequence line.
+// Phase C, per position: round r covers bytes [256r, 256r+256) of the tile,
+//   so a warp owns one 32-byte segment per round -- warps over quality and
+//   header bytes skip uniformly.  The window comes from the segment's codes
+//   and its two predecessors (shared memory; the two before the tile are the
+//   64-byte halo).
+// HIST: per-bucket totals via the bucket-only path.  SCATTER: bucket-only
+// histogram, one reservation per bucket per CTA, then full keys written to
+// routed[base[bucket] + rank].
 template <int NW, int MODE>
 __global__ void __launch_bounds__(EXT_THREADS) extract_kernel(ExtractArgs a) {
     // dynamic smem: u64 base[n_buckets] | u32 hist[n_buckets] | u32 fill[n_buckets]
     extern __shared__ unsigned long long ext_smem[];
-    __shared__ uint64_t tail_codes[EXT_THREADS / 32 + 1][2];
-    __shared__ uint32_t tail_bases[EXT_THREADS / 32 + 1][2];
+    __shared__ uint64_t seg_codes[EXT_THREADS + 2];
+    __shared__ uint32_t seg_bases[EXT_THREADS + 2];
+    __shared__ uint32_t seg_emit[EXT_THREADS];
     __shared__ uint32_t warp_sums[EXT_THREADS / 32];
+    __shared__ uint32_t tile_any;
     unsigned long long* bbase = ext_smem;
     uint32_t* hist = reinterpret_cast<uint32_t*>(ext_smem + a.n_buckets);
     uint32_t* fill = hist + a.n_buckets;
 
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int tid = threadIdx.x;
     const uint64_t tile_start = (uint64_t)blockIdx.x * EXT_TILE;
     const uint64_t seg_start = tile_start + (uint64_t)tid * EXT_BPT;
+    const uint32_t k = a.k;
+    const uint32_t B = 64 - a.bucket_shift;
 
     for (uint32_t b = tid; b < a.n_buckets; b += EXT_THREADS) {
         hist[b] = 0;
-        if (MODE == SCATTER) fill[b] = 0;
+        fill[b] = 0;
     }
+    if (tid == 0) tile_any = 0;
 
+    // ---- phase A: classify own segment (+ the two halo segments)
     uint32_t w[8];
     const uint64_t valid = seg_start < a.n ? a.n - seg_start : 0;
     load32(a.buf + seg_start, valid, w);
     const Seg s = classify(w, valid);
-
-    // Halo segments before the tile (before a batch start they are
-    // buf[-HALO..-1] when has_halo, else no bases); only their bases matter,
-    // a window that reaches them cannot contain a '\n'.
-    if (warp == 0 && lane < 2) {
+    seg_codes[tid + 2] = s.codes;
+    seg_bases[tid + 2] = s.bases;
+    if (tid < 2) {
         uint32_t hw[8];
         const bool readable = tile_start > 0 || a.has_halo;
-        load32(a.buf + (int64_t)tile_start - HALO + 32 * lane, readable ? 32 : 0, hw);
+        load32(a.buf + (int64_t)tile_start - HALO + 32 * tid, readable ? 32 : 0, hw);
         const Seg h = classify(hw, readable ? 32 : 0);
-        tail_codes[0][lane] = h.codes;
-        tail_bases[0][lane] = h.bases;
+        seg_codes[tid] = h.codes;
+        seg_bases[tid] = h.bases;
     }
-    if (lane >= 30) {
-        tail_codes[warp + 1][lane - 30] = s.codes;
-        tail_bases[warp + 1][lane - 30] = s.bases;
-    }
-    // line index at this thread's first byte
     uint32_t nl_total;
     const uint32_t nl_before = block_exclusive_scan<EXT_THREADS>(__popc(s.nls), warp_sums, &nl_total);
-    (void)nl_total;  // block_exclusive_scan synchronised: tails are visible
+    (void)nl_total;  // the scan synchronised the block: seg_* are visible
     const uint32_t line0 = (uint32_t)a.tile_line[blockIdx.x] + nl_before;
 
-    uint64_t p1c = __shfl_up_sync(0xffffffffu, s.codes, 1);
-    uint64_t p2c = __shfl_up_sync(0xffffffffu, s.codes, 2);
-    uint32_t p1b = __shfl_up_sync(0xffffffffu, s.bases, 1);
-    uint32_t p2b = __shfl_up_sync(0xffffffffu, s.bases, 2);
-    if (lane == 0) {
-        p1c = tail_codes[warp][1];
-        p1b = tail_bases[warp][1];
-        p2c = tail_codes[warp][0];
-        p2b = tail_bases[warp][0];
-    } else if (lane == 1) {
-        p2c = tail_codes[warp][1];
-        p2b = tail_bases[warp][1];
+    uint32_t emit = 0;
+    if (s.bases) {
+        const uint32_t seq = sequence_mask(line0, s.nls);
+        if (seq & s.bases) {
+            const u128 X = ((u128)s.bases << 64) | ((u128)seg_bases[tid + 1] << 32) | (u128)seg_bases[tid];
+            emit = (uint32_t)(runs_at_least(X, k) >> 64) & seq;
+        }
+    }
+    seg_emit[tid] = emit;
+    if (emit) tile_any = 1;
+    __syncthreads();
+    if (!tile_any) {
+        return;  // nothing to count in this tile (HIST adds nothing; SCATTER reserves nothing)
     }
 
-    // Does this segment touch a sequence line at all?  Lines inside the
-    // segment are line0, line0+1, ...; a sequence line is = 1 (mod 4).
-    const uint32_t nls = __popc(s.nls);
-    bool any_seq = false;
-#pragma unroll
-    for (uint32_t d = 0; d < 4; ++d) any_seq |= (d <= nls) && (((line0 + d) & 3u) == 1u);
-    any_seq &= (s.bases != 0);
-
-    const uint32_t k = a.k;
-    const uint64_t kmask1 = (k >= 32) ? ~0ull : ((1ull << (2 * k)) - 1ull);
-
-    // Two passes in SCATTER mode: histogram, reservation, then placement.
+    // ---- phase C
+    const int lane = tid & 31;
+    const int warp = tid >> 5;
 #pragma unroll 1
     for (int pass = 0; pass < (MODE == SCATTER ? 2 : 1); ++pass) {
         if (pass == 1) {
-            __syncthreads();
             for (uint32_t b = tid; b < a.n_buckets; b += EXT_THREADS) {
                 const uint32_t c = hist[b];
-                fill[b] = 0;
                 bbase[b] = c ? atomicAdd(a.bucket_cursor + b, (unsigned long long)c) : 0ull;
             }
             __syncthreads();
         }
-        if (any_seq) {
-            uint64_t win_lo = p1c, win_hi = p2c;  // the 64 bases before byte 0
-            uint32_t run = tail_run(p1b);
-            if (run == 32) run += tail_run(p2b);
-            uint32_t line = line0;
-#pragma unroll 4
-            for (int j = 0; j < 32; ++j) {
-                const uint32_t code = (uint32_t)(s.codes >> (62 - 2 * j)) & 3u;
-                const bool base = (s.bases >> j) & 1u;
-                win_hi = (win_hi << 2) | (win_lo >> 62);
-                win_lo = (win_lo << 2) | code;
-                run = base ? run + 1 : 0;
-                if (base && run >= k && (line & 3u) == 1u) {
-                    uint32_t bucket;
-                    typename KeyOf<NW>::T key;
-                    if constexpr (NW == 1) {
-                        key = canonical1(win_lo & kmask1, k);
-                        bucket = (uint32_t)(key >> a.bucket_shift);
-                    } else {
-                        const uint32_t hb = 2 * k - 64;  // bits of the window in win_hi
-                        const uint64_t hmask = hb >= 64 ? ~0ull : ((1ull << hb) - 1ull);
-                        key = canonical2(win_hi & hmask, win_lo, k);
-                        bucket = (uint32_t)(key.w0 >> a.bucket_shift);
-                    }
-                    if (MODE == HIST || pass == 0) {
-                        atomicAdd(hist + bucket, 1u);
-                    } else {
-                        const uint32_t r = atomicAdd(fill + bucket, 1u);
-                        typename KeyOf<NW>::T* out = reinterpret_cast<typename KeyOf<NW>::T*>(a.routed);
-                        out[bbase[bucket] + r] = key;
-                    }
+#pragma unroll 1
+        for (int r = 0; r < EXT_BPT; ++r) {
+            const int t = r * (EXT_THREADS / 32) + warp;  // segment owned by this warp this round
+            const uint32_t em = seg_emit[t];
+            if (!em) continue;  // warp-uniform
+            if (!((em >> lane) & 1u)) continue;
+            uint64_t lo, hi;
+            window_at(seg_codes[t], seg_codes[t + 1], seg_codes[t + 2], (uint32_t)lane, lo, hi);
+            if (pass == 0) {
+                if (NW == 1) {
+                    const uint64_t km = k >= 32 ? ~0ull : ((1ull << (2 * k)) - 1ull);
+                    lo &= km;
+                } else {
+                    const uint32_t hb = 2 * k - 64;
+                    hi &= hb >= 64 ? ~0ull : ((1ull << hb) - 1ull);
                 }
-                if ((s.nls >> j) & 1u) ++line;
+                atomicAdd(hist + bucket_of_window(lo, hi, k, B), 1u);
+            } else {
+                typename KeyOf<NW>::T key;
+                uint32_t bucket;
+                if constexpr (NW == 1) {
+                    const uint64_t km = k >= 32 ? ~0ull : ((1ull << (2 * k)) - 1ull);
+                    key = canonical1(lo & km, k);
+                    bucket = (uint32_t)(key >> a.bucket_shift);
+                } else {
+                    const uint32_t hb = 2 * k - 64;
+                    const uint64_t hmask = hb >= 64 ? ~0ull : ((1ull << hb) - 1ull);
+                    key = canonical2(hi & hmask, lo, k);
+                    bucket = (uint32_t)(key.w0 >> a.bucket_shift);
+                }
+                const uint32_t rnk = atomicAdd(fill + bucket, 1u);
+                if (rnk < hist[bucket]) {
+                    reinterpret_cast<typename KeyOf<NW>::T*>(a.routed)[bbase[bucket] + rnk] = key;
+                } else {
+                    atomicOr(a.error, 1u);  // never write outside the reservation
+                }
             }
         }
+        __syncthreads();
     }
     if (MODE == HIST) {
-        __syncthreads();
         for (uint32_t b = tid; b < a.n_buckets; b += EXT_THREADS) {
             const uint32_t c = hist[b];
             if (c) atomicAdd(a.bucket_count + b, (unsigned long long)c);
@@ -403,14 +512,16 @@ __device__ __forceinline__ uint64_t bloom_bits(uint64_t h) {
     return (1ull << ((h >> 40) & 63)) | (1ull << ((h >> 46) & 63)) | (1ull << ((h >> 52) & 63));
 }
 
-// Insert `add` occurrences of key into a bucket table; false = probe limit hit.
+// Insert `add` occurrences of key into a bucket table; false = probe limit
+// hit.  `seen` is the key word already read from the first probe slot (or
+// EMPTY-1 when none was read), which saves the first load.
 __device__ __forceinline__ bool table_add(Slot1* __restrict__ tab, uint64_t mask, uint64_t h, uint64_t key,
-                                          uint32_t add) {
+                                          uint32_t add, const uint64_t* seen = nullptr) {
     uint64_t i = (h >> 17) & mask;
     const int limit = (int)min((uint64_t)PROBE_LIMIT, mask + 1);
     for (int p = 0; p < limit; ++p) {
         Slot1* s = tab + ((i + p) & mask);
-        uint64_t cur = __ldcg(&s->key);
+        uint64_t cur = (p == 0 && seen) ? *seen : __ldcg(&s->key);
         if (cur == EMPTY) {
             cur = atomicCAS(reinterpret_cast<unsigned long long*>(&s->key), EMPTY, key);
             if (cur == EMPTY) cur = key;
@@ -424,12 +535,12 @@ __device__ __forceinline__ bool table_add(Slot1* __restrict__ tab, uint64_t mask
 }
 
 __device__ __forceinline__ bool table_add(Slot2* __restrict__ tab, uint64_t mask, uint64_t h, const Key2& key,
-                                          uint32_t add) {
+                                          uint32_t add, const ulonglong2* seen = nullptr) {
     uint64_t i = (h >> 17) & mask;
     const int limit = (int)min((uint64_t)PROBE_LIMIT, mask + 1);
     for (int p = 0; p < limit; ++p) {
         Slot2* s = tab + ((i + p) & mask);
-        const ulonglong2 v = __ldcg(reinterpret_cast<const ulonglong2*>(s));
+        const ulonglong2 v = (p == 0 && seen) ? *seen : __ldcg(reinterpret_cast<const ulonglong2*>(s));
         bool mine = (v.x == key.w0 && v.y == key.w1);
         // A slot goes EMPTY -> key exactly once.  A 16-byte read that shows an
         // EMPTY half may be torn, so ask the CAS for the authoritative value.
@@ -463,7 +574,12 @@ struct SlotOf<2> {
 
 template <int NW>
 __host__ __device__ constexpr int count_items() {
-    return NW == 1 ? 16 : 8;
+    return NW == 1 ? 4 : 2;
+}
+// Keys owned by one warp of the count kernel (a contiguous segment).
+template <int NW>
+__host__ __device__ constexpr int count_seg() {
+    return 32 * count_items<NW>();
 }
 template <int NW>
 __host__ __device__ constexpr int count_tile() {
@@ -476,131 +592,164 @@ struct CountArgs {
     const BucketMeta* meta;
     uint64_t* bloom;
     void* table;
-    uint32_t* tile_low;           // first occurrences kept at the tile front
-    uint32_t* tile_fail;          // overflowed keys kept at the tile back
+    uint32_t* seg_low;            // per warp segment: first occurrences kept at its front
+    uint32_t* seg_fail;           // per warp segment: overflowed keys kept at its back
     uint32_t* bucket_overflow;    // set to 1 for a bucket whose table overflowed
     uint32_t bucket_shift;
     int use_filter;               // 0: retry pass (table only, no filter)
 };
 
-// One tile of routed keys per CTA: for each key, the first-occurrence filter
-// decides low.bin (first) or the repeat table (seen before), as the
-// reference's classifier does with ConcurrentBloomFilter::insert
-// (src/FastqClassifier.h:241-349, src/BloomFilter.h:207-234): a relaxed read
-// first, then fetch_or; "first" = the old word lacked one of the bits.
-// Repeats increment the bucket's open-addressing table (replaces KmerTree +
-// ConcurrentMap::increment, src/NewKmerTree.h:383-489,
-// src/ConcurrentMap.h:112-160).
+// For each routed key: the first-occurrence filter decides low.bin (first)
+// or the repeat table (seen before), as the reference's classifier does with
+// ConcurrentBloomFilter::insert (src/FastqClassifier.h:241-349,
+// src/BloomFilter.h:207-234): a relaxed read first, then fetch_or; "first" =
+// the old word lacked one of the bits.  Repeats increment the bucket's
+// open-addressing table (replaces KmerTree + ConcurrentMap::increment,
+// src/NewKmerTree.h:383-489, src/ConcurrentMap.h:112-160).
 //
-// Equal keys inside a warp are merged first (__match_any_sync): one filter
-// probe and one table add per distinct key per warp.
+// Each warp owns a contiguous segment of count_seg<NW>() keys.  The work is
+// staged so that every lane has all its items' memory requests in flight at
+// once (filter reads, then filter atomics, then first table probes) instead
+// of one dependent chain per item.  Equal keys inside a warp are merged first
+// (__match_any_sync): one filter probe and one table add per distinct key.
 //
-// Outputs are compacted IN PLACE into the tile's own range of the routed
-// array, after every key of the tile is in registers: first occurrences at
-// the front, keys that met a full table at the back (for the retry pass).
+// Outputs are compacted IN PLACE into the warp's own segment (only this warp
+// reads it, so __syncwarp orders the reads before the writes): first
+// occurrences at the front, keys that met a full table at the back.
 template <int NW>
-__global__ void __launch_bounds__(CNT_THREADS) count_routed(CountArgs a) {
+__global__ void __launch_bounds__(CNT_THREADS, 4) count_routed(CountArgs a) {
     using K = typename KeyOf<NW>::T;
     using S = typename SlotOf<NW>::T;
     constexpr int ITEMS = count_items<NW>();
-    constexpr int TILE = count_tile<NW>();
-    __shared__ uint32_t s_low, s_fail;
+    constexpr int SEG = count_seg<NW>();
 
     K* keys = reinterpret_cast<K*>(a.routed);
-    const uint64_t t0 = (uint64_t)blockIdx.x * TILE;
-    const uint64_t t_end = min(a.n_keys, t0 + TILE);
-    uint64_t base = t0;
-    uint32_t n_in = (uint32_t)(t_end - t0);
+    const int lane = threadIdx.x & 31;
+    const uint64_t gw = (uint64_t)blockIdx.x * (CNT_THREADS / 32) + (threadIdx.x >> 5);
+    const uint64_t s0 = gw * SEG;
+    if (s0 >= a.n_keys) return;
+    const uint64_t s_end = min(a.n_keys, s0 + SEG);
+    uint64_t base = s0;
+    uint32_t n_in = (uint32_t)(s_end - s0);
     if (!a.use_filter) {
-        // retry pass: only the overflowed keys at the back of the tile
-        const uint32_t nf = a.tile_fail[blockIdx.x];
+        const uint32_t nf = a.seg_fail[gw];
         if (nf == 0) return;
-        base = t_end - nf;
+        base = s_end - nf;
         n_in = nf;
     }
-    const int tid = threadIdx.x, lane = tid & 31;
-    if (tid == 0) {
-        s_low = 0;
-        s_fail = 0;
-    }
-    K item[ITEMS];
-#pragma unroll
-    for (int j = 0; j < ITEMS; ++j) {
-        const uint32_t idx = (uint32_t)(j * CNT_THREADS + tid);
-        if (idx < n_in) item[j] = keys[base + idx];
-    }
-    __syncthreads();  // every read of the tile precedes any in-place write
 
-    const uint32_t fail_base_tile = (uint32_t)(t_end - t0);  // fail slots grow down from t_end
+    K it[ITEMS];
+    uint32_t mult[ITEMS];
 #pragma unroll
     for (int j = 0; j < ITEMS; ++j) {
-        const uint32_t idx = (uint32_t)(j * CNT_THREADS + tid);
-        const bool valid = idx < n_in;
-        const uint32_t active = __ballot_sync(0xffffffffu, valid);
-        if (!active) break;
-        bool first = false;
-        uint32_t fails = 0;
-        K key = item[j];
-        if (valid) {
+        const uint32_t idx = (uint32_t)(j * 32 + lane);
+        mult[j] = idx < n_in ? 1u : 0u;
+        if (mult[j]) it[j] = keys[base + idx];
+    }
+    __syncwarp();  // every read of the segment precedes any in-place write
+
+    // merge equal keys inside the warp: the lowest lane carries the multiplicity
+#pragma unroll
+    for (int j = 0; j < ITEMS; ++j) {
+        const uint32_t active = __ballot_sync(0xffffffffu, mult[j] != 0);
+        if (mult[j]) {
             uint32_t same;
-            if constexpr (NW == 1) {
-                same = __match_any_sync(active, key);
-            } else {
-                same = __match_any_sync(active, key.w0) & __match_any_sync(active, key.w1);
-            }
-            const bool leader = (__ffs(same) - 1) == lane;
-            if (leader) {
-                const uint32_t mult = __popc(same);
-                const uint32_t b = (uint32_t)(key_hi(key) >> a.bucket_shift);
-                const BucketMeta m = a.meta[b];
-                const uint64_t h = hash_key(key);
-                uint32_t reps = mult;
-                if (a.use_filter) {
-                    uint64_t* word = a.bloom + m.bloom_off + (h & m.bloom_mask);
-                    const uint64_t bits = bloom_bits(h);
-                    uint64_t old = __ldcg(word);
-                    if ((old & bits) != bits) old = atomicOr(reinterpret_cast<unsigned long long*>(word), bits);
-                    first = (old & bits) != bits;
-                    reps -= first ? 1u : 0u;
-                }
-                if (reps) {
-                    S* tab = reinterpret_cast<S*>(a.table) + m.tab_off;
-                    if (!table_add(tab, m.tab_mask, h, key, reps)) {
-                        fails = reps;
-                        a.bucket_overflow[b] = 1u;
-                    }
-                }
-            }
-        } else {
-            // inactive lanes still take part in the warp-wide compaction below
+            if constexpr (NW == 1) same = __match_any_sync(active, it[j]);
+            else same = __match_any_sync(active, it[j].w0) & __match_any_sync(active, it[j].w1);
+            mult[j] = ((__ffs(same) - 1) == lane) ? (uint32_t)__popc(same) : 0u;
         }
-        // warp-aggregated reservations in the tile's low / fail regions
-        const uint32_t lowmask = __ballot_sync(0xffffffffu, first);
-        uint32_t low_base = 0;
-        if (lowmask) {
-            if (lane == 0) low_base = atomicAdd(&s_low, __popc(lowmask));
-            low_base = __shfl_sync(0xffffffffu, low_base, 0);
-            if (first) keys[t0 + low_base + __popc(lowmask & ((1u << lane) - 1u))] = key;
+    }
+
+    uint64_t h[ITEMS];
+    uint32_t bucket[ITEMS];
+    uint32_t first_bits = 0;  // bit j: item j is a first occurrence
+    if (a.use_filter) {
+        uint64_t* word[ITEMS];
+        uint64_t old[ITEMS];
+#pragma unroll
+        for (int j = 0; j < ITEMS; ++j) {
+            if (mult[j]) {
+                bucket[j] = (uint32_t)(key_hi(it[j]) >> a.bucket_shift);
+                h[j] = hash_key(it[j]);
+                const uint64_t off = __ldg(&a.meta[bucket[j]].bloom_off), msk = __ldg(&a.meta[bucket[j]].bloom_mask);
+                word[j] = a.bloom + off + (h[j] & msk);
+                old[j] = __ldcg(word[j]);
+            }
         }
-        uint32_t fsum = fails;
+#pragma unroll
+        for (int j = 0; j < ITEMS; ++j) {
+            if (mult[j]) {
+                const uint64_t bits = bloom_bits(h[j]);
+                if ((old[j] & bits) != bits) {
+                    old[j] = atomicOr(reinterpret_cast<unsigned long long*>(word[j]), bits);
+                    if ((old[j] & bits) != bits) first_bits |= 1u << j;
+                }
+            }
+        }
+    } else {
+#pragma unroll
+        for (int j = 0; j < ITEMS; ++j) {
+            if (mult[j]) {
+                bucket[j] = (uint32_t)(key_hi(it[j]) >> a.bucket_shift);
+                h[j] = hash_key(it[j]);
+            }
+        }
+    }
+
+    // repeat occurrences -> tables: all first-probe reads in flight, then resolve
+    using Seen = typename std::conditional<NW == 1, uint64_t, ulonglong2>::type;
+    Seen seen[ITEMS];
+    S* tabp[ITEMS];
+    uint64_t tmask[ITEMS];
+#pragma unroll
+    for (int j = 0; j < ITEMS; ++j) {
+        const uint32_t reps = mult[j] - ((first_bits >> j) & 1u);
+        if (mult[j] && reps) {
+            tabp[j] = reinterpret_cast<S*>(a.table) + __ldg(&a.meta[bucket[j]].tab_off);
+            tmask[j] = __ldg(&a.meta[bucket[j]].tab_mask);
+            const S* slot = tabp[j] + ((h[j] >> 17) & tmask[j]);
+            if constexpr (NW == 1) seen[j] = __ldcg(&slot->key);
+            else seen[j] = __ldcg(reinterpret_cast<const ulonglong2*>(slot));
+        }
+    }
+    uint32_t fails[ITEMS];
+#pragma unroll
+    for (int j = 0; j < ITEMS; ++j) {
+        fails[j] = 0;
+        const uint32_t reps = mult[j] - ((first_bits >> j) & 1u);
+        if (mult[j] && reps) {
+            if (!table_add(tabp[j], tmask[j], h[j], it[j], reps, &seen[j])) {
+                fails[j] = reps;
+                a.bucket_overflow[bucket[j]] = 1u;
+            }
+        }
+    }
+
+    // in-place compaction inside the warp's segment
+    uint32_t n_low = 0, n_fail = 0;
+    const uint32_t lt = (1u << lane) - 1u;
+#pragma unroll
+    for (int j = 0; j < ITEMS; ++j) {
+        const bool first = (first_bits >> j) & 1u;
+        const uint32_t lm = __ballot_sync(0xffffffffu, first);
+        if (first) keys[s0 + n_low + __popc(lm & lt)] = it[j];
+        n_low += __popc(lm);
+        uint32_t fsum = fails[j];
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
             const uint32_t y = __shfl_up_sync(0xffffffffu, fsum, o);
             if (lane >= o) fsum += y;
         }
-        const uint32_t wtotal = __shfl_sync(0xffffffffu, fsum, 31);
-        if (wtotal) {
-            uint32_t fb = 0;
-            if (lane == 0) fb = atomicAdd(&s_fail, wtotal);
-            fb = __shfl_sync(0xffffffffu, fb, 0);
-            const uint32_t my0 = fb + fsum - fails;
-            for (uint32_t r = 0; r < fails; ++r) keys[t0 + fail_base_tile - 1 - (my0 + r)] = key;
+        const uint32_t wtot = __shfl_sync(0xffffffffu, fsum, 31);
+        if (wtot) {
+            const uint32_t my0 = n_fail + fsum - fails[j];
+            for (uint32_t r = 0; r < fails[j]; ++r) keys[s_end - 1 - (my0 + r)] = it[j];
+            n_fail += wtot;
         }
     }
-    __syncthreads();
-    if (tid == 0) {
-        if (a.use_filter) a.tile_low[blockIdx.x] = s_low;
-        a.tile_fail[blockIdx.x] = s_fail;
+    if (lane == 0) {
+        if (a.use_filter) a.seg_low[gw] = n_low;
+        a.seg_fail[gw] = n_fail;
     }
 }
 
@@ -652,42 +801,42 @@ __global__ void init_slots(void* tab, uint64_t n) {
 // little-endian u64, then the top ceil(2(k%32)/8) bytes of the tail word
 // (masked to its 2(k%32) high bits), in little-endian byte order.
 template <int NW>
-__global__ void pack_low(const void* routed, const uint32_t* tile_low, const uint64_t* tile_low_prefix,
-                         uint64_t n_tiles, uint32_t tile_keys, uint32_t k, uint8_t* out, uint64_t out_base) {
+__global__ void pack_low(const void* routed, const uint32_t* seg_low, const uint64_t* seg_low_prefix, uint64_t n_segs,
+                         uint32_t k, uint8_t* out, uint64_t out_base) {
     using K = typename KeyOf<NW>::T;
+    constexpr int SEG = count_seg<NW>();
     const K* keys = reinterpret_cast<const K*>(routed);
     const uint32_t full = k / 32, tail_bits = 2 * (k % 32), tail_bytes = (tail_bits + 7) / 8;
     const uint32_t P = full * 8 + tail_bytes;
     const uint64_t tmask = tail_bits ? (~0ull << (64 - tail_bits)) : 0ull;
-    for (uint64_t t = blockIdx.x; t < n_tiles; t += gridDim.x) {
-        const uint32_t n = tile_low[t];
-        const uint64_t o = out_base + tile_low_prefix[t];
-        for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
-            const K key = keys[t * (uint64_t)tile_keys + i];
-            uint64_t w[2];
+    const int lane = threadIdx.x & 31;
+    const uint64_t warps = (uint64_t)gridDim.x * (blockDim.x >> 5);
+    for (uint64_t sg = (uint64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); sg < n_segs; sg += warps) {
+        const uint32_t n = seg_low[sg];
+        const uint64_t o = out_base + seg_low_prefix[sg];
+        for (uint32_t i = lane; i < n; i += 32) {
+            const K key = keys[sg * (uint64_t)SEG + i];
+            uint64_t w0, w1;
             if constexpr (NW == 1) {
-                w[0] = key;
-                w[1] = 0;
+                w0 = key;
+                w1 = 0;
             } else {
-                w[0] = key.w0;
-                w[1] = key.w1;
+                w0 = key.w0;
+                w1 = key.w1;
             }
             uint8_t* d = out + (o + i) * P;
-            if (P == 8 && full == 0) {
-                *reinterpret_cast<uint64_t*>(d) = w[0] & tmask;
-            } else if (P == 8) {
-                *reinterpret_cast<uint64_t*>(d) = w[0];
+            if (P == 8) {
+                *reinterpret_cast<uint64_t*>(d) = full ? w0 : (w0 & tmask);
             } else if (P == 16) {
-                reinterpret_cast<uint64_t*>(d)[0] = w[0];
-                reinterpret_cast<uint64_t*>(d)[1] = full == 2 ? w[1] : (w[1] & tmask);
+                reinterpret_cast<uint64_t*>(d)[0] = w0;
+                reinterpret_cast<uint64_t*>(d)[1] = full == 2 ? w1 : (w1 & tmask);
             } else {
                 uint32_t q = 0;
-                for (uint32_t f = 0; f < full; ++f)
-                    for (uint32_t b = 0; b < 8; ++b) d[q++] = (uint8_t)(w[f] >> (8 * b));
-                if (tail_bytes) {
-                    const uint64_t tw = w[full] & tmask;
-                    for (uint32_t b = 8 - tail_bytes; b < 8; ++b) d[q++] = (uint8_t)(tw >> (8 * b));
+                if (full) {
+                    for (uint32_t b = 0; b < 8; ++b) d[q++] = (uint8_t)(w0 >> (8 * b));
                 }
+                const uint64_t tw = (full ? w1 : w0) & tmask;
+                for (uint32_t b = 8 - tail_bytes; b < 8; ++b) d[q++] = (uint8_t)(tw >> (8 * b));
             }
         }
     }

@@ -1,0 +1,90 @@
+// Host-side unit test of the extraction helpers in kc_kernels.cuh
+// (compiled by tests/test_kernel_helpers.py; runs on the CPU).
+//
+// For random base strings and every k in 1..64 and bucket widths 8/12 bits:
+//   * window_at() returns exactly the last k bases ending at byte j,
+//   * canonical1/canonical2 equal min(F, C) built from the definition in the
+//     reference (src/GetKmer.h:58-82, :181-207): F = bases in reverse order,
+//     C = complemented bases in read order, both left-aligned,
+//   * bucket_of_window() equals the top bits of that canonical key.
+#include <cstdio>
+#include <cstdint>
+#include <cstdlib>
+#include <random>
+#include <vector>
+
+#include "../../kmertreecounter_b200/csrc/kc_kernels.cuh"
+
+using namespace kc;
+
+static void pack_left(const std::vector<int>& b, uint64_t out[2]) {
+    out[0] = out[1] = 0;
+    for (size_t i = 0; i < b.size(); ++i) {
+        const int w = (int)(i / 32), pos = 62 - 2 * (int)(i % 32);
+        out[w] |= (uint64_t)b[i] << pos;
+    }
+}
+
+int main() {
+    std::mt19937_64 rng(12345);
+    long checks = 0;
+    for (int iter = 0; iter < 20000; ++iter) {
+        // three 32-byte segments of codes, byte 0 of each in bits 63..62
+        std::vector<int> bases(96);
+        for (auto& x : bases) x = (int)(rng() & 3);
+        uint64_t seg[3] = {0, 0, 0};
+        for (int s = 0; s < 3; ++s)
+            for (int j = 0; j < 32; ++j) seg[s] |= (uint64_t)bases[32 * s + j] << (62 - 2 * j);
+        const uint32_t j = (uint32_t)(rng() % 32);
+        uint64_t lo, hi;
+        window_at(seg[0], seg[1], seg[2], j, lo, hi);
+        for (uint32_t k = 1; k <= 64; ++k) {
+            const int end = 64 + (int)j;  // stream index of the newest base
+            std::vector<int> win(bases.begin() + end - k + 1, bases.begin() + end + 1);
+            // window value check (oldest base highest)
+            for (uint32_t i = 0; i < k; ++i) {
+                const uint32_t bit = 2 * (k - 1 - i);
+                const uint64_t v = bit < 64 ? (lo >> bit) & 3 : (hi >> (bit - 64)) & 3;
+                if ((int)v != win[i]) { std::printf("window mismatch k=%u j=%u\n", k, j); return 1; }
+            }
+            std::vector<int> rf(win.rbegin(), win.rend()), cc(win.size());
+            for (size_t i = 0; i < win.size(); ++i) cc[i] = 3 - win[i];
+            uint64_t F[2], C[2];
+            pack_left(rf, F);
+            pack_left(cc, C);
+            const bool f_less = F[0] != C[0] ? F[0] < C[0] : F[1] < C[1];
+            const uint64_t* want = f_less ? F : C;
+            uint64_t got0, got1 = 0;
+            if (k <= 32) {
+                const uint64_t km = k >= 32 ? ~0ull : ((1ull << (2 * k)) - 1ull);
+                got0 = canonical1(lo & km, k);
+            } else {
+                const uint32_t hb = 2 * k - 64;
+                const uint64_t hm = hb >= 64 ? ~0ull : ((1ull << hb) - 1ull);
+                const Key2 key = canonical2(hi & hm, lo, k);
+                got0 = key.w0;
+                got1 = key.w1;
+            }
+            if (got0 != want[0] || got1 != (k <= 32 ? 0 : want[1])) {
+                std::printf("canonical mismatch k=%u\n", k);
+                return 1;
+            }
+            for (uint32_t B : {8u, 12u}) {
+                uint64_t l2 = lo, h2 = hi;
+                if (k <= 32) l2 &= k >= 32 ? ~0ull : ((1ull << (2 * k)) - 1ull);
+                else h2 &= (2 * k - 64) >= 64 ? ~0ull : ((1ull << (2 * k - 64)) - 1ull);
+                const uint32_t b = bucket_of_window(l2, h2, k, B);
+                if (b != (uint32_t)(want[0] >> (64 - B))) {
+                    std::printf("bucket mismatch k=%u B=%u got %u want %u\n", k, B, b, (unsigned)(want[0] >> (64 - B)));
+                    return 1;
+                }
+                // garbage above the window must not matter either
+                const uint32_t b2 = bucket_of_window(lo, k <= 32 ? rng() : h2, k, B);
+                if (k <= 32 && b2 != b) { std::printf("bucket depends on bits above the window k=%u\n", k); return 1; }
+            }
+            ++checks;
+        }
+    }
+    std::printf("ok %ld\n", checks);
+    return 0;
+}
