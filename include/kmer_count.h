@@ -171,6 +171,28 @@ int kc_stage_times(kc_context* ctx, double* ms, uint64_t* launches, int cap);
 
 const char* kc_stage_name(int stage);
 
+/* ---- allocation-free entry point ------------------------------------------
+ * No counterpart in the reference.  For callers that must not allocate device
+ * memory on this path: a framework whose caching allocator owns the device
+ * budget and forbids raw cudaMalloc, or a latency-sensitive thread that cannot
+ * afford cudaMalloc/cudaFree (cudaFree synchronises the device).
+ *
+ * Counts a FASTQ already in device memory (16-byte aligned, at most
+ * KC_NOALLOC_MAX_FASTQ_BYTES, 256 buckets) on `stream` (a cudaStream_t, NULL
+ * = default stream) and writes the packed low.bin bytes to d_low and the
+ * root records, grouped by root id, to d_roots (device buffers with the
+ * given byte capacities); stats receives the counters.  All scratch comes
+ * from one static device array of KC_NOALLOC_SCRATCH_BYTES that every GPU
+ * loading this library holds until exit.  The first call on a device looks up
+ * that array's address (make it before any stream capture).  Calls share the
+ * array: overlapping calls on the GPU race and must be serialised by the
+ * caller.  Larger inputs are rejected with KC_ERR_INVALID. */
+#define KC_NOALLOC_SCRATCH_BYTES (64ull << 20)
+#define KC_NOALLOC_MAX_FASTQ_BYTES (1ull << 20)
+
+int kc_count_device_noalloc(const kc_config* cfg, const uint8_t* d_fastq, uint64_t n, uint8_t* d_low,
+                            uint64_t low_cap, uint8_t* d_roots, uint64_t roots_cap, void* stream, kc_stats* stats);
+
 #ifdef __cplusplus
 }
 #endif

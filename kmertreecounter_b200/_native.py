@@ -28,8 +28,10 @@ ABI_SYMBOLS = (
     "kc_config_default", "kc_last_error", "kc_packed_bytes", "kc_record_bytes", "kc_count_fastq",
     "kc_create", "kc_destroy", "kc_count_host", "kc_count_device", "kc_result_sizes", "kc_copy_low",
     "kc_copy_roots", "kc_write_outputs", "kc_device_results", "kc_host_alloc", "kc_host_free", "kc_stream",
-    "kc_set_profiling", "kc_stage_times", "kc_stage_name",
+    "kc_set_profiling", "kc_stage_times", "kc_stage_name", "kc_count_device_noalloc",
 )
+NOALLOC_SCRATCH_BYTES = 64 << 20
+NOALLOC_MAX_FASTQ_BYTES = 1 << 20
 STAGE_COUNT = 10
 
 
@@ -90,6 +92,7 @@ def _load():
         "kc_set_profiling": (i32, [vp, i32]),
         "kc_stage_times": (i32, [vp, C.POINTER(C.c_double), C.POINTER(u64), i32]),
         "kc_stage_name": (C.c_char_p, [i32]),
+        "kc_count_device_noalloc": (i32, [cfgp, vp, u64, vp, u64, vp, u64, vp, stp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

@@ -42,7 +42,7 @@ def _deps(*names):
 
 def build(force=False, verbose_ptxas=False):
     os.makedirs(os.path.join(HERE, "bin"), exist_ok=True)
-    srcs = ["kc_engine.cu", "kc_sort.cu", "kc_io.cpp"]
+    srcs = ["kc_engine.cu", "kc_sort.cu", "kc_io.cpp", "kc_noalloc.cu"]
     hdrs = ["kc_kernels.cuh", "kc_scan.cuh", "kc_internal.h"]
     if force or _stale(LIB, _deps(*srcs, *hdrs)):
         cmd = [NVCC, *ARCH, "-lineinfo", "-O3", "-std=c++20", "-Xcompiler", "-fPIC", "-shared",

@@ -194,7 +194,7 @@ __device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t v, uint32_t* s
 
 // '\n' count per 8 KiB tile of the batch buf[0..n) (16-byte vector reads,
 // byte reads for the ragged end).
-__global__ void lines_per_tile(const uint8_t* __restrict__ buf, uint64_t n, uint32_t* __restrict__ tile_nl) {
+static __global__ void lines_per_tile(const uint8_t* __restrict__ buf, uint64_t n, uint32_t* __restrict__ tile_nl) {
     __shared__ uint32_t warp_sums[EXT_THREADS / 32];
     const uint64_t tile = blockIdx.x;
     const uint64_t pos = tile * EXT_TILE + (uint64_t)threadIdx.x * EXT_BPT;

@@ -56,7 +56,7 @@ __global__ void __launch_bounds__(SCAN_BLOCK) scan_reduce(const TI* __restrict__
 }
 
 // One block: sums[0..nb) -> exclusive prefix + base; *total_out = base + sum.
-__global__ void __launch_bounds__(SCAN_BLOCK) scan_sums(uint64_t* __restrict__ sums, uint64_t nb, uint64_t base,
+static __global__ void __launch_bounds__(SCAN_BLOCK) scan_sums(uint64_t* __restrict__ sums, uint64_t nb, uint64_t base,
                                                         uint64_t* __restrict__ total_out) {
     __shared__ uint64_t sw[32];
     uint64_t carry = base;
