@@ -63,7 +63,7 @@ typedef struct kc_config {
     int32_t device;        /* CUDA device ordinal */
     uint32_t sort_output;  /* 1: root records sorted by key inside each root file */
     uint64_t chunk_bytes;  /* host->device streaming chunk (default 256 MiB) */
-    uint64_t batch_bytes;  /* FASTQ bytes counted per device pass (default 4 GiB) */
+    uint64_t batch_bytes;  /* FASTQ bytes counted per device pass (default 1 GiB) */
     double bloom_bits;     /* first-occurrence filter bits per k-mer occurrence */
     double table_load;     /* target load factor of the repeat tables */
     double repeat_ratio;   /* sampled sizing: distinct repeat keys per k-mer */
@@ -88,7 +88,7 @@ typedef struct kc_stats {
 typedef struct kc_context kc_context;
 
 /* Defaults: k=31, canonical=1, min=1, max=UINT32_MAX, 256 buckets, sampled
- * sizing, device 0, unsorted roots, 256 MiB chunks, 4 GiB batches. */
+ * sizing, device 0, unsorted roots, 256 MiB chunks, 1 GiB batches. */
 void kc_config_default(kc_config* cfg);
 
 /* Thread-local message for the last failing call on this thread. */
@@ -117,6 +117,21 @@ void kc_destroy(kc_context* ctx);
  * bytes are streamed to the device in chunk_bytes pieces.  Results stay on
  * the device until copied out or written. */
 int kc_count_host(kc_context* ctx, const uint8_t* fastq, uint64_t n, kc_stats* stats);
+
+/* Streaming form of kc_count_host for large inputs: results are handed to
+ * `sink` on the calling thread as they reach host memory, so device->host
+ * copies overlap the counting of later batches.
+ *   kind KC_SINK_LOW   packed low.bin bytes, in file order (first
+ *                      occurrences of a batch are final when emitted)
+ *   kind KC_SINK_ROOT  ExportRecord<N> bytes of root file `root`, roots in
+ *                      order 0..255; an empty root is one call with bytes 0
+ * `data` is page-locked library memory valid only during the call.  A
+ * non-zero return from the sink stops the count with KC_ERR_IO. */
+#define KC_SINK_LOW 0
+#define KC_SINK_ROOT 1
+typedef int (*kc_sink_fn)(void* user, int kind, uint32_t root, const uint8_t* data, uint64_t bytes);
+int kc_count_host_stream(kc_context* ctx, const uint8_t* fastq, uint64_t n, kc_sink_fn sink, void* user,
+                         kc_stats* stats);
 
 /* Same, with the FASTQ already in device memory (a device pointer). */
 int kc_count_device(kc_context* ctx, const uint8_t* d_fastq, uint64_t n, kc_stats* stats);

@@ -28,8 +28,11 @@ ABI_SYMBOLS = (
     "kc_config_default", "kc_last_error", "kc_packed_bytes", "kc_record_bytes", "kc_count_fastq",
     "kc_create", "kc_destroy", "kc_count_host", "kc_count_device", "kc_result_sizes", "kc_copy_low",
     "kc_copy_roots", "kc_write_outputs", "kc_device_results", "kc_host_alloc", "kc_host_free", "kc_stream",
-    "kc_set_profiling", "kc_stage_times", "kc_stage_name", "kc_count_device_noalloc",
+    "kc_set_profiling", "kc_stage_times", "kc_stage_name", "kc_count_device_noalloc", "kc_count_host_stream",
 )
+KC_SINK_LOW = 0
+KC_SINK_ROOT = 1
+SINK_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_int, C.c_uint32, C.c_void_p, C.c_uint64)
 NOALLOC_SCRATCH_BYTES = 64 << 20
 NOALLOC_MAX_FASTQ_BYTES = 1 << 20
 STAGE_COUNT = 10
@@ -93,6 +96,7 @@ def _load():
         "kc_stage_times": (i32, [vp, C.POINTER(C.c_double), C.POINTER(u64), i32]),
         "kc_stage_name": (C.c_char_p, [i32]),
         "kc_count_device_noalloc": (i32, [cfgp, vp, u64, vp, u64, vp, u64, vp, stp]),
+        "kc_count_host_stream": (i32, [vp, vp, u64, SINK_FN, vp, stp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -181,6 +185,13 @@ class Counter:
 
     def count_host_ptr(self, ptr, n):
         check(lib.kc_count_host(self._ctx, C.c_void_p(ptr), n, C.byref(self.stats)))
+        return self.stats
+
+    def count_host_stream(self, ptr, n, sink):
+        """Streamed count of host bytes at address `ptr`; sink(kind, root,
+        data_address, nbytes) -> int is called as results reach host memory."""
+        cb = SINK_FN(lambda u, kind, root, data, nbytes: sink(kind, root, data, nbytes))
+        check(lib.kc_count_host_stream(self._ctx, C.c_void_p(ptr), n, cb, None, C.byref(self.stats)))
         return self.stats
 
     def count_device(self, dptr, n):

@@ -115,7 +115,31 @@ struct kc_context {
     cudaStream_t stream = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     uint32_t nw = 1, bucket_bits = 8, n_buckets = 256, bucket_shift = 56;
+    int sm_count = 148;
     uint64_t slot_bytes = 16, record_bytes = 16, packed_bytes = 8;
+
+    // host-input streaming: copy streams, double-buffered staging, pinned ring
+    cudaStream_t h2d = nullptr, d2h = nullptr;
+    cudaEvent_t ev_h2d[2] = {}, ev_free[2] = {}, ev_pack = nullptr, ev_lowfree[2] = {};
+    DevBuf stage2;       // second [HALO | batch | pad] staging buffer
+    DevBuf lowring[2];   // per-batch packed first occurrences (streamed mode)
+    int batch_slot = 0;  // staging slot of the batch being counted
+    cudaEvent_t after_scatter = nullptr;  // recorded once the batch's FASTQ bytes are no longer read
+    bool stream_low = false;
+    kc_sink_fn sink = nullptr;
+    void* sink_user = nullptr;
+    int sink_rc = 0;
+    static constexpr uint64_t PIN_BYTES = 512ull << 20;
+    static constexpr int PIN_SLOTS = 4;
+    uint8_t* pin[PIN_SLOTS] = {};
+    cudaEvent_t ev_pin[PIN_SLOTS] = {};
+    struct Piece {
+        int kind;
+        uint32_t root;
+        uint64_t bytes;
+        int slot;
+    };
+    std::vector<Piece> pending;  // FIFO of in-flight device->host pieces
 
     // batch pipeline
     DevBuf stage;        // [HALO | batch | pad] for host input
@@ -128,6 +152,7 @@ struct kc_context {
     DevBuf bloom, table;
     DevBuf low_packed;
     DevBuf roots, chunks, root_count, root_cursor;
+    DevBuf sort_tmp, sort_hist, sort_offs, sort_sums;
 
     // host mirrors
     std::vector<kc::BucketMeta> h_meta;
@@ -140,6 +165,7 @@ struct kc_context {
     // run state
     uint64_t line_base = 0;
     uint64_t low_total = 0;
+    uint64_t last_batch_low = 0;
     uint64_t K = 0;
     uint64_t rehashes = 0, batches = 0, input_bytes = 0;
     bool have_result = false;
@@ -269,7 +295,8 @@ int size_structures(kc_context* c, const std::vector<uint64_t>& kb, double scale
 template <int NW>
 void launch_count(kc_context* c, uint64_t n_keys, int use_filter) {
     constexpr int TILE = kc::count_tile<NW>();
-    const uint64_t tiles = ceil_div(n_keys, TILE);  // CTAs; each warp owns count_seg<NW>() keys
+    // each CTA covers CNT_SEGS_PER_WARP segments per warp, in blockIdx order
+    const uint64_t tiles = ceil_div(n_keys, (uint64_t)TILE * kc::CNT_SEGS_PER_WARP);
     if (!tiles) return;
     kc::CountArgs a;
     a.routed = c->routed.p;
@@ -281,6 +308,7 @@ void launch_count(kc_context* c, uint64_t n_keys, int use_filter) {
     a.seg_fail = c->tile_fail.as<uint32_t>();
     a.bucket_overflow = c->overflow.as<uint32_t>();
     a.bucket_shift = c->bucket_shift;
+    a.n_buckets = c->n_buckets;
     a.use_filter = use_filter;
     Stage st(c, use_filter ? KC_STAGE_COUNT_ROUTED : KC_STAGE_REHASH);
     kc::count_routed<NW><<<tiles, kc::CNT_THREADS, 0, c->stream>>>(a);
@@ -354,10 +382,13 @@ int launch_extract(kc_context* c, const uint8_t* buf, uint64_t n, int has_halo, 
     a.bucket_cursor = c->bucket_cursor.as<unsigned long long>();
     a.routed = c->routed.p;
     a.error = c->scalars.as<uint32_t>() + 12;
-    const size_t smem = (size_t)c->n_buckets * 16;
     Stage st(c, mode == kc::HIST ? KC_STAGE_EXTRACT_HIST : KC_STAGE_EXTRACT_SCATTER);
-    if (mode == kc::HIST) kc::extract_kernel<NW, kc::HIST><<<tiles, kc::EXT_THREADS, smem, c->stream>>>(a);
-    else kc::extract_kernel<NW, kc::SCATTER><<<tiles, kc::EXT_THREADS, smem, c->stream>>>(a);
+    if (mode == kc::HIST)
+        kc::extract_kernel<NW, kc::HIST>
+            <<<tiles, kc::EXT_THREADS, kc::extract_smem_bytes<NW, kc::HIST>(c->n_buckets), c->stream>>>(a);
+    else
+        kc::extract_kernel<NW, kc::SCATTER>
+            <<<tiles, kc::EXT_THREADS, kc::extract_smem_bytes<NW, kc::SCATTER>(c->n_buckets), c->stream>>>(a);
     CK(cudaGetLastError());
     return KC_OK;
 }
@@ -369,6 +400,7 @@ int process_batch(kc_context* c, const uint8_t* buf, uint64_t n, int has_halo) {
         return fail(KC_ERR_INVALID, "device FASTQ batch must be 16-byte aligned");
     const uint32_t nb = c->n_buckets;
     const uint64_t tiles = ceil_div(n, kc::EXT_TILE);
+    c->last_batch_low = 0;  // a batch without k-mers packs nothing
     CK(c->tile_nl.ensure(std::max<uint64_t>(tiles, 1) * sizeof(uint32_t)));
     CK(c->tile_line.ensure(std::max<uint64_t>(tiles, 1) * sizeof(uint64_t)));
     CK(c->scalars.ensure(64));
@@ -420,6 +452,7 @@ int process_batch(kc_context* c, const uint8_t* buf, uint64_t n, int has_halo) {
     CK(c->tile_low_prefix.ensure(ctiles * (CT / SEG) * sizeof(uint64_t)));
     CK(cudaMemcpyAsync(c->bucket_cursor.p, start.data(), nb * sizeof(uint64_t), cudaMemcpyHostToDevice, c->stream));
     if ((rc = launch_extract<NW>(c, buf, n, has_halo, kc::SCATTER))) return rc;
+    if (c->after_scatter) CK(cudaEventRecord(c->after_scatter, c->stream));
     uint32_t ext_err = 0;
     CK(cudaMemcpyAsync(&ext_err, c->scalars.as<uint32_t>() + 12, sizeof(uint32_t), cudaMemcpyDeviceToHost, c->stream));
 
@@ -435,14 +468,34 @@ int process_batch(kc_context* c, const uint8_t* buf, uint64_t n, int has_halo) {
     CK(cudaMemcpyAsync(&nlow, d_scal + 1, sizeof(uint64_t), cudaMemcpyDeviceToHost, c->stream));
     CK(cudaStreamSynchronize(c->stream));
     if (ext_err) return fail(KC_ERR_DEVICE, "internal error: routing bucket disagreed with its reservation");
-    CK(c->low_packed.grow_keep((c->low_total + nlow) * c->packed_bytes + 64, c->low_total * c->packed_bytes,
-                               c->stream));
-    Stage st(c, KC_STAGE_PACK_LOW);
-    kc::pack_low<NW><<<std::min<uint64_t>(ceil_div(nsegs, 8), 148 * 16), 256, 0, c->stream>>>(
-        c->routed.p, c->tile_low.as<uint32_t>(), c->tile_low_prefix.as<uint64_t>(), nsegs, c->cfg.k,
-        c->low_packed.as<uint8_t>(), c->low_total);
+    uint8_t* low_dst;
+    uint64_t low_base;
+    if (c->stream_low) {
+        // this batch's first occurrences go to a ring slot that the previous
+        // user (two batches ago) has finished copying out
+        DevBuf& ring = c->lowring[c->batches & 1];
+        if (ring.cap < nlow * c->packed_bytes + 64) {
+            CK(cudaStreamSynchronize(c->d2h));
+            CK(ring.ensure(nlow * c->packed_bytes + 64));
+        }
+        CK(cudaStreamWaitEvent(c->stream, c->ev_lowfree[c->batches & 1], 0));
+        low_dst = ring.as<uint8_t>();
+        low_base = 0;
+    } else {
+        CK(c->low_packed.grow_keep((c->low_total + nlow) * c->packed_bytes + 64, c->low_total * c->packed_bytes,
+                                   c->stream));
+        low_dst = c->low_packed.as<uint8_t>();
+        low_base = c->low_total;
+    }
+    {
+        Stage st(c, KC_STAGE_PACK_LOW);
+        kc::pack_low<NW><<<std::min<uint64_t>(ceil_div(nsegs, 8), 148 * 16), 256, 0, c->stream>>>(
+            c->routed.p, c->tile_low.as<uint32_t>(), c->tile_low_prefix.as<uint64_t>(), nsegs, c->cfg.k, low_dst,
+            low_base);
+    }
     CK(cudaGetLastError());
     c->low_total += nlow;
+    c->last_batch_low = nlow;
     return KC_OK;
 }
 
@@ -534,9 +587,16 @@ int finish_run(kc_context* c) {
     }
     rc = c->nw == 1 ? export_tables<1>(c) : export_tables<2>(c);
     if (rc) return rc;
-    if (c->cfg.sort_output) {
-        Stage st(c, KC_STAGE_SORT, 0);
-        rc = kc_sort_roots(c->roots.p, c->root_total, c->record_bytes, c->cfg.k, c->root_counts, c->stream);
+    if (c->cfg.sort_output && c->root_total > 1) {
+        uint64_t bt, bh, bo, bs;
+        kc_sort_scratch_bytes(c->root_total, c->record_bytes, &bt, &bh, &bo, &bs);
+        CK(c->sort_tmp.ensure(bt));
+        CK(c->sort_hist.ensure(bh));
+        CK(c->sort_offs.ensure(bo));
+        CK(c->sort_sums.ensure(bs));
+        const KcSortScratch w{c->sort_tmp.p, c->sort_hist.p, c->sort_offs.p, c->sort_sums.p};
+        Stage st(c, KC_STAGE_SORT, 4 * ((2 * c->cfg.k + 7) / 8));
+        rc = kc_sort_roots(c->roots.p, c->root_total, c->record_bytes, c->cfg.k, w, c->stream);
         if (rc) return fail(rc, "root record sort failed: %s", kc_sort_error());
     }
     CK(cudaStreamSynchronize(c->stream));
@@ -557,6 +617,78 @@ void fill_stats(kc_context* c, kc_stats* s, double dev_ms, double wall_ms) {
     std::memcpy(s->root_counts, c->root_counts, sizeof s->root_counts);
     s->device_ms = dev_ms;
     s->wall_ms = wall_ms;
+}
+
+// Deliver completed device->host pieces in order; `all` waits for every one.
+int drain_pieces(kc_context* c, bool all) {
+    size_t done = 0;
+    for (; done < c->pending.size(); ++done) {
+        const kc_context::Piece& p = c->pending[done];
+        if (!all && cudaEventQuery(c->ev_pin[p.slot]) == cudaErrorNotReady) break;
+        CK(cudaEventSynchronize(c->ev_pin[p.slot]));
+        if (!c->sink_rc) c->sink_rc = c->sink(c->sink_user, p.kind, p.root, c->pin[p.slot], p.bytes);
+    }
+    c->pending.erase(c->pending.begin(), c->pending.begin() + done);
+    if (c->sink_rc) return fail(KC_ERR_IO, "output sink returned %d", c->sink_rc);
+    return KC_OK;
+}
+
+// Copy `bytes` from device `src` to the caller through the pinned ring, in
+// pieces, after event `ready` on the compute stream.
+int stream_piece(kc_context* c, int kind, uint32_t root, const uint8_t* src, uint64_t bytes, cudaEvent_t ready) {
+    if (bytes == 0) {
+        if (kind == KC_SINK_ROOT) {
+            int rc = drain_pieces(c, true);
+            if (rc) return rc;
+            if (!c->sink_rc) c->sink_rc = c->sink(c->sink_user, kind, root, nullptr, 0);
+            if (c->sink_rc) return fail(KC_ERR_IO, "output sink returned %d", c->sink_rc);
+        }
+        return KC_OK;
+    }
+    CK(cudaStreamWaitEvent(c->d2h, ready, 0));
+    for (uint64_t off = 0; off < bytes; off += kc_context::PIN_BYTES) {
+        const uint64_t m = std::min<uint64_t>(kc_context::PIN_BYTES, bytes - off);
+        // a slot is reusable once its previous piece was delivered
+        int slot = -1;
+        for (;;) {
+            bool busy[kc_context::PIN_SLOTS] = {};
+            for (const auto& p : c->pending) busy[p.slot] = true;
+            for (int q = 0; q < kc_context::PIN_SLOTS && slot < 0; ++q)
+                if (!busy[q]) slot = q;
+            if (slot >= 0) break;
+            // deliver the oldest piece to free its slot
+            CK(cudaEventSynchronize(c->ev_pin[c->pending.front().slot]));
+            int rc = drain_pieces(c, false);
+            if (rc) return rc;
+        }
+        CK(cudaMemcpyAsync(c->pin[slot], src + off, m, cudaMemcpyDeviceToHost, c->d2h));
+        CK(cudaEventRecord(c->ev_pin[slot], c->d2h));
+        c->pending.push_back({kind, root, m, slot});
+    }
+    return drain_pieces(c, false);
+}
+
+int stream_out_low(kc_context* c) {
+    const int ring = (int)((c->batches) & 1);  // ring slot used by the batch just packed
+    CK(cudaEventRecord(c->ev_pack, c->stream));
+    int rc = stream_piece(c, KC_SINK_LOW, 0, c->lowring[ring].as<uint8_t>(), c->last_batch_low * c->packed_bytes,
+                          c->ev_pack);
+    if (rc) return rc;
+    // the ring slot is free for reuse once these copies are done
+    CK(cudaEventRecord(c->ev_lowfree[ring], c->d2h));
+    return KC_OK;
+}
+
+int stream_out_roots(kc_context* c) {
+    CK(cudaEventRecord(c->ev_pack, c->stream));
+    uint64_t off = 0;
+    for (uint32_t r = 0; r < 256; ++r) {
+        const uint64_t bytes = c->root_counts[r] * c->record_bytes;
+        int rc = stream_piece(c, KC_SINK_ROOT, r, c->roots.as<uint8_t>() + off, bytes, c->ev_pack);
+        if (rc) return rc;
+        off += bytes;
+    }
+    return KC_OK;
 }
 
 int run_batch(kc_context* c, const uint8_t* buf, uint64_t n, int has_halo) {
@@ -583,7 +715,7 @@ void kc_config_default(kc_config* g) {
     g->device = 0;
     g->sort_output = 0;
     g->chunk_bytes = 256ull << 20;
-    g->batch_bytes = 4ull << 30;
+    g->batch_bytes = 1ull << 30;
     g->bloom_bits = 8.0;
     g->table_load = 0.7;
     g->repeat_ratio = 0.125;
@@ -616,17 +748,33 @@ int kc_create(const kc_config* cfg, kc_context** out) {
         return fail(KC_ERR_INVALID, "device %d out of range (%d devices)", cfg->device, ndev);
     }
     c->device = cfg->device;
+    cudaDeviceGetAttribute(&c->sm_count, cudaDevAttrMultiProcessorCount, cfg->device);
     if ((e = cudaSetDevice(c->device)) != cudaSuccess || (e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking)) != cudaSuccess ||
         (e = cudaEventCreate(&c->ev0)) != cudaSuccess || (e = cudaEventCreate(&c->ev1)) != cudaSuccess) {
         delete c;
         return fail(KC_ERR_DEVICE, "stream/event creation failed: %s", cudaGetErrorString(e));
     }
-    // 4096-bucket extraction needs 64 KiB of dynamic shared memory.
-    const int smem = 4096 * 16;
-    cudaFuncSetAttribute(kc::extract_kernel<1, kc::HIST>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-    cudaFuncSetAttribute(kc::extract_kernel<1, kc::SCATTER>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-    cudaFuncSetAttribute(kc::extract_kernel<2, kc::HIST>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-    cudaFuncSetAttribute(kc::extract_kernel<2, kc::SCATTER>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if ((e = cudaStreamCreateWithFlags(&c->h2d, cudaStreamNonBlocking)) != cudaSuccess ||
+        (e = cudaStreamCreateWithFlags(&c->d2h, cudaStreamNonBlocking)) != cudaSuccess) {
+        delete c;
+        return fail(KC_ERR_DEVICE, "copy stream creation failed: %s", cudaGetErrorString(e));
+    }
+    for (int i = 0; i < 2; ++i) {
+        cudaEventCreateWithFlags(&c->ev_h2d[i], cudaEventDisableTiming);
+        cudaEventCreateWithFlags(&c->ev_free[i], cudaEventDisableTiming);
+        cudaEventCreateWithFlags(&c->ev_lowfree[i], cudaEventDisableTiming);
+    }
+    for (int i = 0; i < kc_context::PIN_SLOTS; ++i) cudaEventCreateWithFlags(&c->ev_pin[i], cudaEventDisableTiming);
+    cudaEventCreateWithFlags(&c->ev_pack, cudaEventDisableTiming);
+    // 4096-bucket extraction and the scatter staging area exceed 48 KiB.
+    cudaFuncSetAttribute(kc::extract_kernel<1, kc::HIST>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)kc::extract_smem_bytes<1, kc::HIST>(4096));
+    cudaFuncSetAttribute(kc::extract_kernel<1, kc::SCATTER>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)kc::extract_smem_bytes<1, kc::SCATTER>(4096));
+    cudaFuncSetAttribute(kc::extract_kernel<2, kc::HIST>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)kc::extract_smem_bytes<2, kc::HIST>(4096));
+    cudaFuncSetAttribute(kc::extract_kernel<2, kc::SCATTER>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)kc::extract_smem_bytes<2, kc::SCATTER>(4096));
     if ((e = cudaGetLastError()) != cudaSuccess) {
         delete c;
         return fail(KC_ERR_DEVICE, "kernel attribute setup failed: %s", cudaGetErrorString(e));
@@ -642,9 +790,24 @@ void kc_destroy(kc_context* c) {
     DevBuf* bufs[] = {&c->stage,  &c->tile_nl,   &c->tile_line, &c->bucket_count, &c->bucket_cursor, &c->routed,
                       &c->tile_low, &c->tile_fail, &c->tile_low_prefix, &c->scan_sums, &c->scalars, &c->overflow,
                       &c->meta,   &c->bloom,     &c->table,     &c->low_packed,   &c->roots,         &c->chunks,
-                      &c->root_count, &c->root_cursor};
+                      &c->root_count, &c->root_cursor, &c->sort_tmp, &c->sort_hist, &c->sort_offs, &c->sort_sums};
     for (DevBuf* b : bufs) b->release();
     for (cudaEvent_t e : c->ev_pool) cudaEventDestroy(e);
+    if (c->h2d) cudaStreamSynchronize(c->h2d);
+    if (c->d2h) cudaStreamSynchronize(c->d2h);
+    for (int i = 0; i < 2; ++i) {
+        for (cudaEvent_t e : {c->ev_h2d[i], c->ev_free[i], c->ev_lowfree[i]})
+            if (e) cudaEventDestroy(e);
+        c->lowring[i].release();
+    }
+    for (int i = 0; i < kc_context::PIN_SLOTS; ++i) {
+        if (c->ev_pin[i]) cudaEventDestroy(c->ev_pin[i]);
+        if (c->pin[i]) cudaFreeHost(c->pin[i]);
+    }
+    if (c->ev_pack) cudaEventDestroy(c->ev_pack);
+    c->stage2.release();
+    if (c->h2d) cudaStreamDestroy(c->h2d);
+    if (c->d2h) cudaStreamDestroy(c->d2h);
     if (c->ev0) cudaEventDestroy(c->ev0);
     if (c->ev1) cudaEventDestroy(c->ev1);
     if (c->stream) cudaStreamDestroy(c->stream);
@@ -695,34 +858,97 @@ int kc_count_device(kc_context* c, const uint8_t* d_fastq, uint64_t n, kc_stats*
     return KC_OK;
 }
 
-// Host input: stream chunk_bytes pieces into the staging buffer
-// [HALO | batch | pad]; between batches the last HALO bytes move to the
-// front so windows that straddle the split are seen once, as the reference
-// reader's k-1 overlap does (src/FastqReader.h:338-365).
+// Host input, double-buffered: batch i+1 is copied host->device on its own
+// stream (chunk_bytes pieces) while batch i is counted.  Staging buffers are
+// [HALO | batch | pad]; the HALO bytes before a batch are copied from the
+// host too, so windows that straddle a batch split are seen once, as the
+// reference reader's k-1 overlap does (src/FastqReader.h:338-365).
+int host_pipeline(kc_context* c, const uint8_t* fastq, uint64_t n) {
+    const uint64_t B = std::max<uint64_t>(kc::EXT_TILE, c->cfg.batch_bytes & ~(uint64_t)(kc::EXT_TILE - 1));
+    const uint64_t cap = std::min<uint64_t>(B, std::max<uint64_t>(n, 1));
+    const uint64_t nbatch = n ? ceil_div(n, cap) : 0;
+    CK(c->stage.ensure(kc::HALO + cap + kc::EXT_TILE));
+    if (nbatch > 1) CK(c->stage2.ensure(kc::HALO + cap + kc::EXT_TILE));
+    uint8_t* slots[2] = {c->stage.as<uint8_t>(), c->stage2.as<uint8_t>()};
+    const uint64_t chunk = std::max<uint64_t>(c->cfg.chunk_bytes, 1 << 20);
+    auto enqueue_copy = [&](uint64_t i) -> int {
+        const int slot = (int)(i & 1);
+        const uint64_t off = i * cap, len = std::min<uint64_t>(cap, n - off);
+        uint8_t* dst = slots[slot];
+        if (i >= 2) CK(cudaStreamWaitEvent(c->h2d, c->ev_free[slot], 0));
+        if (off >= (uint64_t)kc::HALO) CK(cudaMemcpyAsync(dst, fastq + off - kc::HALO, kc::HALO, cudaMemcpyHostToDevice, c->h2d));
+        for (uint64_t q = 0; q < len; q += chunk)
+            CK(cudaMemcpyAsync(dst + kc::HALO + q, fastq + off + q, std::min<uint64_t>(chunk, len - q),
+                               cudaMemcpyHostToDevice, c->h2d));
+        CK(cudaEventRecord(c->ev_h2d[slot], c->h2d));
+        return KC_OK;
+    };
+    int rc;
+    if (nbatch && (rc = enqueue_copy(0))) return rc;
+    for (uint64_t i = 0; i < nbatch; ++i) {
+        if (i + 1 < nbatch && (rc = enqueue_copy(i + 1))) return rc;
+        const int slot = (int)(i & 1);
+        const uint64_t off = i * cap, len = std::min<uint64_t>(cap, n - off);
+        CK(cudaStreamWaitEvent(c->stream, c->ev_h2d[slot], 0));
+        c->after_scatter = c->ev_free[slot];
+        rc = run_batch(c, slots[slot] + kc::HALO, len, off > 0);
+        c->after_scatter = nullptr;
+        if (rc) return rc;
+        if (c->stream_low && (rc = stream_out_low(c))) return rc;
+    }
+    return KC_OK;
+}
+
 int kc_count_host(kc_context* c, const uint8_t* fastq, uint64_t n, kc_stats* stats) {
     if (!c || (!fastq && n)) return fail(KC_ERR_INVALID, "null argument");
     const auto t0 = std::chrono::steady_clock::now();
     int rc = begin_run(c, n);
     if (rc) return rc;
-    const uint64_t B = std::max<uint64_t>(kc::EXT_TILE, c->cfg.batch_bytes & ~(uint64_t)(kc::EXT_TILE - 1));
-    const uint64_t cap = std::min<uint64_t>(B, std::max<uint64_t>(n, 1));
-    CK(c->stage.ensure(kc::HALO + cap + kc::EXT_TILE));
+    c->stream_low = false;
     CK(cudaEventRecord(c->ev0, c->stream));
-    uint8_t* base = c->stage.as<uint8_t>();
-    const uint64_t chunk = std::max<uint64_t>(c->cfg.chunk_bytes, 1 << 20);
-    for (uint64_t off = 0; off < n; off += cap) {
-        const uint64_t len = std::min<uint64_t>(cap, n - off);
-        if (off > 0) {
-            // previous batch's last HALO bytes (always >= HALO bytes long here)
-            CK(cudaMemcpyAsync(base, base + kc::HALO + cap - kc::HALO, kc::HALO, cudaMemcpyDeviceToDevice, c->stream));
-        }
-        for (uint64_t q = 0; q < len; q += chunk) {
-            const uint64_t m = std::min<uint64_t>(chunk, len - q);
-            CK(cudaMemcpyAsync(base + kc::HALO + q, fastq + off + q, m, cudaMemcpyHostToDevice, c->stream));
-        }
-        if ((rc = run_batch(c, base + kc::HALO, len, off > 0))) return rc;
-    }
+    if ((rc = host_pipeline(c, fastq, n))) return rc;
     if ((rc = finish_run(c))) return rc;
+    CK(cudaEventRecord(c->ev1, c->stream));
+    CK(cudaEventSynchronize(c->ev1));
+    collect_stage_times(c);
+    float ms = 0;
+    cudaEventElapsedTime(&ms, c->ev0, c->ev1);
+    const double wall = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    fill_stats(c, stats, ms, wall);
+    return KC_OK;
+}
+
+int kc_count_host_stream(kc_context* c, const uint8_t* fastq, uint64_t n, kc_sink_fn sink, void* user,
+                         kc_stats* stats) {
+    if (!c || (!fastq && n) || !sink) return fail(KC_ERR_INVALID, "null argument");
+    const auto t0 = std::chrono::steady_clock::now();
+    int rc = begin_run(c, n);
+    if (rc) return rc;
+    for (int i = 0; i < kc_context::PIN_SLOTS; ++i) {
+        if (!c->pin[i]) {
+            if (cudaHostAlloc(reinterpret_cast<void**>(&c->pin[i]), kc_context::PIN_BYTES, cudaHostAllocDefault) !=
+                cudaSuccess) {
+                cudaGetLastError();
+                c->pin[i] = nullptr;
+                return fail(KC_ERR_NOMEM, "pinned staging allocation failed");
+            }
+        }
+        CK(cudaEventRecord(c->ev_pin[i], c->d2h));
+    }
+    for (int i = 0; i < 2; ++i) CK(cudaEventRecord(c->ev_lowfree[i], c->d2h));
+    c->stream_low = true;
+    c->sink = sink;
+    c->sink_user = user;
+    c->sink_rc = 0;
+    c->pending.clear();
+    CK(cudaEventRecord(c->ev0, c->stream));
+    rc = host_pipeline(c, fastq, n);
+    if (!rc) rc = finish_run(c);
+    if (!rc) rc = stream_out_roots(c);
+    const int drc = drain_pieces(c, true);
+    c->stream_low = false;
+    if (rc) return rc;
+    if (drc) return drc;
     CK(cudaEventRecord(c->ev1, c->stream));
     CK(cudaEventSynchronize(c->ev1));
     collect_stage_times(c);

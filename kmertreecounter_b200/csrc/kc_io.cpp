@@ -153,17 +153,57 @@ int kc_write_outputs(kc_context* ctx, const char* out_dir) {
     return rc;
 }
 
+// Sink that writes low.bin sequentially and root_{id}.bin one after another.
+struct FileSink {
+    std::string dir;
+    int low_fd = -1;
+    int root_fd = -1;
+    int cur_root = -1;
+    std::string err;
+    static int call(void* u, int kind, uint32_t root, const uint8_t* data, uint64_t bytes) {
+        FileSink* f = static_cast<FileSink*>(u);
+        if (kind == KC_SINK_LOW) {
+            if (!write_all(f->low_fd, data, bytes)) return f->fail("short write to low.bin");
+            return 0;
+        }
+        if ((int)root != f->cur_root) {
+            if (f->root_fd >= 0 && ::close(f->root_fd) != 0) return f->fail("close failed");
+            const std::string path = f->dir + "root_" + std::to_string(root) + ".bin";
+            f->root_fd = ::open(path.c_str(), O_WRONLY | O_CREAT | O_TRUNC, 0644);
+            if (f->root_fd < 0) return f->fail("failed to open final drain output file " + path);
+            f->cur_root = (int)root;
+        }
+        if (bytes && !write_all(f->root_fd, data, bytes)) return f->fail("short write to a root file");
+        return 0;
+    }
+    int fail(const std::string& m) {
+        err = m + ": " + std::strerror(errno);
+        return 1;
+    }
+};
+
 int kc_count_fastq(const kc_config* cfg, const char* fastq_path, const char* out_dir, kc_stats* stats) {
     if (!cfg || !fastq_path) return kc_internal_set_error(KC_ERR_INVALID, "null argument");
+    FileSink fs;
+    fs.dir = with_slash(out_dir ? out_dir : "./tmp/");
+    if (::mkdir(fs.dir.c_str(), 0755) != 0 && errno != EEXIST)
+        return io_fail("cannot create " + fs.dir + ": " + std::strerror(errno));
     kc_context* ctx = nullptr;
     int rc = kc_create(cfg, &ctx);
     if (rc) return rc;
     uint8_t* data = nullptr;
     uint64_t n = 0;
     if ((rc = read_fastq(fastq_path, &data, &n)) == KC_OK) {
-        rc = kc_count_host(ctx, data, n, stats);
+        fs.low_fd = ::open((fs.dir + "low.bin").c_str(), O_WRONLY | O_CREAT | O_TRUNC, 0644);
+        if (fs.low_fd < 0) {
+            rc = io_fail("Failed to open export file: " + fs.dir + "low.bin");
+        } else {
+            rc = kc_count_host_stream(ctx, data, n, &FileSink::call, &fs, stats);
+            if (rc == KC_ERR_IO && !fs.err.empty()) io_fail(fs.err);
+            if (::close(fs.low_fd) != 0 && rc == KC_OK) rc = io_fail("close of low.bin failed");
+            if (fs.root_fd >= 0 && ::close(fs.root_fd) != 0 && rc == KC_OK) rc = io_fail("close of a root file failed");
+        }
         kc_host_free(data);
-        if (rc == KC_OK) rc = kc_write_outputs(ctx, out_dir ? out_dir : "./tmp/");
     }
     kc_destroy(ctx);
     return rc;

@@ -382,18 +382,38 @@ KC_HD uint32_t bucket_of_window(uint64_t lo, uint64_t hi, uint32_t k, uint32_t B
 // HIST: per-bucket totals via the bucket-only path.  SCATTER: bucket-only
 // histogram, one reservation per bucket per CTA, then full keys written to
 // routed[base[bucket] + rank].
+// Keys of one SCATTER tile staged in shared memory (bucket-sorted) before
+// they are written out as contiguous runs; keys beyond this go out directly.
+template <int NW>
+__host__ __device__ constexpr int stage_keys() {
+    return NW == 1 ? 4096 : 2048;
+}
+
+// Dynamic shared memory of extract_kernel.
+template <int NW, int MODE>
+__host__ __device__ constexpr size_t extract_smem_bytes(uint32_t n_buckets) {
+    return (size_t)n_buckets * (8 + 4 + 4 + 4) +
+           (MODE == SCATTER ? (size_t)stage_keys<NW>() * (8 * NW + 2) : 0);
+}
+
 template <int NW, int MODE>
 __global__ void __launch_bounds__(EXT_THREADS) extract_kernel(ExtractArgs a) {
-    // dynamic smem: u64 base[n_buckets] | u32 hist[n_buckets] | u32 fill[n_buckets]
+    // dynamic smem: u64 base[nb] | u32 hist[nb] | u32 fill[nb] | u32 loff[nb]
+    //               | K keys[stage] | u16 bucket_of_key[stage]
     extern __shared__ unsigned long long ext_smem[];
     __shared__ uint64_t seg_codes[EXT_THREADS + 2];
     __shared__ uint32_t seg_bases[EXT_THREADS + 2];
     __shared__ uint32_t seg_emit[EXT_THREADS];
     __shared__ uint32_t warp_sums[EXT_THREADS / 32];
     __shared__ uint32_t tile_any;
+    using K = typename KeyOf<NW>::T;
+    constexpr int STAGE = stage_keys<NW>();
     unsigned long long* bbase = ext_smem;
     uint32_t* hist = reinterpret_cast<uint32_t*>(ext_smem + a.n_buckets);
     uint32_t* fill = hist + a.n_buckets;
+    uint32_t* loff = fill + a.n_buckets;
+    K* skeys = reinterpret_cast<K*>(loff + a.n_buckets + (a.n_buckets & 1));  // 8-byte aligned
+    uint16_t* sbkt = reinterpret_cast<uint16_t*>(skeys + STAGE);
 
     const int tid = threadIdx.x;
     const uint64_t tile_start = (uint64_t)blockIdx.x * EXT_TILE;
@@ -448,9 +468,26 @@ __global__ void __launch_bounds__(EXT_THREADS) extract_kernel(ExtractArgs a) {
 #pragma unroll 1
     for (int pass = 0; pass < (MODE == SCATTER ? 2 : 1); ++pass) {
         if (pass == 1) {
-            for (uint32_t b = tid; b < a.n_buckets; b += EXT_THREADS) {
-                const uint32_t c = hist[b];
-                bbase[b] = c ? atomicAdd(a.bucket_cursor + b, (unsigned long long)c) : 0ull;
+            // reserve each bucket's run in the routed array; local offsets of
+            // the bucket-sorted staging area (per-thread chunk of buckets +
+            // block scan)
+            const uint32_t per = (a.n_buckets + EXT_THREADS - 1) / EXT_THREADS;
+            uint32_t sum = 0;
+            for (uint32_t q = 0; q < per; ++q) {
+                const uint32_t b = tid * per + q;
+                if (b < a.n_buckets) {
+                    const uint32_t c = hist[b];
+                    bbase[b] = c ? atomicAdd(a.bucket_cursor + b, (unsigned long long)c) : 0ull;
+                    sum += c;
+                }
+            }
+            uint32_t run = block_exclusive_scan<EXT_THREADS>(sum, warp_sums, nullptr);
+            for (uint32_t q = 0; q < per; ++q) {
+                const uint32_t b = tid * per + q;
+                if (b < a.n_buckets) {
+                    loff[b] = run;
+                    run += hist[b];
+                }
             }
             __syncthreads();
         }
@@ -486,13 +523,36 @@ __global__ void __launch_bounds__(EXT_THREADS) extract_kernel(ExtractArgs a) {
                 }
                 const uint32_t rnk = atomicAdd(fill + bucket, 1u);
                 if (rnk < hist[bucket]) {
-                    reinterpret_cast<typename KeyOf<NW>::T*>(a.routed)[bbase[bucket] + rnk] = key;
+                    const uint32_t sidx = loff[bucket] + rnk;
+                    if (sidx < (uint32_t)STAGE) {
+                        skeys[sidx] = key;
+                        sbkt[sidx] = (uint16_t)bucket;
+                    } else {
+                        reinterpret_cast<K*>(a.routed)[bbase[bucket] + rnk] = key;
+                    }
                 } else {
                     atomicOr(a.error, 1u);  // never write outside the reservation
                 }
             }
         }
         __syncthreads();
+        if (MODE == SCATTER && pass == 1) {
+            // staged keys out as contiguous runs: consecutive slots of one
+            // bucket go to consecutive routed positions
+            uint32_t total = 0;
+            for (uint32_t b = tid; b < a.n_buckets; b += EXT_THREADS) total += hist[b];
+            for (int o = 16; o; o >>= 1) total += __shfl_xor_sync(0xffffffffu, total, o);
+            if ((tid & 31) == 0) warp_sums[tid >> 5] = total;
+            __syncthreads();
+            total = 0;
+            for (int w = 0; w < EXT_THREADS / 32; ++w) total += warp_sums[w];
+            const uint32_t staged = min(total, (uint32_t)STAGE);
+            K* out = reinterpret_cast<K*>(a.routed);
+            for (uint32_t i = tid; i < staged; i += EXT_THREADS) {
+                const uint32_t b = sbkt[i];
+                out[bbase[b] + (i - loff[b])] = skeys[i];
+            }
+        }
     }
     if (MODE == HIST) {
         for (uint32_t b = tid; b < a.n_buckets; b += EXT_THREADS) {
@@ -512,16 +572,16 @@ __device__ __forceinline__ uint64_t bloom_bits(uint64_t h) {
     return (1ull << ((h >> 40) & 63)) | (1ull << ((h >> 46) & 63)) | (1ull << ((h >> 52) & 63));
 }
 
-// Insert `add` occurrences of key into a bucket table; false = probe limit
-// hit.  `seen` is the key word already read from the first probe slot (or
-// EMPTY-1 when none was read), which saves the first load.
-__device__ __forceinline__ bool table_add(Slot1* __restrict__ tab, uint64_t mask, uint64_t h, uint64_t key,
-                                          uint32_t add, const uint64_t* seen = nullptr) {
-    uint64_t i = (h >> 17) & mask;
+// Insert `add` occurrences of key into a bucket table starting at slot
+// (h >> 17) & mask; false = probe limit hit.  Linear probing; a slot goes
+// EMPTY -> key exactly once (CAS), counts only grow (atomicAdd).
+static __device__ __noinline__ bool table_add_slow(Slot1* __restrict__ tab, uint64_t mask, uint64_t h, uint64_t key,
+                                            uint32_t add, int first_p) {
+    const uint64_t i = (h >> 17) & mask;
     const int limit = (int)min((uint64_t)PROBE_LIMIT, mask + 1);
-    for (int p = 0; p < limit; ++p) {
+    for (int p = first_p; p < limit; ++p) {
         Slot1* s = tab + ((i + p) & mask);
-        uint64_t cur = (p == 0 && seen) ? *seen : __ldcg(&s->key);
+        uint64_t cur = __ldcg(&s->key);
         if (cur == EMPTY) {
             cur = atomicCAS(reinterpret_cast<unsigned long long*>(&s->key), EMPTY, key);
             if (cur == EMPTY) cur = key;
@@ -534,16 +594,16 @@ __device__ __forceinline__ bool table_add(Slot1* __restrict__ tab, uint64_t mask
     return false;
 }
 
-__device__ __forceinline__ bool table_add(Slot2* __restrict__ tab, uint64_t mask, uint64_t h, const Key2& key,
-                                          uint32_t add, const ulonglong2* seen = nullptr) {
-    uint64_t i = (h >> 17) & mask;
+static __device__ __noinline__ bool table_add_slow(Slot2* __restrict__ tab, uint64_t mask, uint64_t h, const Key2 key,
+                                            uint32_t add, int first_p) {
+    const uint64_t i = (h >> 17) & mask;
     const int limit = (int)min((uint64_t)PROBE_LIMIT, mask + 1);
-    for (int p = 0; p < limit; ++p) {
+    for (int p = first_p; p < limit; ++p) {
         Slot2* s = tab + ((i + p) & mask);
-        const ulonglong2 v = (p == 0 && seen) ? *seen : __ldcg(reinterpret_cast<const ulonglong2*>(s));
+        const ulonglong2 v = __ldcg(reinterpret_cast<const ulonglong2*>(s));
         bool mine = (v.x == key.w0 && v.y == key.w1);
-        // A slot goes EMPTY -> key exactly once.  A 16-byte read that shows an
-        // EMPTY half may be torn, so ask the CAS for the authoritative value.
+        // A 16-byte read that shows an EMPTY half may be torn, so ask the CAS
+        // for the authoritative value.
         if (!mine && (v.x == EMPTY || v.y == EMPTY)) {
             const unsigned __int128 e = ~(unsigned __int128)0;
             const unsigned __int128 kv = ((unsigned __int128)key.w1 << 64) | key.w0;
@@ -556,6 +616,36 @@ __device__ __forceinline__ bool table_add(Slot2* __restrict__ tab, uint64_t mask
         }
     }
     return false;
+}
+
+// Full insert (used by the table rehash).
+__device__ __forceinline__ bool table_add(Slot1* tab, uint64_t mask, uint64_t h, uint64_t key, uint32_t add) {
+    return table_add_slow(tab, mask, h, key, add, 0);
+}
+__device__ __forceinline__ bool table_add(Slot2* tab, uint64_t mask, uint64_t h, const Key2& key, uint32_t add) {
+    return table_add_slow(tab, mask, h, key, add, 0);
+}
+
+// First probe already read (`seen`): settle the common cases inline -- the
+// slot holds the key (add), or is empty (claim, add) -- else walk on.
+__device__ __forceinline__ bool table_add_first(Slot1* tab, uint64_t mask, uint64_t h, uint64_t key, uint32_t add,
+                                                uint64_t seen) {
+    Slot1* s = tab + ((h >> 17) & mask);
+    if (seen == EMPTY) seen = atomicCAS(reinterpret_cast<unsigned long long*>(&s->key), EMPTY, key), seen = seen == EMPTY ? key : seen;
+    if (seen == key) {
+        atomicAdd(&s->count, add);
+        return true;
+    }
+    return table_add_slow(tab, mask, h, key, add, 1);
+}
+__device__ __forceinline__ bool table_add_first(Slot2* tab, uint64_t mask, uint64_t h, const Key2& key, uint32_t add,
+                                                ulonglong2 seen) {
+    Slot2* s = tab + ((h >> 17) & mask);
+    if (seen.x == key.w0 && seen.y == key.w1) {
+        atomicAdd(&s->count, add);
+        return true;
+    }
+    return table_add_slow(tab, mask, h, key, add, 0);
 }
 
 __device__ __forceinline__ bool key_eq(uint64_t a, uint64_t b) { return a == b; }
@@ -596,8 +686,17 @@ struct CountArgs {
     uint32_t* seg_fail;           // per warp segment: overflowed keys kept at its back
     uint32_t* bucket_overflow;    // set to 1 for a bucket whose table overflowed
     uint32_t bucket_shift;
+    uint32_t n_buckets;
     int use_filter;               // 0: retry pass (table only, no filter)
 };
+
+// Bucket placement as read by the count kernel (shared memory copy).
+struct MetaS {
+    uint64_t bloom_off, tab_off;
+    uint32_t bloom_mask, tab_mask;
+};
+constexpr int META_SMEM_BUCKETS = 256;
+constexpr int CNT_SEGS_PER_WARP = 4;
 
 // For each routed key: the first-occurrence filter decides low.bin (first)
 // or the repeat table (seen before), as the reference's classifier does with
@@ -607,149 +706,155 @@ struct CountArgs {
 // open-addressing table (replaces KmerTree + ConcurrentMap::increment,
 // src/NewKmerTree.h:383-489, src/ConcurrentMap.h:112-160).
 //
-// Each warp owns a contiguous segment of count_seg<NW>() keys.  The work is
-// staged so that every lane has all its items' memory requests in flight at
-// once (filter reads, then filter atomics, then first table probes) instead
-// of one dependent chain per item.  Equal keys inside a warp are merged first
-// (__match_any_sync): one filter probe and one table add per distinct key.
-//
-// Outputs are compacted IN PLACE into the warp's own segment (only this warp
-// reads it, so __syncwarp orders the reads before the writes): first
+// Persistent CTAs; each warp walks contiguous segments of count_seg<NW>()
+// keys.  Per segment: equal keys inside the warp are merged
+// (__match_any_sync); every item's filter word and first table slot are read
+// together (one round trip settles most repeats); filter atomics and table
+// adds follow.  Outputs are compacted IN PLACE into the warp's own segment
+// (only this warp reads it; __syncwarp orders reads before writes): first
 // occurrences at the front, keys that met a full table at the back.
 template <int NW>
 __global__ void __launch_bounds__(CNT_THREADS, 4) count_routed(CountArgs a) {
     using K = typename KeyOf<NW>::T;
     using S = typename SlotOf<NW>::T;
+    using Seen = typename std::conditional<NW == 1, uint64_t, ulonglong2>::type;
     constexpr int ITEMS = count_items<NW>();
     constexpr int SEG = count_seg<NW>();
+    __shared__ MetaS sm[META_SMEM_BUCKETS];
+    const bool meta_in_smem = a.n_buckets <= META_SMEM_BUCKETS;
+    if (meta_in_smem) {
+        for (uint32_t b = threadIdx.x; b < a.n_buckets; b += blockDim.x) {
+            const BucketMeta m = a.meta[b];
+            sm[b] = MetaS{m.bloom_off, m.tab_off, (uint32_t)m.bloom_mask, (uint32_t)m.tab_mask};
+        }
+        __syncthreads();
+    }
+    auto meta_of = [&](uint32_t b) -> MetaS {
+        if (meta_in_smem) return sm[b];
+        const BucketMeta* m = a.meta + b;
+        return MetaS{__ldg(&m->bloom_off), __ldg(&m->tab_off), (uint32_t)__ldg(&m->bloom_mask),
+                     (uint32_t)__ldg(&m->tab_mask)};
+    };
 
     K* keys = reinterpret_cast<K*>(a.routed);
+    S* table = reinterpret_cast<S*>(a.table);
     const int lane = threadIdx.x & 31;
-    const uint64_t gw = (uint64_t)blockIdx.x * (CNT_THREADS / 32) + (threadIdx.x >> 5);
-    const uint64_t s0 = gw * SEG;
-    if (s0 >= a.n_keys) return;
-    const uint64_t s_end = min(a.n_keys, s0 + SEG);
-    uint64_t base = s0;
-    uint32_t n_in = (uint32_t)(s_end - s0);
-    if (!a.use_filter) {
-        const uint32_t nf = a.seg_fail[gw];
-        if (nf == 0) return;
-        base = s_end - nf;
-        n_in = nf;
-    }
-
-    K it[ITEMS];
-    uint32_t mult[ITEMS];
-#pragma unroll
-    for (int j = 0; j < ITEMS; ++j) {
-        const uint32_t idx = (uint32_t)(j * 32 + lane);
-        mult[j] = idx < n_in ? 1u : 0u;
-        if (mult[j]) it[j] = keys[base + idx];
-    }
-    __syncwarp();  // every read of the segment precedes any in-place write
-
-    // merge equal keys inside the warp: the lowest lane carries the multiplicity
-#pragma unroll
-    for (int j = 0; j < ITEMS; ++j) {
-        const uint32_t active = __ballot_sync(0xffffffffu, mult[j] != 0);
-        if (mult[j]) {
-            uint32_t same;
-            if constexpr (NW == 1) same = __match_any_sync(active, it[j]);
-            else same = __match_any_sync(active, it[j].w0) & __match_any_sync(active, it[j].w1);
-            mult[j] = ((__ffs(same) - 1) == lane) ? (uint32_t)__popc(same) : 0u;
+    const uint32_t lt = (1u << lane) - 1u;
+    const uint64_t n_segs = (a.n_keys + SEG - 1) / SEG;
+    // Each CTA owns CNT_SEGS_PER_WARP consecutive segments per warp; CTAs are
+    // dispatched in blockIdx order, so the keys in flight stay within a narrow
+    // window of the bucket-sorted array (one or two buckets' filter and table
+    // lines live in L2 at a time).
+    const uint64_t cta_seg0 = (uint64_t)blockIdx.x * (CNT_THREADS / 32) * CNT_SEGS_PER_WARP;
+    const uint64_t cta_seg1 = min(n_segs, cta_seg0 + (uint64_t)(CNT_THREADS / 32) * CNT_SEGS_PER_WARP);
+    for (uint64_t gw = cta_seg0 + (threadIdx.x >> 5); gw < cta_seg1; gw += CNT_THREADS / 32) {
+        const uint64_t s0 = gw * SEG;
+        const uint64_t s_end = min(a.n_keys, s0 + SEG);
+        uint64_t base = s0;
+        uint32_t n_in = (uint32_t)(s_end - s0);
+        if (!a.use_filter) {
+            const uint32_t nf = a.seg_fail[gw];
+            if (nf == 0) continue;  // warp-uniform
+            base = s_end - nf;
+            n_in = nf;
         }
-    }
 
-    uint64_t h[ITEMS];
-    uint32_t bucket[ITEMS];
-    uint32_t first_bits = 0;  // bit j: item j is a first occurrence
-    if (a.use_filter) {
-        uint64_t* word[ITEMS];
-        uint64_t old[ITEMS];
+        K it[ITEMS];
+        uint32_t mult[ITEMS];
 #pragma unroll
         for (int j = 0; j < ITEMS; ++j) {
+            const uint32_t idx = (uint32_t)(j * 32 + lane);
+            mult[j] = idx < n_in ? 1u : 0u;
+            if (mult[j]) it[j] = keys[base + idx];
+        }
+        __syncwarp();  // every read of the segment precedes any in-place write
+
+        // merge equal keys: the lowest lane of a group carries the multiplicity
+#pragma unroll
+        for (int j = 0; j < ITEMS; ++j) {
+            const uint32_t active = __ballot_sync(0xffffffffu, mult[j] != 0);
             if (mult[j]) {
-                bucket[j] = (uint32_t)(key_hi(it[j]) >> a.bucket_shift);
-                h[j] = hash_key(it[j]);
-                const uint64_t off = __ldg(&a.meta[bucket[j]].bloom_off), msk = __ldg(&a.meta[bucket[j]].bloom_mask);
-                word[j] = a.bloom + off + (h[j] & msk);
-                old[j] = __ldcg(word[j]);
+                uint32_t same;
+                if constexpr (NW == 1) same = __match_any_sync(active, it[j]);
+                else same = __match_any_sync(active, it[j].w0) & __match_any_sync(active, it[j].w1);
+                mult[j] = ((__ffs(same) - 1) == lane) ? (uint32_t)__popc(same) : 0u;
             }
         }
+
+        // one round trip: filter word + first table slot of every item
+        uint64_t h[ITEMS];
+        uint64_t old[ITEMS];
+        Seen seen[ITEMS];
 #pragma unroll
         for (int j = 0; j < ITEMS; ++j) {
             if (mult[j]) {
-                const uint64_t bits = bloom_bits(h[j]);
-                if ((old[j] & bits) != bits) {
-                    old[j] = atomicOr(reinterpret_cast<unsigned long long*>(word[j]), bits);
-                    if ((old[j] & bits) != bits) first_bits |= 1u << j;
+                h[j] = hash_key(it[j]);
+                const MetaS m = meta_of((uint32_t)(key_hi(it[j]) >> a.bucket_shift));
+                if (a.use_filter) old[j] = __ldcg(a.bloom + m.bloom_off + (h[j] & m.bloom_mask));
+                const S* slot = table + m.tab_off + ((h[j] >> 17) & m.tab_mask);
+                if constexpr (NW == 1) seen[j] = __ldcg(&slot->key);
+                else seen[j] = __ldcg(reinterpret_cast<const ulonglong2*>(slot));
+            }
+        }
+        uint32_t first_bits = 0;  // bit j: item j is a first occurrence
+        if (a.use_filter) {
+#pragma unroll
+            for (int j = 0; j < ITEMS; ++j) {
+                if (mult[j]) {
+                    const uint64_t bits = bloom_bits(h[j]);
+                    if ((old[j] & bits) != bits) {
+                        const MetaS m = meta_of((uint32_t)(key_hi(it[j]) >> a.bucket_shift));
+                        const uint64_t o = atomicOr(
+                            reinterpret_cast<unsigned long long*>(a.bloom + m.bloom_off + (h[j] & m.bloom_mask)), bits);
+                        if ((o & bits) != bits) first_bits |= 1u << j;
+                    }
                 }
             }
         }
-    } else {
+        uint32_t fail_bits = 0;
 #pragma unroll
         for (int j = 0; j < ITEMS; ++j) {
-            if (mult[j]) {
-                bucket[j] = (uint32_t)(key_hi(it[j]) >> a.bucket_shift);
-                h[j] = hash_key(it[j]);
+            const uint32_t reps = mult[j] - ((first_bits >> j) & 1u);
+            if (mult[j] && reps) {
+                const uint32_t b = (uint32_t)(key_hi(it[j]) >> a.bucket_shift);
+                const MetaS m = meta_of(b);
+                if (!table_add_first(table + m.tab_off, m.tab_mask, h[j], it[j], reps, seen[j])) {
+                    fail_bits |= 1u << j;
+                    mult[j] = reps;  // keep the count that still has to be added
+                    a.bucket_overflow[b] = 1u;
+                }
             }
         }
-    }
 
-    // repeat occurrences -> tables: all first-probe reads in flight, then resolve
-    using Seen = typename std::conditional<NW == 1, uint64_t, ulonglong2>::type;
-    Seen seen[ITEMS];
-    S* tabp[ITEMS];
-    uint64_t tmask[ITEMS];
+        // in-place compaction inside the warp's segment
+        uint32_t n_low = 0, n_fail = 0;
 #pragma unroll
-    for (int j = 0; j < ITEMS; ++j) {
-        const uint32_t reps = mult[j] - ((first_bits >> j) & 1u);
-        if (mult[j] && reps) {
-            tabp[j] = reinterpret_cast<S*>(a.table) + __ldg(&a.meta[bucket[j]].tab_off);
-            tmask[j] = __ldg(&a.meta[bucket[j]].tab_mask);
-            const S* slot = tabp[j] + ((h[j] >> 17) & tmask[j]);
-            if constexpr (NW == 1) seen[j] = __ldcg(&slot->key);
-            else seen[j] = __ldcg(reinterpret_cast<const ulonglong2*>(slot));
+        for (int j = 0; j < ITEMS; ++j) {
+            const bool first = (first_bits >> j) & 1u;
+            const uint32_t lm = __ballot_sync(0xffffffffu, first);
+            if (first) keys[s0 + n_low + __popc(lm & lt)] = it[j];
+            n_low += __popc(lm);
         }
-    }
-    uint32_t fails[ITEMS];
+        if (__any_sync(0xffffffffu, fail_bits != 0)) {
 #pragma unroll
-    for (int j = 0; j < ITEMS; ++j) {
-        fails[j] = 0;
-        const uint32_t reps = mult[j] - ((first_bits >> j) & 1u);
-        if (mult[j] && reps) {
-            if (!table_add(tabp[j], tmask[j], h[j], it[j], reps, &seen[j])) {
-                fails[j] = reps;
-                a.bucket_overflow[bucket[j]] = 1u;
+            for (int j = 0; j < ITEMS; ++j) {
+                const uint32_t f = ((fail_bits >> j) & 1u) ? mult[j] : 0u;
+                uint32_t fsum = f;
+#pragma unroll
+                for (int o = 1; o < 32; o <<= 1) {
+                    const uint32_t y = __shfl_up_sync(0xffffffffu, fsum, o);
+                    if (lane >= o) fsum += y;
+                }
+                const uint32_t wtot = __shfl_sync(0xffffffffu, fsum, 31);
+                const uint32_t my0 = n_fail + fsum - f;
+                for (uint32_t r = 0; r < f; ++r) keys[s_end - 1 - (my0 + r)] = it[j];
+                n_fail += wtot;
             }
         }
-    }
-
-    // in-place compaction inside the warp's segment
-    uint32_t n_low = 0, n_fail = 0;
-    const uint32_t lt = (1u << lane) - 1u;
-#pragma unroll
-    for (int j = 0; j < ITEMS; ++j) {
-        const bool first = (first_bits >> j) & 1u;
-        const uint32_t lm = __ballot_sync(0xffffffffu, first);
-        if (first) keys[s0 + n_low + __popc(lm & lt)] = it[j];
-        n_low += __popc(lm);
-        uint32_t fsum = fails[j];
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const uint32_t y = __shfl_up_sync(0xffffffffu, fsum, o);
-            if (lane >= o) fsum += y;
+        if (lane == 0) {
+            if (a.use_filter) a.seg_low[gw] = n_low;
+            a.seg_fail[gw] = n_fail;
         }
-        const uint32_t wtot = __shfl_sync(0xffffffffu, fsum, 31);
-        if (wtot) {
-            const uint32_t my0 = n_fail + fsum - fails[j];
-            for (uint32_t r = 0; r < fails[j]; ++r) keys[s_end - 1 - (my0 + r)] = it[j];
-            n_fail += wtot;
-        }
-    }
-    if (lane == 0) {
-        if (a.use_filter) a.seg_low[gw] = n_low;
-        a.seg_fail[gw] = n_fail;
     }
 }
 

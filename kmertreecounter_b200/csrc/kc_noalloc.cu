@@ -114,8 +114,7 @@ int run(const kc_config* g, const uint8_t* d_fastq, uint64_t n, uint8_t* d_low, 
     ea.bucket_count = bcount;
     ea.bucket_cursor = bcursor;
     ea.error = reinterpret_cast<uint32_t*>(scal + 8);
-    const size_t smem = (size_t)NB * 16;
-    if (tiles) kc::extract_kernel<NW, kc::HIST><<<tiles, kc::EXT_THREADS, smem, st>>>(ea);
+    if (tiles) kc::extract_kernel<NW, kc::HIST><<<tiles, kc::EXT_THREADS, kc::extract_smem_bytes<NW, kc::HIST>(NB), st>>>(ea);
     NK(cudaGetLastError());
     uint64_t h_count[NB];
     NK(cudaMemcpyAsync(h_count, bcount, sizeof h_count, cudaMemcpyDeviceToHost, st));
@@ -160,7 +159,10 @@ int run(const kc_config* g, const uint8_t* d_fastq, uint64_t n, uint8_t* d_low, 
     kc::init_slots<NW><<<256, 256, 0, st>>>(table, ts);
     NK(cudaMemcpyAsync(bcursor, start, sizeof start, cudaMemcpyHostToDevice, st));
     ea.routed = routed;
-    if (tiles) kc::extract_kernel<NW, kc::SCATTER><<<tiles, kc::EXT_THREADS, smem, st>>>(ea);
+    // the scatter's staging area needs more than the default 48 KiB
+    const size_t smem_sc = kc::extract_smem_bytes<NW, kc::SCATTER>(NB);
+    NK(cudaFuncSetAttribute(kc::extract_kernel<NW, kc::SCATTER>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_sc));
+    if (tiles) kc::extract_kernel<NW, kc::SCATTER><<<tiles, kc::EXT_THREADS, smem_sc, st>>>(ea);
 
     kc::CountArgs ca{};
     ca.routed = routed;
@@ -172,8 +174,10 @@ int run(const kc_config* g, const uint8_t* d_fastq, uint64_t n, uint8_t* d_low, 
     ca.seg_fail = seg_fail;
     ca.bucket_overflow = overflow;
     ca.bucket_shift = SHIFT;
+    ca.n_buckets = NB;
     ca.use_filter = 1;
-    if (ctiles) kc::count_routed<NW><<<ctiles, kc::CNT_THREADS, 0, st>>>(ca);
+    const uint64_t cgrid = cdiv(K, (uint64_t)CT * kc::CNT_SEGS_PER_WARP);
+    if (cgrid) kc::count_routed<NW><<<cgrid, kc::CNT_THREADS, 0, st>>>(ca);
     NK(cudaGetLastError());
 
     // overflow: grow the bucket's table inside the arena, move, retry
@@ -206,7 +210,7 @@ int run(const kc_config* g, const uint8_t* d_fastq, uint64_t n, uint8_t* d_low, 
         }
         NK(cudaMemcpyAsync(meta, h_meta, sizeof h_meta, cudaMemcpyHostToDevice, st));
         ca.use_filter = 0;
-        kc::count_routed<NW><<<ctiles, kc::CNT_THREADS, 0, st>>>(ca);
+        kc::count_routed<NW><<<cgrid, kc::CNT_THREADS, 0, st>>>(ca);
         NK(cudaGetLastError());
     }
 

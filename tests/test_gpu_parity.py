@@ -136,3 +136,76 @@ def test_cli_output_read_by_reference_tool(golden, tmp_path):
         subprocess.run([oracle.REF_HIST, "precise", str(tmp_path / "tmp"), "33", "4", "4", str(h), "1", "64"],
                        check=True, capture_output=True)
         assert [int(line.split("\t")[1]) for line in h.read_text().splitlines()] == g["histogram_tool_precise_1_64"]
+
+
+@pytest.mark.parametrize("k", [21, 31, 32, 45, 63, 64])
+def test_sorted_roots(k):
+    """sort_output=1: every root file ordered by key (radix sort replacing
+    sort/ExportRecordRadixSort.h), same records as unsorted."""
+    p = synth.plain_small(seed=60 + k, scale=0.08)
+    data = synth.fastq(p)
+    with kc.Counter(k=k, sort_output=1) as c:
+        c.count_host(data)
+        low, roots = parity.check_exact(c, data, k)
+        _, _, per_root = c.sizes()
+    nw = oracle.words(k)
+    rk = roots["key"].reshape(-1, nw)
+    off = 0
+    for n in per_root:
+        seg = rk[off:off + n]
+        if n > 1:
+            order = np.lexsort(tuple(seg[:, i] for i in range(nw - 1, -1, -1)))
+            assert np.array_equal(order, np.arange(n)), "root file not sorted by key"
+        off += n
+
+
+@pytest.mark.parametrize("batch", [1 << 20, 4 << 20, 1 << 30])
+def test_stream_sink_matches(golden, batch):
+    """kc_count_host_stream: low.bin bytes and root files delivered through
+    the sink (copies overlapped with counting) give the exact multiset."""
+    import ctypes
+    data = golden_input(golden, "adversarial")
+    k = 31
+    low_parts, roots = [], {}
+
+    def sink(kind, root, addr, nbytes):
+        buf = ctypes.string_at(addr, nbytes) if nbytes else b""
+        if kind == kc.KC_SINK_LOW:
+            low_parts.append(buf)
+        else:
+            roots.setdefault(root, []).append(buf)
+        return 0
+
+    with kc.Counter(k=k, batch_bytes=batch, chunk_bytes=1 << 20) as c:
+        st = c.count_host_stream(data.ctypes.data, data.size, sink)
+    assert sorted(roots) == list(range(256)), "every root delivered, in order"
+    low = oracle.unpack(np.frombuffer(b"".join(low_parts), np.uint8), k)
+    dt = kc.record_dtype(k)
+    per_root = [sum(len(b) for b in roots[r]) // dt.itemsize for r in range(256)]
+    rec = np.frombuffer(b"".join(b"".join(roots[r]) for r in range(256)), dtype=dt)
+    parity.check_layout(low, rec, per_root, k)
+    mk, mc = parity.merged(low, rec, k)
+    g = golden["adversarial"]["k"][str(k)]
+    assert st.total_kmers == g["K"] and oracle.digest(mk, mc) == g["digest"]
+
+
+def test_gzip_input_cli(golden, tmp_path):
+    """gzip input is detected by its magic bytes (src/FastqReader.h:93-104)."""
+    import gzip
+    data = golden_input(golden, "plain_small_s7")
+    fq = tmp_path / "in.fastq.gz"
+    with gzip.open(fq, "wb", compresslevel=1) as f:
+        f.write(data.tobytes())
+    tree = os.path.join(ROOT, "kmertreecounter_b200", "bin", "Tree")
+    p = subprocess.run([tree, str(fq), "21", "8", "4"], cwd=tmp_path, capture_output=True, text=True)
+    assert p.returncode == 0, p.stderr
+    low, roots, _ = oracle.read_outputs(str(tmp_path / "tmp"), 21)
+    mk, mc = oracle.merged_counts(low, roots["key"], roots["count"])
+    assert oracle.digest(mk, mc) == golden["plain_small_s7"]["k"]["21"]["digest"]
+
+
+def test_cli_missing_input_is_io_error(tmp_path):
+    tree = os.path.join(ROOT, "kmertreecounter_b200", "bin", "Tree")
+    p = subprocess.run([tree, str(tmp_path / "nope.fastq"), "31", "8", "4"], cwd=tmp_path, capture_output=True,
+                       text=True)
+    assert p.returncode == 255 and "Failed to open" in p.stderr
