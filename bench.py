@@ -8,8 +8,8 @@ low.bin packing and root-record export, all on the device.
 
   value   FASTQ resident in HBM, outputs left in HBM (kc_count_device)
   e2e     the C ABI on HOST buffers: pinned FASTQ -> H2D -> count -> packed
-          low.bin + root records copied back into pinned host buffers
-          (kc_count_host + kc_copy_low + kc_copy_roots)
+          low.bin bytes and root records delivered to host memory through the
+          streaming call (kc_count_host_stream), copies overlapped with counting
 
 `--impl reference` times the reference's own CPU implementation (the `Tree`
 binary built from the reference sources into oracle/_ref, else the oracle
@@ -168,6 +168,21 @@ def time_reference(path, data, k, bases, runs, workdir):
     return out, kind, cores
 
 
+def profile_traffic(args):
+    """DRAM bytes (read + write) of count_routed per step from the committed
+    ncu summary of this workload (profiles/count_routed_genome_scale.md)."""
+    if args.workload != "genome_scale" or args.scale != 1.0:
+        return None
+    try:
+        with open(os.path.join(ROOT, "profiles", "count_routed_genome_scale.md")) as f:
+            for line in f:
+                if line.startswith("traffic_bytes_per_step:"):
+                    return int(line.split(":")[1])
+    except OSError:
+        pass
+    return None
+
+
 # --------------------------------------------------------------- our arm
 
 def run_ours(args):
@@ -231,6 +246,7 @@ def run_ours(args):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         total_ms = float(t.item())
     ms_step = total_ms / args.steps
+    _, distinct = counter.histogram(1, 2)  # exact distinct keys (outside the timed region)
     stats = st.as_dict()
     stats.pop("root_counts", None)
     gpu_launches = int(sum(stage_launch.values()))
@@ -296,7 +312,8 @@ def run_ours(args):
                    if args.workload == "genome_scale" and args.scale == 1.0 else f"{args.workload} scale={args.scale}",
                    "k": k, "n_buckets": buckets, "fastq_bytes": n, "bases": bases, "reads": int(p.n_reads),
                    "l2": "inputs larger than L2 (FASTQ %.1f GB)" % (n / 1e9), "parallelism": f"replica x{world}"},
-        "distinct_kmers_per_s": None,
+        "distinct_kmers": distinct,
+        "distinct_kmers_per_s": distinct * world / (ms_step / 1e3),
         "stats": stats,
         "stages_ms_per_step": {s: v / args.steps for s, v in stage_ms.items()},
         "gpu_launches": gpu_launches,
@@ -304,7 +321,8 @@ def run_ours(args):
                 "h2d_bytes_per_step": n, "d2h_bytes_per_step": lb + nr * rec},
         "roofline": {"bound": "hbm", "kernel": "count_routed", "achieved": achieved, "peak": pk["hbm_gbs"],
                      "unit": "GB/s", "frac": (achieved / pk["hbm_gbs"]) if achieved else None,
-                     "peak_source": pk["source"], "alg_bytes_per_launch": alg_bytes, "traffic": None,
+                     "peak_source": pk["source"], "alg_bytes_per_launch": alg_bytes,
+                     "traffic": profile_traffic(args), "per": "step (all count_routed launches of one count)",
                      "dominant_stage": dominant},
         "clocks": clk,
     }

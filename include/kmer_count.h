@@ -147,6 +147,14 @@ int kc_copy_low(kc_context* ctx, uint8_t* dst, uint64_t cap);
  * order) into dst (cap bytes). */
 int kc_copy_roots(kc_context* ctx, uint8_t* dst, uint64_t cap);
 
+/* Merged count histogram of the last device-held result (kc_count_host or
+ * kc_count_device): hist[i] = number of distinct keys whose exact count
+ * (root count + [key in low.bin]) equals min_freq + i, for i in
+ * 0..max_freq-min_freq; *distinct = number of distinct keys.  The device form
+ * of tool/histogram_tool.cpp "precise" (tool/HighFrequencyInsertThreadPool.h:
+ * 150-177, tool/LowFrequencyQueryThreadPool.h:375-432). */
+int kc_histogram(kc_context* ctx, uint32_t min_freq, uint32_t max_freq, uint64_t* hist, uint64_t* distinct);
+
 /* Write low.bin and root_0..255.bin of the last result into out_dir. */
 int kc_write_outputs(kc_context* ctx, const char* out_dir);
 

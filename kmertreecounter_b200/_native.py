@@ -29,6 +29,7 @@ ABI_SYMBOLS = (
     "kc_create", "kc_destroy", "kc_count_host", "kc_count_device", "kc_result_sizes", "kc_copy_low",
     "kc_copy_roots", "kc_write_outputs", "kc_device_results", "kc_host_alloc", "kc_host_free", "kc_stream",
     "kc_set_profiling", "kc_stage_times", "kc_stage_name", "kc_count_device_noalloc", "kc_count_host_stream",
+    "kc_histogram",
 )
 KC_SINK_LOW = 0
 KC_SINK_ROOT = 1
@@ -97,6 +98,7 @@ def _load():
         "kc_stage_name": (C.c_char_p, [i32]),
         "kc_count_device_noalloc": (i32, [cfgp, vp, u64, vp, u64, vp, u64, vp, stp]),
         "kc_count_host_stream": (i32, [vp, vp, u64, SINK_FN, vp, stp]),
+        "kc_histogram": (i32, [vp, u32, u32, C.POINTER(u64), C.POINTER(u64)]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -217,6 +219,14 @@ class Counter:
         out = np.empty(nr, dtype=dt)
         check(lib.kc_copy_roots(self._ctx, out.ctypes.data if nr else None, nr * dt.itemsize))
         return out, counts
+
+    def histogram(self, min_freq=1, max_freq=10000):
+        """(hist array for freq min..max, distinct keys) of the last result."""
+        n = max_freq - min_freq + 1
+        h = (C.c_uint64 * n)()
+        d = C.c_uint64()
+        check(lib.kc_histogram(self._ctx, min_freq, max_freq, h, C.byref(d)))
+        return np.array(h, dtype=np.uint64), d.value
 
     def set_profiling(self, on=True):
         check(lib.kc_set_profiling(self._ctx, 1 if on else 0))

@@ -959,6 +959,51 @@ int kc_count_host_stream(kc_context* c, const uint8_t* fastq, uint64_t n, kc_sin
     return KC_OK;
 }
 
+// Merged count histogram and distinct keys of the last device-held result.
+int kc_histogram(kc_context* c, uint32_t min_freq, uint32_t max_freq, uint64_t* hist, uint64_t* distinct) {
+    if (!c) return fail(KC_ERR_INVALID, "null context");
+    if (!c->have_result) return fail(KC_ERR_STATE, "no result: run a count first");
+    if (c->stream_low) return fail(KC_ERR_STATE, "streamed results are not kept on the device");
+    if (max_freq < min_freq || min_freq == 0) return fail(KC_ERR_INVALID, "need 1 <= min_freq <= max_freq");
+    const uint64_t bins = (uint64_t)max_freq - min_freq + 1;
+    if (bins > (1ull << 26)) return fail(KC_ERR_INVALID, "histogram range too large");
+    DevBuf gh;
+    CK(gh.ensure((bins + 1) * sizeof(unsigned long long)));
+    unsigned long long* d = gh.as<unsigned long long>();
+    CK(cudaMemsetAsync(d, 0, (bins + 1) * sizeof(unsigned long long), c->stream));
+    const int grid = c->sm_count * 8;
+    const uint64_t slots = c->table_slots_used;
+    if (c->nw == 1) {
+        kc::hist_clear_marks<1><<<grid, 256, 0, c->stream>>>(c->table.p, slots);
+        kc::hist_low_pass<1><<<grid, 256, 0, c->stream>>>(c->low_packed.as<uint8_t>(), c->low_total, c->cfg.k,
+                                                          c->meta.as<kc::BucketMeta>(), c->bucket_shift, c->table.p,
+                                                          min_freq, max_freq, d);
+    } else {
+        kc::hist_clear_marks<2><<<grid, 256, 0, c->stream>>>(c->table.p, slots);
+        kc::hist_low_pass<2><<<grid, 256, 0, c->stream>>>(c->low_packed.as<uint8_t>(), c->low_total, c->cfg.k,
+                                                          c->meta.as<kc::BucketMeta>(), c->bucket_shift, c->table.p,
+                                                          min_freq, max_freq, d);
+    }
+    // only slots that belong to a live bucket table (regions left by a rehash
+    // are stale copies) -- walk each bucket's region
+    for (uint32_t b = 0; b < c->n_buckets; ++b) {
+        const uint64_t n = c->h_meta[b].tab_mask + 1;
+        uint8_t* t = c->table.as<uint8_t>() + c->h_meta[b].tab_off * c->slot_bytes;
+        const int g = (int)std::min<uint64_t>(grid, ceil_div(n, 256));
+        if (c->nw == 1) kc::hist_table_pass<1><<<g, 256, 0, c->stream>>>(t, n, min_freq, max_freq, d, d + bins);
+        else kc::hist_table_pass<2><<<g, 256, 0, c->stream>>>(t, n, min_freq, max_freq, d, d + bins);
+    }
+    CK(cudaGetLastError());
+    std::vector<unsigned long long> h(bins + 1);
+    CK(cudaMemcpyAsync(h.data(), d, (bins + 1) * sizeof(unsigned long long), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    gh.release();
+    if (hist)
+        for (uint64_t i = 0; i < bins; ++i) hist[i] = h[i];
+    if (distinct) *distinct = c->low_total + h[bins];
+    return KC_OK;
+}
+
 int kc_result_sizes(kc_context* c, uint64_t* low_bytes, uint64_t* n_root, uint64_t* root_counts) {
     if (!c) return fail(KC_ERR_INVALID, "null context");
     if (!c->have_result) return fail(KC_ERR_STATE, "no result: run a count first");

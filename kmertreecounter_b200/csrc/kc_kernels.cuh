@@ -1062,4 +1062,129 @@ __global__ void export_write(const void* table, const ExportChunk* chunks, uint6
     }
 }
 
+// ------------------------------------------------------ merged histogram
+//
+// Device form of tool/histogram_tool.cpp "precise"
+// (tool/HighFrequencyInsertThreadPool.h:150-177,
+// tool/LowFrequencyQueryThreadPool.h:375-432): exact count of a key = its
+// table count + [key in low.bin].  Pass 1 walks the packed low.bin keys,
+// looks each up in its bucket's table, marks the slot (pad field) and adds
+// count+1 (or 1) to the histogram; pass 2 adds every unmarked table key with
+// its table count.  Histogram bins are aggregated per CTA in shared memory
+// (HIST_SMEM bins; larger counts go straight to global atomics).
+
+constexpr int HIST_SMEM = 1024;
+
+template <int NW>
+__device__ __forceinline__ bool table_find(const typename SlotOf<NW>::T* tab, uint64_t mask, uint64_t h,
+                                           const typename KeyOf<NW>::T& key, uint64_t* where) {
+    const uint64_t i0 = (h >> 17) & mask;
+    for (uint64_t p = 0; p <= mask; ++p) {
+        const uint64_t i = (i0 + p) & mask;
+        const typename SlotOf<NW>::T& s = tab[i];
+        bool empty, eq;
+        if constexpr (NW == 1) {
+            empty = s.key == EMPTY;
+            eq = s.key == key;
+        } else {
+            empty = s.w0 == EMPTY && s.w1 == EMPTY;
+            eq = s.w0 == key.w0 && s.w1 == key.w1;
+        }
+        if (eq) {
+            *where = i;
+            return true;
+        }
+        if (empty) return false;
+    }
+    return false;
+}
+
+__device__ __forceinline__ void hist_add(uint32_t* sh, unsigned long long* gh, uint64_t merged, uint32_t lo,
+                                         uint32_t hi) {
+    if (merged < lo || merged > hi) return;
+    const uint64_t bin = merged - lo;
+    if (bin < HIST_SMEM) atomicAdd(sh + bin, 1u);
+    else atomicAdd(gh + bin, 1ull);
+}
+
+template <int NW>
+__global__ void hist_clear_marks(void* table, uint64_t n_slots) {
+    using S = typename SlotOf<NW>::T;
+    S* t = reinterpret_cast<S*>(table);
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n_slots; i += (uint64_t)gridDim.x * blockDim.x) {
+        if constexpr (NW == 1) t[i].pad = 0;
+        else t[i].pad[0] = 0;
+    }
+}
+
+template <int NW>
+__global__ void hist_low_pass(const uint8_t* low, uint64_t n_low, uint32_t k, const BucketMeta* meta,
+                              uint32_t bucket_shift, void* table, uint32_t lo, uint32_t hi,
+                              unsigned long long* gh) {
+    using K = typename KeyOf<NW>::T;
+    using S = typename SlotOf<NW>::T;
+    __shared__ uint32_t sh[HIST_SMEM];
+    for (int i = threadIdx.x; i < HIST_SMEM; i += blockDim.x) sh[i] = 0;
+    __syncthreads();
+    const uint32_t full = k / 32, tail_bits = 2 * (k % 32), tail_bytes = (tail_bits + 7) / 8;
+    const uint32_t P = full * 8 + tail_bytes;
+    for (uint64_t r = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; r < n_low; r += (uint64_t)gridDim.x * blockDim.x) {
+        const uint8_t* p = low + r * P;
+        uint64_t w[2] = {0, 0};
+        for (uint32_t f = 0; f < full; ++f)
+            for (uint32_t b = 0; b < 8; ++b) w[f] |= (uint64_t)p[8 * f + b] << (8 * b);
+        for (uint32_t b = 0; b < tail_bytes; ++b) w[full] |= (uint64_t)p[8 * full + b] << (8 * (8 - tail_bytes + b));
+        K key;
+        if constexpr (NW == 1) key = w[0];
+        else key = Key2{w[0], w[1]};
+        const BucketMeta m = meta[key_hi(key) >> bucket_shift];
+        S* tab = reinterpret_cast<S*>(table) + m.tab_off;
+        uint64_t at;
+        uint64_t merged = 1;
+        if (table_find<NW>(tab, m.tab_mask, hash_key(key), key, &at)) {
+            merged = (uint64_t)tab[at].count + 1;
+            if constexpr (NW == 1) tab[at].pad = 1;
+            else tab[at].pad[0] = 1;
+        }
+        hist_add(sh, gh, merged, lo, hi);
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < HIST_SMEM; i += blockDim.x)
+        if (sh[i]) atomicAdd(gh + i, (unsigned long long)sh[i]);
+}
+
+template <int NW>
+__global__ void hist_table_pass(const void* table, uint64_t n_slots, uint32_t lo, uint32_t hi, unsigned long long* gh,
+                                unsigned long long* unmarked) {
+    using S = typename SlotOf<NW>::T;
+    __shared__ uint32_t sh[HIST_SMEM];
+    __shared__ unsigned long long s_un;
+    for (int i = threadIdx.x; i < HIST_SMEM; i += blockDim.x) sh[i] = 0;
+    if (threadIdx.x == 0) s_un = 0;
+    __syncthreads();
+    const S* t = reinterpret_cast<const S*>(table);
+    uint32_t un = 0;
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n_slots; i += (uint64_t)gridDim.x * blockDim.x) {
+        const S s = t[i];
+        bool used, marked;
+        if constexpr (NW == 1) {
+            used = s.key != EMPTY;
+            marked = s.pad != 0;
+        } else {
+            used = !(s.w0 == EMPTY && s.w1 == EMPTY);
+            marked = s.pad[0] != 0;
+        }
+        if (used && !marked) {
+            ++un;
+            hist_add(sh, gh, s.count, lo, hi);
+        }
+    }
+    for (int o = 16; o; o >>= 1) un += __shfl_xor_sync(0xffffffffu, un, o);
+    if ((threadIdx.x & 31) == 0 && un) atomicAdd(&s_un, (unsigned long long)un);
+    __syncthreads();
+    for (int i = threadIdx.x; i < HIST_SMEM; i += blockDim.x)
+        if (sh[i]) atomicAdd(gh + i, (unsigned long long)sh[i]);
+    if (threadIdx.x == 0 && s_un) atomicAdd(unmarked, s_un);
+}
+
 }  // namespace kc

@@ -209,3 +209,18 @@ def test_cli_missing_input_is_io_error(tmp_path):
     p = subprocess.run([tree, str(tmp_path / "nope.fastq"), "31", "8", "4"], cwd=tmp_path, capture_output=True,
                        text=True)
     assert p.returncode == 255 and "Failed to open" in p.stderr
+
+
+@pytest.mark.parametrize("name,k", [("plain_small", 31), ("adversarial", 33), ("plain_small_s7", 63)])
+def test_device_histogram(golden, name, k):
+    """kc_histogram (device form of histogram_tool precise) reproduces the
+    reference's histogram and the distinct count."""
+    g = golden[name]["k"][str(k)]
+    data = golden_input(golden, name)
+    with kc.Counter(k=k, repeat_ratio=0.01) as c:  # small tables: exercises rehash + stale regions
+        c.count_host(data)
+        h, distinct = c.histogram(1, 64)
+        assert [int(x) for x in h] == g["histogram_tool_precise_1_64"]
+        assert distinct == g["D"]
+        h2, _ = c.histogram(3, 5)  # a second call reuses cleared marks
+        assert [int(x) for x in h2] == g["histogram_tool_precise_1_64"][2:5]
