@@ -16,6 +16,7 @@
 #include <algorithm>
 #include <bit>
 #include <chrono>
+#include <cmath>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
@@ -25,6 +26,7 @@
 #include <cuda_runtime.h>
 
 #include "../../include/kmer_count.h"
+#include "../../include/kmer_sizing.h"
 #include "kc_internal.h"
 #include "kc_kernels.cuh"
 #include "kc_scan.cuh"
@@ -173,7 +175,7 @@ struct kc_context {
     uint64_t root_counts[256] = {};
 
     // optional learned sizing hook (per-bucket repeat-key predictions)
-    std::vector<double> predicted_repeat_keys;
+    std::vector<double> pred_distinct, pred_table;  // learned sizing, per model bucket (4096)
 
     // stage profiling: CUDA event pairs recorded on `stream` around each stage
     bool profiling = false;
@@ -258,12 +260,25 @@ int size_structures(kc_context* c, const std::vector<uint64_t>& kb, double scale
     const uint32_t nb = c->n_buckets;
     c->h_meta.assign(nb, kc::BucketMeta{});
     uint64_t bw = 0, ts = 0;
-    const bool learned = g.sizing == KC_SIZING_LEARNED && c->predicted_repeat_keys.size() == nb;
+    const bool learned = g.sizing == KC_SIZING_LEARNED && c->pred_table.size() == KC_MODEL_BUCKETS;
+    const uint32_t per = KC_MODEL_BUCKETS / nb;  // model buckets per engine bucket (16 or 1)
     for (uint32_t b = 0; b < nb; ++b) {
         const double kest = (double)kb[b] * scale;
-        const uint64_t words = pow2_at_least(std::max<uint64_t>((uint64_t)(kest * g.bloom_bits / 64.0), 256));
-        double rep = learned ? c->predicted_repeat_keys[b] : kest * g.repeat_ratio;
-        const uint64_t slots = pow2_at_least(std::max<uint64_t>((uint64_t)(rep / g.table_load), 256));
+        uint64_t words, slots;
+        if (learned) {
+            // filter: 12 bits per predicted distinct key; table: predicted
+            // table keys with 15% headroom at the target load
+            double d = 0, t = 0;
+            for (uint32_t q = 0; q < per; ++q) {
+                d += c->pred_distinct[b * per + q];
+                t += c->pred_table[b * per + q];
+            }
+            words = pow2_at_least(std::max<uint64_t>((uint64_t)(d * 12.0 / 64.0), 256));
+            slots = pow2_at_least(std::max<uint64_t>((uint64_t)(t * 1.15 / g.table_load), 256));
+        } else {
+            words = pow2_at_least(std::max<uint64_t>((uint64_t)(kest * g.bloom_bits / 64.0), 256));
+            slots = pow2_at_least(std::max<uint64_t>((uint64_t)(kest * g.repeat_ratio / g.table_load), 256));
+        }
         c->h_meta[b].bloom_off = bw;
         c->h_meta[b].bloom_mask = words - 1;
         c->h_meta[b].tab_off = ts;
@@ -1065,16 +1080,61 @@ void kc_host_free(void* p) {
 
 }  // extern "C"
 
-// Internal hook for the learned sizing model: per-bucket predicted distinct
-// repeat keys for the next count on this context.
-int kc_internal_set_predictions(kc_context* c, const double* per_bucket, uint32_t n) {
-    if (!c) return KC_ERR_INVALID;
-    if (!per_bucket || n == 0) {
-        c->predicted_repeat_keys.clear();
+extern "C" int kc_set_predicted_loads(kc_context* c, const double* distinct, const double* table_keys) {
+    if (!c) return fail(KC_ERR_INVALID, "null context");
+    if (!distinct || !table_keys) {
+        c->pred_distinct.clear();
+        c->pred_table.clear();
         return KC_OK;
     }
-    if (n != c->n_buckets) return fail(KC_ERR_INVALID, "prediction count %u != n_buckets %u", n, c->n_buckets);
-    c->predicted_repeat_keys.assign(per_bucket, per_bucket + n);
+    for (int i = 0; i < KC_MODEL_BUCKETS; ++i)
+        if (!(distinct[i] >= 0.0) || !(table_keys[i] >= 0.0) || !std::isfinite(distinct[i]) ||
+            !std::isfinite(table_keys[i]))
+            return fail(KC_ERR_INVALID, "predicted loads must be finite and non-negative");
+    c->pred_distinct.assign(distinct, distinct + KC_MODEL_BUCKETS);
+    c->pred_table.assign(table_keys, table_keys + KC_MODEL_BUCKETS);
+    return KC_OK;
+}
+
+extern "C" int kc_bucket_loads(kc_context* c, uint64_t* distinct, uint64_t* table_keys, uint64_t* kmers) {
+    if (!c) return fail(KC_ERR_INVALID, "null context");
+    if (!c->have_result) return fail(KC_ERR_STATE, "no result: run a count first");
+    if (c->stream_low) return fail(KC_ERR_STATE, "streamed results are not kept on the device");
+    DevBuf d;
+    CK(d.ensure(3 * KC_MODEL_BUCKETS * sizeof(unsigned long long)));
+    unsigned long long* dd = d.as<unsigned long long>();
+    CK(cudaMemsetAsync(dd, 0, 3 * KC_MODEL_BUCKETS * sizeof(unsigned long long), c->stream));
+    const int grid = c->sm_count * 8;
+    if (c->nw == 1) {
+        kc::hist_clear_marks<1><<<grid, 256, 0, c->stream>>>(c->table.p, c->table_slots_used);
+        kc::loads_low_pass<1><<<grid, 256, 0, c->stream>>>(c->low_packed.as<uint8_t>(), c->low_total, c->cfg.k,
+                                                           c->meta.as<kc::BucketMeta>(), c->bucket_shift, c->table.p,
+                                                           dd, dd + 2 * KC_MODEL_BUCKETS);
+    } else {
+        kc::hist_clear_marks<2><<<grid, 256, 0, c->stream>>>(c->table.p, c->table_slots_used);
+        kc::loads_low_pass<2><<<grid, 256, 0, c->stream>>>(c->low_packed.as<uint8_t>(), c->low_total, c->cfg.k,
+                                                           c->meta.as<kc::BucketMeta>(), c->bucket_shift, c->table.p,
+                                                           dd, dd + 2 * KC_MODEL_BUCKETS);
+    }
+    for (uint32_t b = 0; b < c->n_buckets; ++b) {
+        const uint64_t n = c->h_meta[b].tab_mask + 1;
+        uint8_t* t = c->table.as<uint8_t>() + c->h_meta[b].tab_off * c->slot_bytes;
+        const int g = (int)std::min<uint64_t>(grid, ceil_div(n, 256));
+        if (c->nw == 1)
+            kc::loads_table_pass<1><<<g, 256, 0, c->stream>>>(t, n, dd, dd + KC_MODEL_BUCKETS, dd + 2 * KC_MODEL_BUCKETS);
+        else
+            kc::loads_table_pass<2><<<g, 256, 0, c->stream>>>(t, n, dd, dd + KC_MODEL_BUCKETS, dd + 2 * KC_MODEL_BUCKETS);
+    }
+    CK(cudaGetLastError());
+    std::vector<unsigned long long> h(3 * KC_MODEL_BUCKETS);
+    CK(cudaMemcpyAsync(h.data(), dd, h.size() * sizeof(unsigned long long), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    d.release();
+    for (int i = 0; i < KC_MODEL_BUCKETS; ++i) {
+        if (distinct) distinct[i] = h[i];
+        if (table_keys) table_keys[i] = h[KC_MODEL_BUCKETS + i];
+        if (kmers) kmers[i] = h[2 * KC_MODEL_BUCKETS + i];
+    }
     return KC_OK;
 }
 

@@ -23,6 +23,5 @@ int kc_sort_roots(void* records, uint64_t n, uint64_t record_bytes, uint32_t k, 
                   cudaStream_t stream);
 const char* kc_sort_error();
 
-int kc_internal_set_predictions(kc_context* c, const double* per_bucket, uint32_t n);
 int kc_internal_set_error(int code, const char* msg);
 uint64_t kc_internal_record_bytes(const kc_context* c);

@@ -1187,4 +1187,65 @@ __global__ void hist_table_pass(const void* table, uint64_t n_slots, uint32_t lo
     if (threadIdx.x == 0 && s_un) atomicAdd(unmarked, s_un);
 }
 
+// Per model bucket (key word 0 >> 52) loads of the last result: low keys,
+// looked up in their table (marked as in hist_low_pass), then every table
+// key.  distinct = low keys + unmarked table keys; kmers = occurrences.
+template <int NW>
+__global__ void loads_low_pass(const uint8_t* low, uint64_t n_low, uint32_t k, const BucketMeta* meta,
+                               uint32_t bucket_shift, void* table, unsigned long long* distinct,
+                               unsigned long long* kmers) {
+    using K = typename KeyOf<NW>::T;
+    using S = typename SlotOf<NW>::T;
+    const uint32_t full = k / 32, tail_bits = 2 * (k % 32), tail_bytes = (tail_bits + 7) / 8;
+    const uint32_t P = full * 8 + tail_bytes;
+    for (uint64_t r = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; r < n_low; r += (uint64_t)gridDim.x * blockDim.x) {
+        const uint8_t* p = low + r * P;
+        uint64_t w[2] = {0, 0};
+        for (uint32_t f = 0; f < full; ++f)
+            for (uint32_t b = 0; b < 8; ++b) w[f] |= (uint64_t)p[8 * f + b] << (8 * b);
+        for (uint32_t b = 0; b < tail_bytes; ++b) w[full] |= (uint64_t)p[8 * full + b] << (8 * (8 - tail_bytes + b));
+        K key;
+        if constexpr (NW == 1) key = w[0];
+        else key = Key2{w[0], w[1]};
+        const BucketMeta m = meta[key_hi(key) >> bucket_shift];
+        S* tab = reinterpret_cast<S*>(table) + m.tab_off;
+        uint64_t at;
+        unsigned long long occ = 1;
+        if (table_find<NW>(tab, m.tab_mask, hash_key(key), key, &at)) {
+            occ += tab[at].count;
+            if constexpr (NW == 1) tab[at].pad = 1;
+            else tab[at].pad[0] = 1;
+        }
+        atomicAdd(distinct + (key_hi(key) >> 52), 1ull);
+        atomicAdd(kmers + (key_hi(key) >> 52), occ);
+    }
+}
+
+template <int NW>
+__global__ void loads_table_pass(const void* table, uint64_t n_slots, unsigned long long* distinct,
+                                 unsigned long long* tkeys, unsigned long long* kmers) {
+    using S = typename SlotOf<NW>::T;
+    const S* t = reinterpret_cast<const S*>(table);
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n_slots; i += (uint64_t)gridDim.x * blockDim.x) {
+        const S s = t[i];
+        uint64_t hi;
+        bool used, marked;
+        if constexpr (NW == 1) {
+            used = s.key != EMPTY;
+            marked = s.pad != 0;
+            hi = s.key;
+        } else {
+            used = !(s.w0 == EMPTY && s.w1 == EMPTY);
+            marked = s.pad[0] != 0;
+            hi = s.w0;
+        }
+        if (!used) continue;
+        atomicAdd(tkeys + (hi >> 52), 1ull);
+        if (!marked) {
+            atomicAdd(distinct + (hi >> 52), 1ull);
+            atomicAdd(kmers + (hi >> 52), (unsigned long long)s.count);
+        }
+    }
+}
+
 }  // namespace kc

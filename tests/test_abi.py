@@ -11,7 +11,8 @@ from conftest import ROOT, has_cuda
 import kmertreecounter_b200 as kc
 from kmertreecounter_b200 import _native, synth
 
-HEADERS = {"kmer_count.h": _native.LIB_PATH, "kmer_synth.h": _native.SYNTH_PATH}
+HEADERS = {"kmer_count.h": _native.LIB_PATH, "kmer_synth.h": _native.SYNTH_PATH,
+           "kmer_sizing.h": _native.LIB_PATH}
 
 
 def declared(header):
