@@ -183,6 +183,42 @@ def profile_traffic(args):
     return None
 
 
+def compare_sizing(args, kc, torch, dev, n, host, k, buckets, st_sampled, ms_sampled):
+    """Learned vs sampled sizing on the same resident FASTQ: the sizing MLP
+    predicts per-bucket loads from the first 1% of the reads (prefix counted
+    on the GPU, network run by the library's kernels); the count then runs
+    with those sizes.  Device time per step, rehashes and structure memory for
+    both rules; counts are identical by construction (checked by histogram)."""
+    from kmertreecounter_b200 import sizing
+    if not os.path.exists(sizing.MODEL_PATH):
+        return None
+    model = sizing.MLP.load()
+    t0 = time.perf_counter()
+    pred = sizing.predict_loads(model, host, k, 150)
+    predict_ms = (time.perf_counter() - t0) * 1e3
+    cfg = kc.default_config(k=k, n_buckets=buckets, sizing=kc.KC_SIZING_LEARNED)
+    with kc.Counter(cfg) as c:
+        sizing.apply(c, pred)
+        c.count_device(dev.data_ptr(), n)
+        stream = torch.cuda.ExternalStream(c.stream)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.steps):
+            stl = c.count_device(dev.data_ptr(), n)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms_learned = e0.elapsed_time(e1) / args.steps
+        h_l, d_l = c.histogram(1, 1000)
+        l = dict(ms_per_step=ms_learned, rehashes=stl.rehashes, table_slots=stl.table_slots,
+                 filter_words=stl.filter_words, table_keys=stl.table_keys, predict_ms=predict_ms,
+                 predicted_table_keys=float(pred[1].sum()), distinct=int(d_l))
+    return {"sampled": dict(ms_per_step=ms_sampled, rehashes=st_sampled["rehashes"],
+                            table_slots=st_sampled["table_slots"], filter_words=st_sampled["filter_words"],
+                            table_keys=st_sampled["table_keys"]),
+            "learned": l}
+
+
 # --------------------------------------------------------------- our arm
 
 def run_ours(args):
@@ -247,6 +283,7 @@ def run_ours(args):
         total_ms = float(t.item())
     ms_step = total_ms / args.steps
     _, distinct = counter.histogram(1, 2)  # exact distinct keys (outside the timed region)
+    sizing_cmp = compare_sizing(args, kc, torch, dev, n, host, k, buckets, st.as_dict(), ms_step)
     stats = st.as_dict()
     stats.pop("root_counts", None)
     gpu_launches = int(sum(stage_launch.values()))
@@ -325,6 +362,7 @@ def run_ours(args):
                      "traffic": profile_traffic(args), "per": "step (all count_routed launches of one count)",
                      "dominant_stage": dominant},
         "clocks": clk,
+        "sizing": sizing_cmp,
     }
     del dev
     counter.close()

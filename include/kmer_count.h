@@ -83,6 +83,8 @@ typedef struct kc_stats {
     uint64_t root_counts[256];/* records per root file */
     double device_ms;         /* time spent in kernels and copies on the stream */
     double wall_ms;
+    uint64_t table_slots;     /* repeat-table slots in use at the end (after any growth) */
+    uint64_t filter_words;    /* 64-bit words of the first-occurrence filter */
 } kc_stats;
 
 typedef struct kc_context kc_context;

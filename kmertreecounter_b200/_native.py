@@ -53,7 +53,7 @@ class KcStats(C.Structure):
         ("input_bytes", C.c_uint64), ("total_kmers", C.c_uint64), ("low_records", C.c_uint64),
         ("root_records", C.c_uint64), ("table_keys", C.c_uint64), ("rehashes", C.c_uint64),
         ("batches", C.c_uint64), ("root_counts", C.c_uint64 * 256), ("device_ms", C.c_double),
-        ("wall_ms", C.c_double),
+        ("wall_ms", C.c_double), ("table_slots", C.c_uint64), ("filter_words", C.c_uint64),
     ]
 
     def as_dict(self):

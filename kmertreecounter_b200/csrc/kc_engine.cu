@@ -632,6 +632,10 @@ void fill_stats(kc_context* c, kc_stats* s, double dev_ms, double wall_ms) {
     std::memcpy(s->root_counts, c->root_counts, sizeof s->root_counts);
     s->device_ms = dev_ms;
     s->wall_ms = wall_ms;
+    uint64_t live = 0;
+    for (const auto& m : c->h_meta) live += m.tab_mask + 1;
+    s->table_slots = live;
+    s->filter_words = c->bloom_words;
 }
 
 // Deliver completed device->host pieces in order; `all` waits for every one.
