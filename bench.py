@@ -54,6 +54,9 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--sample-scale", type=float, default=0.05, help="CPU sample size, fraction of the workload")
+    ap.add_argument("--batch-scale", type=float, default=0.05,
+                    help="read-set batch comparison: shrink genomes and read counts of the 512 sets")
+    ap.add_argument("--no-batched", action="store_true")
     return ap.parse_args()
 
 
@@ -181,6 +184,59 @@ def profile_traffic(args):
     except OSError:
         pass
     return None
+
+
+def compare_batched(args, kc, torch):
+    """512 independent read sets (genomes 1-20 Mbp, GC 30-70%, reads
+    log-uniform 10k-2M per set, length 50-300, substitution 0.5-2%, k 21 or 31;
+    genomes and read counts scaled by --batch-scale), FASTQ resident in HBM.
+    plain: one kc_count_device call per set (per-set launches and host syncs);
+    batched: kc_count_sets over autotuned groups of sets, one launch per stage
+    per group.  Both wall-clock on the host around device-synchronous calls."""
+    from kmertreecounter_b200 import autotune, synth
+    specs = synth.batched_sets(n_sets=512, seed=3, scale=args.batch_scale)
+    datas = [synth.fastq(p) for p, _ in specs]
+    ks = [k for _, k in specs]
+    offs, pos = [], 0
+    for d in datas:
+        offs.append(pos)
+        pos += (d.size + 15) // 16 * 16
+    buf = np.full(pos, ord("\n"), np.uint8)
+    for o, d in zip(offs, datas):
+        buf[o:o + d.size] = d
+    bases = int(sum(int(p.n_reads) * int(p.read_len_min) for p, _ in specs))
+    dev = torch.from_numpy(buf).cuda()
+    torch.cuda.synchronize()
+    sets = [(o, d.size, k) for o, d, k in zip(offs, datas, ks)]
+    base = dev.data_ptr()
+    # plain: one context per k, one call per set
+    ctx = {k: kc.Counter(k=k) for k in sorted(set(ks))}
+    for o, nb, k in sets[:8]:
+        ctx[k].count_device(base + o, nb)
+    torch.cuda.synchronize()
+    t = time.perf_counter()
+    for o, nb, k in sets:
+        ctx[k].count_device(base + o, nb)
+    torch.cuda.synchronize()
+    plain_ms = (time.perf_counter() - t) * 1e3
+    for c in ctx.values():
+        c.close()
+    # batched: autotuned knobs and sets per pass
+    best = autotune.tune(base, sets, 31, use_cache=False)
+    knobs = {k: v for k, v in best.items() if k in ("table_load", "repeat_ratio", "bloom_bits")}
+    with kc.Counter(k=31, **knobs) as c:
+        autotune.count_in_passes(c, base, sets, best["sets_per_pass"])
+        torch.cuda.synchronize()
+        t = time.perf_counter()
+        _, res = autotune.count_in_passes(c, base, sets, best["sets_per_pass"])
+        torch.cuda.synchronize()
+        batched_ms = (time.perf_counter() - t) * 1e3
+    del dev
+    return {"sets": len(sets), "bases": bases, "fastq_bytes": int(buf.size), "scale": args.batch_scale,
+            "plain": {"ms": plain_ms, "gbases_s": bases / plain_ms / 1e6},
+            "batched": {"ms": batched_ms, "gbases_s": bases / batched_ms / 1e6,
+                        "tuned": {k: v for k, v in best.items() if k != "trials"}},
+            "speedup": plain_ms / batched_ms, "kmers": int(sum(r.total_kmers for r in res))}
 
 
 def compare_sizing(args, kc, torch, dev, n, host, k, buckets, st_sampled, ms_sampled):
@@ -368,6 +424,8 @@ def run_ours(args):
     counter.close()
     kc.host_free(host_ptr)
 
+    if rank == 0 and not args.no_batched and args.workload == "genome_scale":
+        line["batched_sets"] = compare_batched(args, kc, torch)
     if rank == 0 and not args.no_cpu_baseline:
         with tempfile.TemporaryDirectory() as wd:
             path, data, kk, sbases, sp = cpu_sample(args.workload, args.sample_scale, wd)

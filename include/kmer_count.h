@@ -138,6 +138,35 @@ int kc_count_host_stream(kc_context* ctx, const uint8_t* fastq, uint64_t n, kc_s
 /* Same, with the FASTQ already in device memory (a device pointer). */
 int kc_count_device(kc_context* ctx, const uint8_t* d_fastq, uint64_t n, kc_stats* stats);
 
+/* ---- many read sets in one pass ----------------------------------------
+ * Benchmark pattern "batched uneven samples": independent read sets of uneven
+ * size and read length counted together -- every pipeline stage is one launch
+ * over all sets, with host synchronisation only at the sizing points.  Set s
+ * is bytes [offset, offset + bytes) of one device buffer (offset 16-byte
+ * aligned) counted with its own k (all sets in the key width of the
+ * context's k: all <= 32 or all 33..64) into its own filter, tables, low.bin
+ * range and 256 root files.  No counterpart in the reference, which counts one
+ * file per process. */
+typedef struct kc_set_desc {
+    uint64_t offset;
+    uint64_t bytes;
+    uint32_t k;
+    uint32_t reserved;
+} kc_set_desc;
+
+typedef struct kc_set_result {
+    uint64_t total_kmers;
+    uint64_t low_records;
+    uint64_t low_offset;      /* byte offset of this set's low.bin in kc_copy_low's buffer */
+    uint64_t low_bytes;
+    uint64_t root_records;
+    uint64_t root_offset;     /* record offset of this set's root files in kc_copy_roots's buffer */
+    uint64_t root_counts[256];/* records per root file, files in order 0..255 */
+} kc_set_result;
+
+int kc_count_sets(kc_context* ctx, const uint8_t* d_fastq, const kc_set_desc* sets, uint32_t n_sets,
+                  kc_set_result* results, kc_stats* stats);
+
 /* Sizes of the last result: packed low.bin bytes, number of root records,
  * and per-root record counts (256 entries, may be NULL). */
 int kc_result_sizes(kc_context* ctx, uint64_t* low_bytes, uint64_t* n_root_records, uint64_t* root_counts);

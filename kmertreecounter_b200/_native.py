@@ -29,7 +29,7 @@ ABI_SYMBOLS = (
     "kc_create", "kc_destroy", "kc_count_host", "kc_count_device", "kc_result_sizes", "kc_copy_low",
     "kc_copy_roots", "kc_write_outputs", "kc_device_results", "kc_host_alloc", "kc_host_free", "kc_stream",
     "kc_set_profiling", "kc_stage_times", "kc_stage_name", "kc_count_device_noalloc", "kc_count_host_stream",
-    "kc_histogram",
+    "kc_histogram", "kc_count_sets",
 )
 KC_SINK_LOW = 0
 KC_SINK_ROOT = 1
@@ -60,6 +60,16 @@ class KcStats(C.Structure):
         d = {f: getattr(self, f) for f, _ in self._fields_ if f != "root_counts"}
         d["root_counts"] = list(self.root_counts)
         return d
+
+
+class KcSetDesc(C.Structure):
+    _fields_ = [("offset", C.c_uint64), ("bytes", C.c_uint64), ("k", C.c_uint32), ("reserved", C.c_uint32)]
+
+
+class KcSetResult(C.Structure):
+    _fields_ = [("total_kmers", C.c_uint64), ("low_records", C.c_uint64), ("low_offset", C.c_uint64),
+                ("low_bytes", C.c_uint64), ("root_records", C.c_uint64), ("root_offset", C.c_uint64),
+                ("root_counts", C.c_uint64 * 256)]
 
 
 class KcError(RuntimeError):
@@ -99,6 +109,7 @@ def _load():
         "kc_count_device_noalloc": (i32, [cfgp, vp, u64, vp, u64, vp, u64, vp, stp]),
         "kc_count_host_stream": (i32, [vp, vp, u64, SINK_FN, vp, stp]),
         "kc_histogram": (i32, [vp, u32, u32, C.POINTER(u64), C.POINTER(u64)]),
+        "kc_count_sets": (i32, [vp, vp, C.POINTER(KcSetDesc), u32, C.POINTER(KcSetResult), stp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -219,6 +230,15 @@ class Counter:
         out = np.empty(nr, dtype=dt)
         check(lib.kc_copy_roots(self._ctx, out.ctypes.data if nr else None, nr * dt.itemsize))
         return out, counts
+
+    def count_sets(self, dptr, sets):
+        """Count many read sets in one device buffer in one pass.  `sets` is a
+        list of (offset, bytes, k); returns one KcSetResult per set."""
+        n = len(sets)
+        desc = (KcSetDesc * n)(*[KcSetDesc(o, b, k, 0) for o, b, k in sets])
+        res = (KcSetResult * n)()
+        check(lib.kc_count_sets(self._ctx, C.c_void_p(dptr), desc, n, res, C.byref(self.stats)))
+        return list(res)
 
     def histogram(self, min_freq=1, max_freq=10000):
         """(hist array for freq min..max, distinct keys) of the last result."""

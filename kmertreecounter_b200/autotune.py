@@ -1,0 +1,107 @@
+"""Autotuner for batched read-set counting (kc_count_sets).
+
+Times a small grid of the run-time knobs on a sample of the caller's read
+sets and keeps the fastest: table load factor and table headroom (repeat
+ratio), filter bits per k-mer, and the number of sets counted per pass (the
+batch granularity -- how many sets' tiles, keys and tables one pass holds).
+Every candidate produces identical counts (sizing never changes results), so
+only time decides.  Results are cached per GPU and workload signature in
+~/.cache/kmertreecounter_b200/tune.json.
+"""
+import hashlib
+import json
+import os
+import time
+
+import numpy as np
+
+from ._native import Counter
+
+CACHE = os.path.join(os.path.expanduser("~"), ".cache", "kmertreecounter_b200", "tune.json")
+
+GRID = [
+    dict(table_load=0.7, repeat_ratio=0.125, bloom_bits=8.0),
+    dict(table_load=0.5, repeat_ratio=0.125, bloom_bits=8.0),
+    dict(table_load=0.7, repeat_ratio=0.25, bloom_bits=8.0),
+    dict(table_load=0.7, repeat_ratio=0.0625, bloom_bits=8.0),
+    dict(table_load=0.7, repeat_ratio=0.125, bloom_bits=5.0),
+    dict(table_load=0.7, repeat_ratio=0.125, bloom_bits=12.0),
+]
+SETS_PER_PASS = [64, 128, 512]
+
+
+def _gpu_name():
+    try:
+        import torch
+        return torch.cuda.get_device_name(0)
+    except Exception:
+        return "unknown"
+
+
+def signature(sets):
+    sizes = sorted(int(b) for _, b, _ in sets)
+    ks = sorted({int(k) for _, _, k in sets})
+    key = f"{len(sets)}:{sum(sizes)}:{sizes[len(sizes) // 2] if sizes else 0}:{ks}"
+    return hashlib.sha1(key.encode()).hexdigest()[:16]
+
+
+def count_in_passes(counter, dptr, sets, per_pass):
+    """kc_count_sets over `sets` in groups of `per_pass`; device ms total."""
+    ms = 0.0
+    results = []
+    for i in range(0, len(sets), per_pass):
+        group = sets[i:i + per_pass]
+        base = group[0][0]
+        res = counter.count_sets(dptr + base, [(o - base, b, k) for o, b, k in group])
+        ms += counter.stats.device_ms
+        results.extend(res)
+    return ms, results
+
+
+def tune(dptr, sets, k, sample=64, repeats=2, use_cache=True):
+    """Best knob setting for these sets: dict of kc_config fields plus
+    `sets_per_pass`."""
+    sig = f"{_gpu_name()}|{signature(sets)}|{k}"
+    cache = {}
+    if use_cache and os.path.exists(CACHE):
+        try:
+            with open(CACHE) as f:
+                cache = json.load(f)
+        except (OSError, ValueError):
+            cache = {}
+        if sig in cache:
+            return cache[sig]
+    rng = np.random.default_rng(0)
+    pick = sorted(rng.choice(len(sets), size=min(sample, len(sets)), replace=False))
+    sub = [sets[i] for i in pick]
+    best, best_ms = None, float("inf")
+    trials = []
+    for knobs in GRID:
+        with Counter(k=k, **knobs) as c:
+            count_in_passes(c, dptr, sub, len(sub))  # warm-up: sizes every buffer
+            t = min(count_in_passes(c, dptr, sub, len(sub))[0] for _ in range(repeats))
+        trials.append(dict(knobs, ms=t))
+        if t < best_ms:
+            best, best_ms = dict(knobs), t
+    per_best, per_ms = SETS_PER_PASS[-1], float("inf")
+    with Counter(k=k, **best) as c:
+        for per in SETS_PER_PASS:
+            count_in_passes(c, dptr, sub, per)
+            t = min(count_in_passes(c, dptr, sub, per)[0] for _ in range(repeats))
+            trials.append(dict(best, sets_per_pass=per, ms=t))
+            if t < per_ms:
+                per_best, per_ms = per, t
+    best["sets_per_pass"] = per_best
+    best["trials"] = trials
+    if use_cache:
+        cache[sig] = best
+        os.makedirs(os.path.dirname(CACHE), exist_ok=True)
+        with open(CACHE, "w") as f:
+            json.dump(cache, f, indent=1)
+    return best
+
+
+def timed_wall(fn):
+    t = time.perf_counter()
+    out = fn()
+    return out, (time.perf_counter() - t) * 1e3

@@ -155,6 +155,7 @@ struct kc_context {
     DevBuf low_packed;
     DevBuf roots, chunks, root_count, root_cursor;
     DevBuf sort_tmp, sort_hist, sort_offs, sort_sums;
+    DevBuf set_tiles, tile_prefix, set_info;  // multi-set batches
 
     // host mirrors
     std::vector<kc::BucketMeta> h_meta;
@@ -171,6 +172,8 @@ struct kc_context {
     uint64_t K = 0;
     uint64_t rehashes = 0, batches = 0, input_bytes = 0;
     bool have_result = false;
+    bool batch_result = false;   // last result came from kc_count_sets
+    uint64_t batch_low_bytes = 0;
     uint64_t root_total = 0, table_keys = 0;
     uint64_t root_counts[256] = {};
 
@@ -313,7 +316,7 @@ void launch_count(kc_context* c, uint64_t n_keys, int use_filter) {
     // each CTA covers CNT_SEGS_PER_WARP segments per warp, in blockIdx order
     const uint64_t tiles = ceil_div(n_keys, (uint64_t)TILE * kc::CNT_SEGS_PER_WARP);
     if (!tiles) return;
-    kc::CountArgs a;
+    kc::CountArgs a{};
     a.routed = c->routed.p;
     a.n_keys = n_keys;
     a.meta = c->meta.as<kc::BucketMeta>();
@@ -385,7 +388,7 @@ template <int NW>
 int launch_extract(kc_context* c, const uint8_t* buf, uint64_t n, int has_halo, int mode) {
     const uint64_t tiles = ceil_div(n, kc::EXT_TILE);
     if (!tiles) return KC_OK;
-    kc::ExtractArgs a;
+    kc::ExtractArgs a{};
     a.buf = buf;
     a.n = n;
     a.has_halo = has_halo;
@@ -575,6 +578,7 @@ int begin_run(kc_context* c, uint64_t total_bytes) {
     c->input_bytes = 0;
     c->sized = false;
     c->have_result = false;
+    c->batch_result = false;
     c->expected_total_bytes = total_bytes;
     c->ev_used = 0;
     c->spans.clear();
@@ -809,7 +813,8 @@ void kc_destroy(kc_context* c) {
     DevBuf* bufs[] = {&c->stage,  &c->tile_nl,   &c->tile_line, &c->bucket_count, &c->bucket_cursor, &c->routed,
                       &c->tile_low, &c->tile_fail, &c->tile_low_prefix, &c->scan_sums, &c->scalars, &c->overflow,
                       &c->meta,   &c->bloom,     &c->table,     &c->low_packed,   &c->roots,         &c->chunks,
-                      &c->root_count, &c->root_cursor, &c->sort_tmp, &c->sort_hist, &c->sort_offs, &c->sort_sums};
+                      &c->root_count, &c->root_cursor, &c->sort_tmp, &c->sort_hist, &c->sort_offs, &c->sort_sums,
+                      &c->set_tiles, &c->tile_prefix, &c->set_info};
     for (DevBuf* b : bufs) b->release();
     for (cudaEvent_t e : c->ev_pool) cudaEventDestroy(e);
     if (c->h2d) cudaStreamSynchronize(c->h2d);
@@ -982,6 +987,7 @@ int kc_count_host_stream(kc_context* c, const uint8_t* fastq, uint64_t n, kc_sin
 int kc_histogram(kc_context* c, uint32_t min_freq, uint32_t max_freq, uint64_t* hist, uint64_t* distinct) {
     if (!c) return fail(KC_ERR_INVALID, "null context");
     if (!c->have_result) return fail(KC_ERR_STATE, "no result: run a count first");
+    if (c->batch_result) return fail(KC_ERR_STATE, "a multi-set result has one histogram per set; not supported");
     if (c->stream_low) return fail(KC_ERR_STATE, "streamed results are not kept on the device");
     if (max_freq < min_freq || min_freq == 0) return fail(KC_ERR_INVALID, "need 1 <= min_freq <= max_freq");
     const uint64_t bins = (uint64_t)max_freq - min_freq + 1;
@@ -1026,7 +1032,7 @@ int kc_histogram(kc_context* c, uint32_t min_freq, uint32_t max_freq, uint64_t* 
 int kc_result_sizes(kc_context* c, uint64_t* low_bytes, uint64_t* n_root, uint64_t* root_counts) {
     if (!c) return fail(KC_ERR_INVALID, "null context");
     if (!c->have_result) return fail(KC_ERR_STATE, "no result: run a count first");
-    if (low_bytes) *low_bytes = c->low_total * c->packed_bytes;
+    if (low_bytes) *low_bytes = c->batch_result ? c->batch_low_bytes : c->low_total * c->packed_bytes;
     if (n_root) *n_root = c->root_total;
     if (root_counts) std::memcpy(root_counts, c->root_counts, sizeof c->root_counts);
     return KC_OK;
@@ -1035,7 +1041,7 @@ int kc_result_sizes(kc_context* c, uint64_t* low_bytes, uint64_t* n_root, uint64
 int kc_copy_low(kc_context* c, uint8_t* dst, uint64_t cap) {
     if (!c) return fail(KC_ERR_INVALID, "null context");
     if (!c->have_result) return fail(KC_ERR_STATE, "no result: run a count first");
-    const uint64_t bytes = c->low_total * c->packed_bytes;
+    const uint64_t bytes = c->batch_result ? c->batch_low_bytes : c->low_total * c->packed_bytes;
     if (cap < bytes) return fail(KC_ERR_INVALID, "destination too small: %llu < %llu", (unsigned long long)cap,
                                  (unsigned long long)bytes);
     if (bytes) {
@@ -1062,7 +1068,7 @@ int kc_device_results(kc_context* c, const void** d_low, uint64_t* low_bytes, co
     if (!c) return fail(KC_ERR_INVALID, "null context");
     if (!c->have_result) return fail(KC_ERR_STATE, "no result: run a count first");
     if (d_low) *d_low = c->low_packed.p;
-    if (low_bytes) *low_bytes = c->low_total * c->packed_bytes;
+    if (low_bytes) *low_bytes = c->batch_result ? c->batch_low_bytes : c->low_total * c->packed_bytes;
     if (d_roots) *d_roots = c->roots.p;
     if (n_roots) *n_roots = c->root_total;
     return KC_OK;
@@ -1103,6 +1109,7 @@ extern "C" int kc_set_predicted_loads(kc_context* c, const double* distinct, con
 extern "C" int kc_bucket_loads(kc_context* c, uint64_t* distinct, uint64_t* table_keys, uint64_t* kmers) {
     if (!c) return fail(KC_ERR_INVALID, "null context");
     if (!c->have_result) return fail(KC_ERR_STATE, "no result: run a count first");
+    if (c->batch_result) return fail(KC_ERR_STATE, "not available for a multi-set result");
     if (c->stream_low) return fail(KC_ERR_STATE, "streamed results are not kept on the device");
     DevBuf d;
     CK(d.ensure(3 * KC_MODEL_BUCKETS * sizeof(unsigned long long)));
@@ -1145,3 +1152,364 @@ extern "C" int kc_bucket_loads(kc_context* c, uint64_t* distinct, uint64_t* tabl
 int kc_internal_set_error(int code, const char* msg) { return fail(code, "%s", msg); }
 
 uint64_t kc_internal_record_bytes(const kc_context* c) { return c ? c->record_bytes : 0; }
+
+// ------------------------------------------------------------------ batches
+//
+// Many independent read sets in one device buffer, counted in one pass: every
+// pipeline stage is ONE launch over all sets.  Set s owns buckets
+// [256 s, 256 s + 256) and a routed region aligned to a count segment (the gap
+// holds EMPTY keys, which the count kernel skips), so segments, filter and
+// tables never mix sets.  Host synchronisation happens only at the sizing
+// points (after the histogram, after counting, after the low scan, after the
+// export count) instead of per set; the scatter -> gap fill -> count sequence
+// runs as one captured CUDA graph.
+
+namespace {
+
+// Per-set first-occurrence totals from the per-segment exclusive scan.  A set
+// whose routed region is empty starts at segment index nsegs, one past the end
+// of the scan, so that index reads the grand total instead.
+__global__ void set_low_counts(const uint64_t* seg_prefix, const uint64_t* set_seg_start, uint32_t n_sets,
+                               uint64_t nsegs, const uint64_t* total, uint64_t* out) {
+    for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < n_sets; s += gridDim.x * blockDim.x) {
+        const uint64_t sa = set_seg_start[s];
+        const uint64_t sb = (s + 1 < n_sets) ? set_seg_start[s + 1] : nsegs;
+        const uint64_t a = sa < nsegs ? seg_prefix[sa] : *total;
+        const uint64_t b = sb < nsegs ? seg_prefix[sb] : *total;
+        out[s] = b - a;
+    }
+}
+
+template <int NW>
+int count_sets_impl(kc_context* c, const uint8_t* buf, const kc_set_desc* sets, uint32_t n_sets, kc_set_result* res) {
+    constexpr int SEG = kc::count_seg<NW>();
+    constexpr int CT = kc::count_tile<NW>();
+    constexpr uint32_t NB = 256;
+    const kc_config& g = c->cfg;
+    const uint64_t nbk = (uint64_t)n_sets * NB;
+    using KeyT = typename kc::KeyOf<NW>::T;
+
+    // tiles
+    std::vector<kc::SetTile> tiles;
+    for (uint32_t s = 0; s < n_sets; ++s) {
+        const uint32_t first = (uint32_t)tiles.size();
+        for (uint64_t off = 0; off < sets[s].bytes; off += kc::EXT_TILE)
+            tiles.push_back(kc::SetTile{sets[s].offset + off, sets[s].offset + sets[s].bytes, s, sets[s].k, first, 0});
+    }
+    const uint64_t nt = tiles.size();
+    CK(c->set_tiles.ensure(std::max<uint64_t>(nt, 1) * sizeof(kc::SetTile)));
+    CK(c->tile_nl.ensure(std::max<uint64_t>(nt, 1) * sizeof(uint32_t)));
+    CK(c->tile_line.ensure(std::max<uint64_t>(nt, 1) * sizeof(uint64_t)));
+    CK(c->tile_prefix.ensure(std::max<uint64_t>(nt, 1) * sizeof(uint64_t)));
+    CK(c->scalars.ensure(64));
+    uint64_t* d_scal = c->scalars.as<uint64_t>();
+    CK(cudaMemsetAsync(c->scalars.as<uint32_t>() + 12, 0, sizeof(uint32_t), c->stream));
+    if (nt) CK(cudaMemcpyAsync(c->set_tiles.p, tiles.data(), nt * sizeof(kc::SetTile), cudaMemcpyHostToDevice, c->stream));
+    const kc::SetTile* d_tiles = c->set_tiles.as<kc::SetTile>();
+    int rc;
+    if (nt) {
+        Stage st(c, KC_STAGE_LINES, 2);
+        kc::lines_per_set_tile<<<nt, kc::EXT_THREADS, 0, c->stream>>>(buf, d_tiles, c->tile_nl.as<uint32_t>());
+    }
+    if ((rc = device_scan<uint32_t, uint64_t>(c, c->tile_nl.as<uint32_t>(), nt, c->tile_prefix.as<uint64_t>(), 0,
+                                              d_scal + 0)))
+        return rc;
+    if (nt) kc::rebase_set_lines<<<std::min<uint64_t>(ceil_div(nt, 256), 1184), 256, 0, c->stream>>>(
+        c->tile_prefix.as<uint64_t>(), d_tiles, nt, c->tile_line.as<uint64_t>());
+
+    kc::ExtractArgs a{};
+    a.tiles = d_tiles;
+    a.buf = buf;
+    a.tile_line = c->tile_line.as<uint64_t>();
+    a.bucket_shift = 56;
+    a.n_buckets = NB;
+    CK(c->bucket_count.ensure(nbk * sizeof(uint64_t)));
+    CK(c->bucket_cursor.ensure(nbk * sizeof(uint64_t)));
+    a.bucket_count = c->bucket_count.as<unsigned long long>();
+    a.bucket_cursor = c->bucket_cursor.as<unsigned long long>();
+    a.error = c->scalars.as<uint32_t>() + 12;
+    CK(cudaMemsetAsync(c->bucket_count.p, 0, nbk * sizeof(uint64_t), c->stream));
+    if (nt) {
+        Stage st(c, KC_STAGE_EXTRACT_HIST);
+        kc::extract_kernel<NW, kc::HIST><<<nt, kc::EXT_THREADS, kc::extract_smem_bytes<NW, kc::HIST>(NB), c->stream>>>(a);
+    }
+    CK(cudaGetLastError());
+    std::vector<uint64_t> cnt(nbk);
+    CK(cudaMemcpyAsync(cnt.data(), c->bucket_count.p, nbk * sizeof(uint64_t), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+
+    // layout: each set's routed region starts on a segment boundary
+    std::vector<uint64_t> start(nbk), set_key0(n_sets), set_key1(n_sets), set_next(n_sets), set_seg(n_sets);
+    uint64_t pos = 0;
+    c->h_meta.assign(nbk, kc::BucketMeta{});
+    uint64_t bw = 0, ts = 0, K = 0;
+    for (uint32_t s = 0; s < n_sets; ++s) {
+        pos = ceil_div(pos, SEG) * SEG;
+        set_key0[s] = pos;
+        set_seg[s] = pos / SEG;
+        for (uint32_t b = 0; b < NB; ++b) {
+            const uint64_t kb = cnt[(uint64_t)s * NB + b];
+            start[(uint64_t)s * NB + b] = pos;
+            pos += kb;
+            K += kb;
+            const uint64_t words = pow2_at_least(std::max<uint64_t>((uint64_t)(kb * g.bloom_bits / 64.0), 64));
+            const uint64_t slots = pow2_at_least(std::max<uint64_t>((uint64_t)(kb * g.repeat_ratio / g.table_load), 64));
+            c->h_meta[(uint64_t)s * NB + b] = kc::BucketMeta{bw, words - 1, ts, slots - 1};
+            bw += words;
+            ts += slots;
+        }
+        set_key1[s] = pos;
+    }
+    const uint64_t n_keys = ceil_div(pos, SEG) * SEG;
+    for (uint32_t s = 0; s < n_sets; ++s) set_next[s] = (s + 1 < n_sets) ? set_key0[s + 1] : n_keys;
+    c->K = K;
+    c->bloom_words = bw;
+    c->table_slots_used = ts;
+    CK(c->bloom.ensure(bw * sizeof(uint64_t)));
+    CK(c->table.ensure(ts * c->slot_bytes + ts * c->slot_bytes / 2));
+    CK(c->meta.ensure(nbk * sizeof(kc::BucketMeta)));
+    CK(c->overflow.ensure(nbk * sizeof(uint32_t)));
+    const uint64_t nsegs = n_keys / SEG;
+    CK(c->routed.ensure(std::max<uint64_t>(ceil_div(n_keys, CT) * CT, 1) * sizeof(KeyT)));
+    CK(c->tile_low.ensure(std::max<uint64_t>(nsegs, 1) * sizeof(uint32_t)));
+    CK(c->tile_fail.ensure(std::max<uint64_t>(nsegs, 1) * sizeof(uint32_t)));
+    CK(c->tile_low_prefix.ensure(std::max<uint64_t>(nsegs, 1) * sizeof(uint64_t)));
+    CK(c->set_info.ensure((size_t)n_sets * 6 * sizeof(uint64_t) + 64));
+    uint64_t* d_seg = c->set_info.as<uint64_t>();              // set_seg_start[n_sets]
+    uint64_t* d_end = d_seg + n_sets;                          // set_key1
+    uint64_t* d_next = d_end + n_sets;                         // next set's first key
+    uint64_t* d_low = d_next + n_sets;                         // low count per set
+    uint64_t* d_lowbase = d_low + n_sets;                      // low byte base per set
+    uint32_t* d_k = reinterpret_cast<uint32_t*>(d_lowbase + n_sets);
+    std::vector<uint32_t> ks(n_sets);
+    for (uint32_t s = 0; s < n_sets; ++s) ks[s] = sets[s].k;
+    CK(cudaMemcpyAsync(d_seg, set_seg.data(), n_sets * sizeof(uint64_t), cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(d_end, set_key1.data(), n_sets * sizeof(uint64_t), cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(d_next, set_next.data(), n_sets * sizeof(uint64_t), cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(d_k, ks.data(), n_sets * sizeof(uint32_t), cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(c->meta.p, c->h_meta.data(), nbk * sizeof(kc::BucketMeta), cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(c->bucket_cursor.p, start.data(), nbk * sizeof(uint64_t), cudaMemcpyHostToDevice, c->stream));
+    {
+        Stage st(c, KC_STAGE_INIT, 1);
+        CK(cudaMemsetAsync(c->bloom.p, 0, bw * sizeof(uint64_t), c->stream));
+        kc::init_slots<NW><<<c->sm_count * 8, 256, 0, c->stream>>>(c->table.p, ts);
+        CK(cudaMemsetAsync(c->overflow.p, 0, nbk * sizeof(uint32_t), c->stream));
+    }
+    CK(cudaGetLastError());
+
+    kc::CountArgs ca{};
+    ca.routed = c->routed.p;
+    ca.n_keys = n_keys;
+    ca.meta = c->meta.as<kc::BucketMeta>();
+    ca.bloom = c->bloom.as<uint64_t>();
+    ca.table = c->table.p;
+    ca.seg_low = c->tile_low.as<uint32_t>();
+    ca.seg_fail = c->tile_fail.as<uint32_t>();
+    ca.bucket_overflow = c->overflow.as<uint32_t>();
+    ca.bucket_shift = 56;
+    ca.n_buckets = (uint32_t)std::min<uint64_t>(nbk, 0xFFFFFFFFu);
+    ca.set_seg_start = d_seg;
+    ca.n_sets = n_sets;
+    ca.set_buckets = NB;
+    ca.use_filter = 1;
+    const uint64_t cgrid = ceil_div(n_keys, (uint64_t)CT * kc::CNT_SEGS_PER_WARP);
+
+    // scatter -> gap fill -> count as one graph
+    {
+        Stage st(c, KC_STAGE_COUNT_ROUTED, 3);
+        a.routed = c->routed.p;
+        cudaGraph_t graph = nullptr;
+        cudaGraphExec_t exec = nullptr;
+        CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+        if (nt)
+            kc::extract_kernel<NW, kc::SCATTER>
+                <<<nt, kc::EXT_THREADS, kc::extract_smem_bytes<NW, kc::SCATTER>(NB), c->stream>>>(a);
+        kc::fill_set_gaps<NW><<<n_sets, 256, 0, c->stream>>>(c->routed.p, d_end, d_next, n_sets);
+        if (cgrid) kc::count_routed<NW><<<cgrid, kc::CNT_THREADS, 0, c->stream>>>(ca);
+        const cudaError_t ce = cudaStreamEndCapture(c->stream, &graph);
+        if (ce != cudaSuccess) return fail(KC_ERR_DEVICE, "graph capture failed: %s", cudaGetErrorString(ce));
+        cudaError_t e = cudaGraphInstantiate(&exec, graph, 0);
+        if (e == cudaSuccess) e = cudaGraphLaunch(exec, c->stream);
+        if (exec) cudaGraphExecDestroy(exec);
+        cudaGraphDestroy(graph);
+        if (e != cudaSuccess) return fail(KC_ERR_DEVICE, "graph launch failed: %s", cudaGetErrorString(e));
+    }
+
+    // overflowed tables: grow x4, move, retry only the failed keys
+    for (int round = 0;; ++round) {
+        std::vector<uint32_t> ov(nbk);
+        CK(cudaMemcpyAsync(ov.data(), c->overflow.p, nbk * sizeof(uint32_t), cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
+        bool any = false;
+        for (uint64_t b = 0; b < nbk; ++b) any |= ov[b] != 0;
+        if (!any) break;
+        if (round > 24) return fail(KC_ERR_OVERFLOW, "repeat tables kept overflowing");
+        CK(cudaMemsetAsync(c->overflow.p, 0, nbk * sizeof(uint32_t), c->stream));
+        uint32_t* d_failed = c->scalars.as<uint32_t>() + 8;
+        for (uint64_t b = 0; b < nbk; ++b) {
+            if (!ov[b]) continue;
+            const uint64_t old_slots = c->h_meta[b].tab_mask + 1;
+            uint64_t new_slots = old_slots * 4;
+            for (;;) {
+                CK(c->table.grow_keep((c->table_slots_used + new_slots) * c->slot_bytes, c->table_slots_used * c->slot_bytes,
+                                      c->stream));
+                uint8_t* nt_ = c->table.as<uint8_t>() + c->table_slots_used * c->slot_bytes;
+                const uint8_t* ot = c->table.as<uint8_t>() + c->h_meta[b].tab_off * c->slot_bytes;
+                Stage st(c, KC_STAGE_REHASH, 2);
+                kc::init_slots<NW><<<64, 256, 0, c->stream>>>(nt_, new_slots);
+                CK(cudaMemsetAsync(d_failed, 0, sizeof(uint32_t), c->stream));
+                kc::rehash_bucket<NW><<<std::max<uint64_t>(1, std::min<uint64_t>(1184, ceil_div(old_slots, 256))), 256, 0,
+                                        c->stream>>>(ot, old_slots, nt_, new_slots - 1, d_failed);
+                uint32_t h_failed = 0;
+                CK(cudaMemcpyAsync(&h_failed, d_failed, sizeof h_failed, cudaMemcpyDeviceToHost, c->stream));
+                CK(cudaStreamSynchronize(c->stream));
+                const uint64_t off = c->table_slots_used;
+                c->table_slots_used += new_slots;
+                if (!h_failed) {
+                    c->h_meta[b].tab_off = off;
+                    c->h_meta[b].tab_mask = new_slots - 1;
+                    break;
+                }
+                new_slots *= 4;
+            }
+            ++c->rehashes;
+        }
+        CK(cudaMemcpyAsync(c->meta.p, c->h_meta.data(), nbk * sizeof(kc::BucketMeta), cudaMemcpyHostToDevice, c->stream));
+        ca.table = c->table.p;
+        ca.use_filter = 0;
+        Stage st(c, KC_STAGE_REHASH);
+        if (cgrid) kc::count_routed<NW><<<cgrid, kc::CNT_THREADS, 0, c->stream>>>(ca);
+        CK(cudaGetLastError());
+    }
+
+    // first occurrences: per-set counts, byte bases, packing
+    if ((rc = device_scan<uint32_t, uint64_t>(c, c->tile_low.as<uint32_t>(), nsegs, c->tile_low_prefix.as<uint64_t>(), 0,
+                                              d_scal + 1)))
+        return rc;
+    set_low_counts<<<std::max<uint64_t>(1, ceil_div(n_sets, 256)), 256, 0, c->stream>>>(
+        c->tile_low_prefix.as<uint64_t>(), d_seg, n_sets, nsegs, d_scal + 1, d_low);
+    CK(cudaGetLastError());
+    std::vector<uint64_t> lows(n_sets);
+    CK(cudaMemcpyAsync(lows.data(), d_low, n_sets * sizeof(uint64_t), cudaMemcpyDeviceToHost, c->stream));
+    uint32_t ext_err = 0;
+    CK(cudaMemcpyAsync(&ext_err, c->scalars.as<uint32_t>() + 12, sizeof ext_err, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    if (ext_err) return fail(KC_ERR_DEVICE, "internal error: routing bucket disagreed with its reservation");
+    std::vector<uint64_t> lowbase(n_sets);
+    uint64_t lb = 0, total_low = 0;
+    for (uint32_t s = 0; s < n_sets; ++s) {
+        total_low += lows[s];
+        lowbase[s] = lb;
+        lb += lows[s] * kc_packed_bytes(sets[s].k);
+    }
+    CK(cudaMemcpyAsync(d_lowbase, lowbase.data(), n_sets * sizeof(uint64_t), cudaMemcpyHostToDevice, c->stream));
+    CK(c->low_packed.ensure(lb + 64));
+    if (nsegs) {
+        Stage st(c, KC_STAGE_PACK_LOW);
+        kc::pack_low_sets<NW><<<std::min<uint64_t>(ceil_div(nsegs, 8), 148 * 16), 256, 0, c->stream>>>(
+            c->routed.p, c->tile_low.as<uint32_t>(), c->tile_low_prefix.as<uint64_t>(), nsegs, d_seg, d_k, d_lowbase,
+            n_sets, c->low_packed.as<uint8_t>());
+    }
+    CK(cudaGetLastError());
+
+    // root records grouped by (set, root id)
+    std::vector<kc::ExportChunk> ch;
+    const uint32_t CH = 16384;
+    for (uint64_t b = 0; b < nbk; ++b) {
+        const uint64_t slots = c->h_meta[b].tab_mask + 1;
+        for (uint64_t q = 0; q < slots; q += CH)
+            ch.push_back(kc::ExportChunk{c->h_meta[b].tab_off + q, (uint32_t)std::min<uint64_t>(CH, slots - q), (uint32_t)b});
+    }
+    CK(c->chunks.ensure(ch.size() * sizeof(kc::ExportChunk)));
+    CK(cudaMemcpyAsync(c->chunks.p, ch.data(), ch.size() * sizeof(kc::ExportChunk), cudaMemcpyHostToDevice, c->stream));
+    CK(c->root_count.ensure((nbk + 1) * sizeof(uint64_t)));
+    CK(c->root_cursor.ensure(nbk * sizeof(uint64_t)));
+    CK(cudaMemsetAsync(c->root_count.p, 0, (nbk + 1) * sizeof(uint64_t), c->stream));
+    unsigned long long* rcd = c->root_count.as<unsigned long long>();
+    const uint64_t grid = std::min<uint64_t>(ch.size(), 148 * 16);
+    {
+        Stage st(c, KC_STAGE_EXPORT);
+        kc::export_count<NW><<<grid, 256, 0, c->stream>>>(c->table.p, c->chunks.as<kc::ExportChunk>(), ch.size(),
+                                                          g.min_count, g.max_count, rcd, rcd + nbk);
+    }
+    std::vector<uint64_t> rc_h(nbk + 1);
+    CK(cudaMemcpyAsync(rc_h.data(), rcd, (nbk + 1) * sizeof(uint64_t), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    std::vector<uint64_t> rstart(nbk);
+    uint64_t R = 0;
+    for (uint64_t b = 0; b < nbk; ++b) {
+        rstart[b] = R;
+        R += rc_h[b];
+    }
+    CK(c->roots.ensure(std::max<uint64_t>(R, 1) * c->record_bytes));
+    CK(cudaMemcpyAsync(c->root_cursor.p, rstart.data(), nbk * sizeof(uint64_t), cudaMemcpyHostToDevice, c->stream));
+    {
+        Stage st(c, KC_STAGE_EXPORT);
+        kc::export_write<NW><<<grid, 256, 0, c->stream>>>(c->table.p, c->chunks.as<kc::ExportChunk>(), ch.size(),
+                                                          g.min_count, g.max_count, c->root_cursor.as<unsigned long long>(),
+                                                          c->roots.as<uint8_t>());
+    }
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(c->stream));
+
+    // per-set results; per-set table keys from the live table regions
+    for (uint32_t s = 0; s < n_sets; ++s) {
+        kc_set_result& r = res[s];
+        std::memset(&r, 0, sizeof r);
+        uint64_t km = 0;
+        for (uint32_t b = 0; b < NB; ++b) {
+            km += cnt[(uint64_t)s * NB + b];
+            r.root_counts[b] = rc_h[(uint64_t)s * NB + b];
+            r.root_records += r.root_counts[b];
+        }
+        r.total_kmers = km;
+        r.low_records = lows[s];
+        r.low_offset = lowbase[s];
+        r.low_bytes = lows[s] * kc_packed_bytes(sets[s].k);
+        r.root_offset = rstart[(uint64_t)s * NB];
+    }
+    c->low_total = total_low;
+    c->batch_low_bytes = lb;
+    c->root_total = R;
+    c->table_keys = rc_h[nbk];
+    std::memset(c->root_counts, 0, sizeof c->root_counts);
+    for (uint64_t b = 0; b < nbk; ++b) c->root_counts[b % NB] += rc_h[b];
+    c->batch_result = true;
+    c->have_result = true;
+    return KC_OK;
+}
+
+}  // namespace
+
+extern "C" int kc_count_sets(kc_context* c, const uint8_t* d_fastq, const kc_set_desc* sets, uint32_t n_sets,
+                             kc_set_result* results, kc_stats* stats) {
+    if (!c || !sets || !results || n_sets == 0 || (!d_fastq)) return fail(KC_ERR_INVALID, "null argument");
+    if (c->n_buckets != 256) return fail(KC_ERR_INVALID, "read-set batches use 256 buckets per set");
+    for (uint32_t s = 0; s < n_sets; ++s) {
+        const uint32_t k = sets[s].k;
+        if (k < 1 || k > 64 || (k <= 32) != (c->cfg.k <= 32))
+            return fail(KC_ERR_INVALID, "set %u: k=%u must be in the key width of the context's k (%u)", s, k, c->cfg.k);
+        if (sets[s].offset % 16) return fail(KC_ERR_INVALID, "set %u: offset must be 16-byte aligned", s);
+    }
+    const auto t0 = std::chrono::steady_clock::now();
+    int rc = begin_run(c, 0);
+    if (rc) return rc;
+    c->stream_low = false;
+    CK(cudaEventRecord(c->ev0, c->stream));
+    uint64_t bytes = 0;
+    for (uint32_t s = 0; s < n_sets; ++s) bytes += sets[s].bytes;
+    c->input_bytes = bytes;
+    c->batches = 1;
+    rc = c->nw == 1 ? count_sets_impl<1>(c, d_fastq, sets, n_sets, results)
+                    : count_sets_impl<2>(c, d_fastq, sets, n_sets, results);
+    if (rc) return rc;
+    CK(cudaEventRecord(c->ev1, c->stream));
+    CK(cudaEventSynchronize(c->ev1));
+    collect_stage_times(c);
+    float ms = 0;
+    cudaEventElapsedTime(&ms, c->ev0, c->ev1);
+    const double wall = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    fill_stats(c, stats, ms, wall);
+    if (stats) stats->low_records = c->low_total;
+    return KC_OK;
+}

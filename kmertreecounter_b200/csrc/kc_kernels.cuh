@@ -62,6 +62,15 @@ struct Key2 {
     uint64_t w0, w1;
 };
 
+// One extraction tile of a multi-set batch: bytes [start, min(start + 8 KiB,
+// end)) of read set `set`, whose k-mers are counted with `k` into buckets
+// [set * n_buckets, (set + 1) * n_buckets).  first_tile = index of the set's
+// first tile (line numbers restart there; no halo before it).
+struct SetTile {
+    uint64_t start, end;
+    uint32_t set, k, first_tile, pad;
+};
+
 // Per-bucket placement of the first-occurrence filter and the repeat table.
 struct BucketMeta {
     uint64_t bloom_off;   // in 64-bit words
@@ -216,6 +225,37 @@ static __global__ void lines_per_tile(const uint8_t* __restrict__ buf, uint64_t 
     if (threadIdx.x == 0) tile_nl[tile] = total;
 }
 
+// '\n' count of each set tile (multi-set batches).
+static __global__ void lines_per_set_tile(const uint8_t* __restrict__ buf, const SetTile* __restrict__ tiles,
+                                          uint32_t* __restrict__ tile_nl) {
+    __shared__ uint32_t warp_sums[EXT_THREADS / 32];
+    const SetTile t = tiles[blockIdx.x];
+    const uint64_t pos = t.start + (uint64_t)threadIdx.x * EXT_BPT;
+    uint32_t cnt = 0;
+    if (pos < t.end) {
+        const uint64_t rem = t.end - pos;
+        if (rem >= 32) {
+            const uint4* p = reinterpret_cast<const uint4*>(buf + pos);
+            const uint4 a = __ldcs(p), b = __ldcs(p + 1);
+            const uint32_t w[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
+#pragma unroll
+            for (int i = 0; i < 8; ++i) cnt += __popc(__vcmpeq4(w[i], 0x0A0A0A0Au) & 0x01010101u);
+        } else {
+            for (uint32_t j = 0; j < (uint32_t)rem; ++j) cnt += buf[pos + j] == '\n';
+        }
+    }
+    uint32_t total;
+    block_exclusive_scan<EXT_THREADS>(cnt, warp_sums, &total);
+    if (threadIdx.x == 0) tile_nl[blockIdx.x] = total;
+}
+
+// Line index at each tile start, counted from its own set's first byte.
+static __global__ void rebase_set_lines(const uint64_t* __restrict__ global_prefix, const SetTile* __restrict__ tiles,
+                                        uint64_t n_tiles, uint64_t* __restrict__ tile_line) {
+    for (uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; t < n_tiles; t += (uint64_t)gridDim.x * blockDim.x)
+        tile_line[t] = global_prefix[t] - global_prefix[tiles[t].first_tile];
+}
+
 // ------------------------------------------------------- k-mer extraction
 
 enum ExtractMode { HIST = 0, SCATTER = 1 };
@@ -328,6 +368,7 @@ KC_HD void window_at(uint64_t s0, uint64_t s1, uint64_t s2, uint32_t j, uint64_t
 }
 
 struct ExtractArgs {
+    const SetTile* tiles;    // multi-set batch: per-tile descriptor (nullptr: one input)
     const uint8_t* buf;      // batch start (16-byte aligned)
     uint64_t n;              // batch bytes
     int has_halo;            // buf[-HALO..-1] are the bytes before the batch
@@ -416,9 +457,20 @@ __global__ void __launch_bounds__(EXT_THREADS) extract_kernel(ExtractArgs a) {
     uint16_t* sbkt = reinterpret_cast<uint16_t*>(skeys + STAGE);
 
     const int tid = threadIdx.x;
-    const uint64_t tile_start = (uint64_t)blockIdx.x * EXT_TILE;
+    uint64_t tile_start = (uint64_t)blockIdx.x * EXT_TILE;
+    uint64_t n_end = a.n;
+    bool halo_ok = tile_start > 0 || a.has_halo;
+    uint32_t k = a.k;
+    uint64_t bucket_off = 0;
+    if (a.tiles) {
+        const SetTile t = a.tiles[blockIdx.x];
+        tile_start = t.start;
+        n_end = t.end;
+        halo_ok = t.first_tile != blockIdx.x;
+        k = t.k;
+        bucket_off = (uint64_t)t.set * a.n_buckets;
+    }
     const uint64_t seg_start = tile_start + (uint64_t)tid * EXT_BPT;
-    const uint32_t k = a.k;
     const uint32_t B = 64 - a.bucket_shift;
 
     for (uint32_t b = tid; b < a.n_buckets; b += EXT_THREADS) {
@@ -429,14 +481,14 @@ __global__ void __launch_bounds__(EXT_THREADS) extract_kernel(ExtractArgs a) {
 
     // ---- phase A: classify own segment (+ the two halo segments)
     uint32_t w[8];
-    const uint64_t valid = seg_start < a.n ? a.n - seg_start : 0;
+    const uint64_t valid = seg_start < n_end ? n_end - seg_start : 0;
     load32(a.buf + seg_start, valid, w);
     const Seg s = classify(w, valid);
     seg_codes[tid + 2] = s.codes;
     seg_bases[tid + 2] = s.bases;
     if (tid < 2) {
         uint32_t hw[8];
-        const bool readable = tile_start > 0 || a.has_halo;
+        const bool readable = halo_ok;
         load32(a.buf + (int64_t)tile_start - HALO + 32 * tid, readable ? 32 : 0, hw);
         const Seg h = classify(hw, readable ? 32 : 0);
         seg_codes[tid] = h.codes;
@@ -477,7 +529,7 @@ __global__ void __launch_bounds__(EXT_THREADS) extract_kernel(ExtractArgs a) {
                 const uint32_t b = tid * per + q;
                 if (b < a.n_buckets) {
                     const uint32_t c = hist[b];
-                    bbase[b] = c ? atomicAdd(a.bucket_cursor + b, (unsigned long long)c) : 0ull;
+                    bbase[b] = c ? atomicAdd(a.bucket_cursor + bucket_off + b, (unsigned long long)c) : 0ull;
                     sum += c;
                 }
             }
@@ -557,7 +609,7 @@ __global__ void __launch_bounds__(EXT_THREADS) extract_kernel(ExtractArgs a) {
     if (MODE == HIST) {
         for (uint32_t b = tid; b < a.n_buckets; b += EXT_THREADS) {
             const uint32_t c = hist[b];
-            if (c) atomicAdd(a.bucket_count + b, (unsigned long long)c);
+            if (c) atomicAdd(a.bucket_count + bucket_off + b, (unsigned long long)c);
         }
     }
 }
@@ -688,6 +740,11 @@ struct CountArgs {
     uint32_t bucket_shift;
     uint32_t n_buckets;
     int use_filter;               // 0: retry pass (table only, no filter)
+    // multi-set batch: set s owns segments [set_seg_start[s], set_seg_start[s+1])
+    // and buckets [s * set_buckets, (s + 1) * set_buckets); EMPTY keys are gaps
+    const uint64_t* set_seg_start;
+    uint32_t n_sets;
+    uint32_t set_buckets;
 };
 
 // Bucket placement as read by the count kernel (shared memory copy).
@@ -759,13 +816,27 @@ __global__ void __launch_bounds__(CNT_THREADS, 4) count_routed(CountArgs a) {
             n_in = nf;
         }
 
+        uint32_t set_bucket0 = 0;
+        if (a.n_sets) {
+            uint32_t lo = 0, hi = a.n_sets;  // last set whose first segment <= gw
+            while (hi - lo > 1) {
+                const uint32_t mid = (lo + hi) / 2;
+                if (a.set_seg_start[mid] <= gw) lo = mid;
+                else hi = mid;
+            }
+            set_bucket0 = lo * a.set_buckets;
+        }
         K it[ITEMS];
         uint32_t mult[ITEMS];
 #pragma unroll
         for (int j = 0; j < ITEMS; ++j) {
             const uint32_t idx = (uint32_t)(j * 32 + lane);
             mult[j] = idx < n_in ? 1u : 0u;
-            if (mult[j]) it[j] = keys[base + idx];
+            if (mult[j]) {
+                it[j] = keys[base + idx];
+                if constexpr (NW == 1) mult[j] = it[j] != EMPTY;
+                else mult[j] = !(it[j].w0 == EMPTY && it[j].w1 == EMPTY);
+            }
         }
         __syncwarp();  // every read of the segment precedes any in-place write
 
@@ -789,7 +860,7 @@ __global__ void __launch_bounds__(CNT_THREADS, 4) count_routed(CountArgs a) {
         for (int j = 0; j < ITEMS; ++j) {
             if (mult[j]) {
                 h[j] = hash_key(it[j]);
-                const MetaS m = meta_of((uint32_t)(key_hi(it[j]) >> a.bucket_shift));
+                const MetaS m = meta_of(set_bucket0 + (uint32_t)(key_hi(it[j]) >> a.bucket_shift));
                 if (a.use_filter) old[j] = __ldcg(a.bloom + m.bloom_off + (h[j] & m.bloom_mask));
                 const S* slot = table + m.tab_off + ((h[j] >> 17) & m.tab_mask);
                 if constexpr (NW == 1) seen[j] = __ldcg(&slot->key);
@@ -803,7 +874,7 @@ __global__ void __launch_bounds__(CNT_THREADS, 4) count_routed(CountArgs a) {
                 if (mult[j]) {
                     const uint64_t bits = bloom_bits(h[j]);
                     if ((old[j] & bits) != bits) {
-                        const MetaS m = meta_of((uint32_t)(key_hi(it[j]) >> a.bucket_shift));
+                        const MetaS m = meta_of(set_bucket0 + (uint32_t)(key_hi(it[j]) >> a.bucket_shift));
                         const uint64_t o = atomicOr(
                             reinterpret_cast<unsigned long long*>(a.bloom + m.bloom_off + (h[j] & m.bloom_mask)), bits);
                         if ((o & bits) != bits) first_bits |= 1u << j;
@@ -816,7 +887,7 @@ __global__ void __launch_bounds__(CNT_THREADS, 4) count_routed(CountArgs a) {
         for (int j = 0; j < ITEMS; ++j) {
             const uint32_t reps = mult[j] - ((first_bits >> j) & 1u);
             if (mult[j] && reps) {
-                const uint32_t b = (uint32_t)(key_hi(it[j]) >> a.bucket_shift);
+                const uint32_t b = set_bucket0 + (uint32_t)(key_hi(it[j]) >> a.bucket_shift);
                 const MetaS m = meta_of(b);
                 if (!table_add_first(table + m.tab_off, m.tab_mask, h[j], it[j], reps, seen[j])) {
                     fail_bits |= 1u << j;
@@ -1244,6 +1315,72 @@ __global__ void loads_table_pass(const void* table, uint64_t n_slots, unsigned l
         if (!marked) {
             atomicAdd(distinct + (hi >> 52), 1ull);
             atomicAdd(kmers + (hi >> 52), (unsigned long long)s.count);
+        }
+    }
+}
+
+// ------------------------------------------------------- multi-set batches
+
+// EMPTY keys into the alignment gap after each set's routed region.
+template <int NW>
+__global__ void fill_set_gaps(void* routed, const uint64_t* set_end_key, const uint64_t* set_next_key, uint32_t n_sets) {
+    using K = typename KeyOf<NW>::T;
+    K* keys = reinterpret_cast<K*>(routed);
+    const uint32_t s = blockIdx.x;
+    if (s >= n_sets) return;
+    for (uint64_t i = set_end_key[s] + threadIdx.x; i < set_next_key[s]; i += blockDim.x) {
+        if constexpr (NW == 1) keys[i] = EMPTY;
+        else keys[i] = Key2{EMPTY, EMPTY};
+    }
+}
+
+// Pack first occurrences of a multi-set batch: segment sg of set s writes at
+// low_byte_base[s] + (prefix[sg] - prefix[first segment of s]) * P(k_s).
+template <int NW>
+__global__ void pack_low_sets(const void* routed, const uint32_t* seg_low, const uint64_t* seg_low_prefix, uint64_t n_segs,
+                              const uint64_t* set_seg_start, const uint32_t* set_k, const uint64_t* low_byte_base,
+                              uint32_t n_sets, uint8_t* out) {
+    using K = typename KeyOf<NW>::T;
+    constexpr int SEG = count_seg<NW>();
+    const K* keys = reinterpret_cast<const K*>(routed);
+    const int lane = threadIdx.x & 31;
+    const uint64_t warps = (uint64_t)gridDim.x * (blockDim.x >> 5);
+    for (uint64_t sg = (uint64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); sg < n_segs; sg += warps) {
+        const uint32_t n = seg_low[sg];
+        if (!n) continue;
+        uint32_t lo = 0, hi = n_sets;
+        while (hi - lo > 1) {
+            const uint32_t mid = (lo + hi) / 2;
+            if (set_seg_start[mid] <= sg) lo = mid;
+            else hi = mid;
+        }
+        const uint32_t k = set_k[lo];
+        const uint32_t full = k / 32, tail_bits = 2 * (k % 32), tail_bytes = (tail_bits + 7) / 8;
+        const uint32_t P = full * 8 + tail_bytes;
+        const uint64_t tmask = tail_bits ? (~0ull << (64 - tail_bits)) : 0ull;
+        const uint64_t first = seg_low_prefix[set_seg_start[lo]];
+        uint8_t* dst0 = out + low_byte_base[lo] + (seg_low_prefix[sg] - first) * P;
+        for (uint32_t i = lane; i < n; i += 32) {
+            const K key = keys[sg * (uint64_t)SEG + i];
+            uint64_t w0, w1;
+            if constexpr (NW == 1) {
+                w0 = key;
+                w1 = 0;
+            } else {
+                w0 = key.w0;
+                w1 = key.w1;
+            }
+            uint8_t* d = dst0 + (uint64_t)i * P;
+            uint32_t q = 0;
+            if (full) {
+                for (uint32_t b = 0; b < 8; ++b) d[q++] = (uint8_t)(w0 >> (8 * b));
+                if (full == 2)
+                    for (uint32_t b = 0; b < 8; ++b) d[q++] = (uint8_t)(w1 >> (8 * b));
+            }
+            if (tail_bytes) {
+                const uint64_t tw = (full ? w1 : w0) & tmask;
+                for (uint32_t b = 8 - tail_bytes; b < 8; ++b) d[q++] = (uint8_t)(tw >> (8 * b));
+            }
         }
     }
 }

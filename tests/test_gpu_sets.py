@@ -1,0 +1,74 @@
+"""Many read sets counted in one pass (kc_count_sets) against the oracle and
+against counting each set on its own."""
+import numpy as np
+import pytest
+
+import oracle
+import parity
+
+pytestmark = pytest.mark.gpu
+
+kc = pytest.importorskip("kmertreecounter_b200")
+torch = pytest.importorskip("torch")
+from kmertreecounter_b200 import synth  # noqa: E402
+
+
+def make_sets(ks, seed=0):
+    rng = np.random.default_rng(seed)
+    datas = []
+    for i, k in enumerate(ks):
+        L = int(rng.integers(50, 301))
+        p = synth.params(seed=1000 + seed * 97 + i, genome_len=int(rng.integers(20_000, 300_000)),
+                         gc=float(rng.uniform(0.3, 0.7)), n_reads=int(rng.integers(0, 4000)) if i % 5 else 0,
+                         read_len=(L, L), sub_rate=float(rng.uniform(0.005, 0.02)))
+        datas.append(synth.fastq(p) if p.n_reads else np.zeros(0, np.uint8))
+    offs, pos = [], 0
+    for d in datas:
+        offs.append(pos)
+        pos += (d.size + 15) // 16 * 16
+    buf = np.full(max(pos, 16), ord("\n"), np.uint8)
+    for o, d in zip(offs, datas):
+        buf[o:o + d.size] = d
+    return buf, [(o, d.size, k) for o, d, k in zip(offs, datas, ks)], datas
+
+
+def check_sets(c, res, sets, datas):
+    low_all = c.low_bytes()
+    roots_all, _ = c.root_records()
+    for (o, n, k), r, d in zip(sets, res, datas):
+        low = oracle.unpack(low_all[r.low_offset:r.low_offset + r.low_bytes], k)
+        rec = roots_all[r.root_offset:r.root_offset + r.root_records]
+        parity.check_layout(low, rec, list(r.root_counts), k)
+        mk, mc = parity.merged(low, rec, k)
+        keys, counts, K = oracle.count(d, k)
+        assert r.total_kmers == K
+        assert np.array_equal(mk, keys) and np.array_equal(mc, counts.astype(np.uint64))
+
+
+@pytest.mark.parametrize("ks,cfg", [([21, 31] * 12, {}), ([31, 21, 25] * 5, {"repeat_ratio": 1e-6}),
+                                    ([33, 63, 47, 64] * 4, {"k": 63})])
+def test_sets_match_oracle(ks, cfg):
+    buf, sets, datas = make_sets(ks, seed=len(ks))
+    d = torch.from_numpy(buf).cuda()
+    with kc.Counter(k=cfg.get("k", 31), **{k: v for k, v in cfg.items() if k != "k"}) as c:
+        res = c.count_sets(d.data_ptr(), sets)
+        if "repeat_ratio" in cfg:
+            assert c.stats.rehashes > 0
+        check_sets(c, res, sets, datas)
+
+
+def test_sets_equal_single_counts():
+    buf, sets, datas = make_sets([31] * 6, seed=9)
+    d = torch.from_numpy(buf).cuda()
+    with kc.Counter(k=31) as c:
+        res = c.count_sets(d.data_ptr(), sets)
+        lows = c.low_bytes()
+        roots_all, _ = c.root_records()
+    for (o, n, k), r, data in zip(sets, res, datas):
+        with kc.Counter(k=k) as single:
+            single.count_host(data)
+            low1, roots1, _ = parity.gpu_outputs(single, k)
+        a = parity.merged(oracle.unpack(lows[r.low_offset:r.low_offset + r.low_bytes], k),
+                          roots_all[r.root_offset:r.root_offset + r.root_records], k)
+        b = parity.merged(low1, roots1, k)
+        assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1])
