@@ -67,6 +67,12 @@ typedef struct kc_config {
     double bloom_bits;     /* first-occurrence filter bits per k-mer occurrence */
     double table_load;     /* target load factor of the repeat tables */
     double repeat_ratio;   /* sampled sizing: distinct repeat keys per k-mer */
+    uint64_t device_batch_bytes; /* FASTQ bytes per pass when the input is already in
+                                  * device memory (kc_count_device; default 8 GiB, 0 =
+                                  * batch_bytes).  Larger passes reuse each bucket's
+                                  * filter and table lines more often in L2; the cost is
+                                  * the routed-key buffer, about 3 bytes per FASTQ byte
+                                  * for k <= 32 and 6 for k <= 64. */
 } kc_config;
 
 /* Counters of one run.  total_kmers and root_records match the reference's

@@ -20,11 +20,11 @@ from ._native import Counter
 CACHE = os.path.join(os.path.expanduser("~"), ".cache", "kmertreecounter_b200", "tune.json")
 
 GRID = [
-    dict(table_load=0.7, repeat_ratio=0.125, bloom_bits=8.0),
-    dict(table_load=0.5, repeat_ratio=0.125, bloom_bits=8.0),
-    dict(table_load=0.7, repeat_ratio=0.25, bloom_bits=8.0),
-    dict(table_load=0.7, repeat_ratio=0.0625, bloom_bits=8.0),
     dict(table_load=0.7, repeat_ratio=0.125, bloom_bits=5.0),
+    dict(table_load=0.5, repeat_ratio=0.125, bloom_bits=5.0),
+    dict(table_load=0.7, repeat_ratio=0.25, bloom_bits=5.0),
+    dict(table_load=0.7, repeat_ratio=0.0625, bloom_bits=5.0),
+    dict(table_load=0.7, repeat_ratio=0.125, bloom_bits=8.0),
     dict(table_load=0.7, repeat_ratio=0.125, bloom_bits=12.0),
 ]
 SETS_PER_PASS = [64, 128, 512]

@@ -153,7 +153,7 @@ struct kc_context {
     DevBuf overflow, meta;
     DevBuf bloom, table;
     DevBuf low_packed;
-    DevBuf roots, chunks, root_count, root_cursor;
+    DevBuf roots, chunks, chunk_pass, chunk_off, root_count;
     DevBuf sort_tmp, sort_hist, sort_offs, sort_sums;
     DevBuf set_tiles, tile_prefix, set_info;  // multi-set batches
 
@@ -231,6 +231,8 @@ int setup_shape(kc_context* c) {
     if (g.bloom_bits <= 0.0 || g.table_load <= 0.05 || g.table_load > 0.95 || g.repeat_ratio <= 0.0)
         return fail(KC_ERR_INVALID, "bloom_bits, table_load (0.05..0.95) and repeat_ratio must be positive");
     if (g.batch_bytes < (1ull << 20)) return fail(KC_ERR_INVALID, "batch_bytes must be at least 1 MiB");
+    if (g.device_batch_bytes && g.device_batch_bytes < (1ull << 20))
+        return fail(KC_ERR_INVALID, "device_batch_bytes must be 0 or at least 1 MiB");
     c->nw = g.k <= 32 ? 1 : 2;
     c->n_buckets = g.n_buckets;
     c->bucket_bits = g.n_buckets == 256 ? 8 : 12;
@@ -517,6 +519,52 @@ int process_batch(kc_context* c, const uint8_t* buf, uint64_t n, int has_halo) {
     return KC_OK;
 }
 
+// Export every table slot whose count passes min..max: per-chunk counts
+// (export_count), their scan in chunk order = each chunk's first output
+// record, then one read of the table that places the records
+// (export_write).  Chunks are listed group by group (root id, or set x root
+// id), so each group's records are contiguous; totals[g] receives group g's
+// record count and totals[n_groups] the occupied slots.
+template <int NW>
+int run_export(kc_context* c, const std::vector<kc::ExportChunk>& ch, uint64_t n_groups,
+               std::vector<uint64_t>& totals) {
+    const uint64_t nch = ch.size();
+    CK(c->chunks.ensure(std::max<uint64_t>(nch, 1) * sizeof(kc::ExportChunk)));
+    CK(c->chunk_pass.ensure(std::max<uint64_t>(nch, 1) * sizeof(uint32_t)));
+    CK(c->chunk_off.ensure(std::max<uint64_t>(nch, 1) * sizeof(uint64_t)));
+    CK(c->root_count.ensure((n_groups + 1) * sizeof(uint64_t)));
+    if (nch)
+        CK(cudaMemcpyAsync(c->chunks.p, ch.data(), nch * sizeof(kc::ExportChunk), cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemsetAsync(c->root_count.p, 0, (n_groups + 1) * sizeof(uint64_t), c->stream));
+    unsigned long long* rcd = c->root_count.as<unsigned long long>();
+    const uint64_t grid = std::min<uint64_t>(std::max<uint64_t>(nch, 1), (uint64_t)c->sm_count * 8);
+    if (nch) {
+        Stage st(c, KC_STAGE_EXPORT);
+        kc::export_count<NW><<<grid, kc::EXP_THREADS, 0, c->stream>>>(
+            c->table.p, c->chunks.as<kc::ExportChunk>(), nch, c->cfg.min_count, c->cfg.max_count,
+            c->chunk_pass.as<uint32_t>(), rcd, rcd + n_groups);
+        CK(cudaGetLastError());
+    }
+    int rc;
+    if ((rc = device_scan<uint32_t, uint64_t>(c, c->chunk_pass.as<uint32_t>(), nch, c->chunk_off.as<uint64_t>(), 0,
+                                              nullptr)))
+        return rc;
+    totals.assign(n_groups + 1, 0);
+    CK(cudaMemcpyAsync(totals.data(), rcd, (n_groups + 1) * sizeof(uint64_t), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    uint64_t R = 0;
+    for (uint64_t g = 0; g < n_groups; ++g) R += totals[g];
+    CK(c->roots.ensure(std::max<uint64_t>(R, 1) * c->record_bytes));
+    if (nch && R) {
+        Stage st(c, KC_STAGE_EXPORT);
+        kc::export_write<NW><<<grid, kc::EXP_THREADS, 0, c->stream>>>(
+            c->table.p, c->chunks.as<kc::ExportChunk>(), nch, c->cfg.min_count, c->cfg.max_count,
+            c->chunk_off.as<uint64_t>(), c->roots.as<uint8_t>());
+        CK(cudaGetLastError());
+    }
+    return KC_OK;
+}
+
 template <int NW>
 int export_tables(kc_context* c) {
     const uint32_t nb = c->n_buckets;
@@ -532,39 +580,20 @@ int export_tables(kc_context* c) {
             ch.push_back(e);
         }
     }
-    CK(c->chunks.ensure(ch.size() * sizeof(kc::ExportChunk)));
-    CK(cudaMemcpyAsync(c->chunks.p, ch.data(), ch.size() * sizeof(kc::ExportChunk), cudaMemcpyHostToDevice,
-                       c->stream));
-    CK(c->root_count.ensure(257 * sizeof(uint64_t)));
-    CK(c->root_cursor.ensure(256 * sizeof(uint64_t)));
-    CK(cudaMemsetAsync(c->root_count.p, 0, 257 * sizeof(uint64_t), c->stream));
-    unsigned long long* rc_d = c->root_count.as<unsigned long long>();
-    const uint64_t grid = std::min<uint64_t>(ch.size(), 148 * 16);
-    Stage st1(c, KC_STAGE_EXPORT);
-    kc::export_count<NW><<<grid, 256, 0, c->stream>>>(c->table.p, c->chunks.as<kc::ExportChunk>(), ch.size(),
-                                                      c->cfg.min_count, c->cfg.max_count, rc_d, rc_d + 256);
-    CK(cudaGetLastError());
-    uint64_t h[257];
-    CK(cudaMemcpyAsync(h, rc_d, sizeof h, cudaMemcpyDeviceToHost, c->stream));
-    CK(cudaStreamSynchronize(c->stream));
-    uint64_t start[256], tot = 0;
+    std::vector<uint64_t> h;
+    int rc;
+    if ((rc = run_export<NW>(c, ch, 256, h))) return rc;
+    uint64_t tot = 0;
     for (int r = 0; r < 256; ++r) {
-        start[r] = tot;
         c->root_counts[r] = h[r];
         tot += h[r];
     }
     c->root_total = tot;
     c->table_keys = h[256];
-    CK(c->roots.ensure(std::max<uint64_t>(tot, 1) * c->record_bytes));
-    CK(cudaMemcpyAsync(c->root_cursor.p, start, sizeof start, cudaMemcpyHostToDevice, c->stream));
-    Stage st2(c, KC_STAGE_EXPORT);
-    kc::export_write<NW><<<grid, 256, 0, c->stream>>>(c->table.p, c->chunks.as<kc::ExportChunk>(), ch.size(),
-                                                      c->cfg.min_count, c->cfg.max_count,
-                                                      c->root_cursor.as<unsigned long long>(), c->roots.as<uint8_t>());
-    CK(cudaGetLastError());
     // Record order inside a root file is unspecified in the reference (DFS and
-    // hash-bucket order, src/NewKmerTree.h:773-859); sorting is applied by the
-    // caller of export_tables when cfg.sort_output is set.
+    // hash-bucket order, src/NewKmerTree.h:773-859); here it is table order,
+    // and sorting is applied by the caller of export_tables when
+    // cfg.sort_output is set.
     return KC_OK;
 }
 
@@ -739,9 +768,10 @@ void kc_config_default(kc_config* g) {
     g->sort_output = 0;
     g->chunk_bytes = 256ull << 20;
     g->batch_bytes = 1ull << 30;
-    g->bloom_bits = 8.0;
+    g->bloom_bits = 5.0;  // the reference sizes its filters at 4.81 bits per estimated k-mer (src/main.cpp:88-108)
     g->table_load = 0.7;
     g->repeat_ratio = 0.125;
+    g->device_batch_bytes = 8ull << 30;
 }
 
 const char* kc_last_error(void) { return g_err.c_str(); }
@@ -813,7 +843,7 @@ void kc_destroy(kc_context* c) {
     DevBuf* bufs[] = {&c->stage,  &c->tile_nl,   &c->tile_line, &c->bucket_count, &c->bucket_cursor, &c->routed,
                       &c->tile_low, &c->tile_fail, &c->tile_low_prefix, &c->scan_sums, &c->scalars, &c->overflow,
                       &c->meta,   &c->bloom,     &c->table,     &c->low_packed,   &c->roots,         &c->chunks,
-                      &c->root_count, &c->root_cursor, &c->sort_tmp, &c->sort_hist, &c->sort_offs, &c->sort_sums,
+                      &c->root_count, &c->chunk_pass, &c->chunk_off, &c->sort_tmp, &c->sort_hist, &c->sort_offs, &c->sort_sums,
                       &c->set_tiles, &c->tile_prefix, &c->set_info};
     for (DevBuf* b : bufs) b->release();
     for (cudaEvent_t e : c->ev_pool) cudaEventDestroy(e);
@@ -865,7 +895,8 @@ int kc_count_device(kc_context* c, const uint8_t* d_fastq, uint64_t n, kc_stats*
     int rc = begin_run(c, n);
     if (rc) return rc;
     CK(cudaEventRecord(c->ev0, c->stream));
-    const uint64_t B = c->cfg.batch_bytes & ~(uint64_t)(kc::EXT_TILE - 1);
+    const uint64_t want = c->cfg.device_batch_bytes ? c->cfg.device_batch_bytes : c->cfg.batch_bytes;
+    const uint64_t B = std::max<uint64_t>(kc::EXT_TILE, want & ~(uint64_t)(kc::EXT_TILE - 1));
     for (uint64_t off = 0; off < n || (n == 0 && off == 0); off += B) {
         if (n == 0) break;
         const uint64_t len = std::min<uint64_t>(B, n - off);
@@ -1420,36 +1451,14 @@ int count_sets_impl(kc_context* c, const uint8_t* buf, const kc_set_desc* sets, 
         for (uint64_t q = 0; q < slots; q += CH)
             ch.push_back(kc::ExportChunk{c->h_meta[b].tab_off + q, (uint32_t)std::min<uint64_t>(CH, slots - q), (uint32_t)b});
     }
-    CK(c->chunks.ensure(ch.size() * sizeof(kc::ExportChunk)));
-    CK(cudaMemcpyAsync(c->chunks.p, ch.data(), ch.size() * sizeof(kc::ExportChunk), cudaMemcpyHostToDevice, c->stream));
-    CK(c->root_count.ensure((nbk + 1) * sizeof(uint64_t)));
-    CK(c->root_cursor.ensure(nbk * sizeof(uint64_t)));
-    CK(cudaMemsetAsync(c->root_count.p, 0, (nbk + 1) * sizeof(uint64_t), c->stream));
-    unsigned long long* rcd = c->root_count.as<unsigned long long>();
-    const uint64_t grid = std::min<uint64_t>(ch.size(), 148 * 16);
-    {
-        Stage st(c, KC_STAGE_EXPORT);
-        kc::export_count<NW><<<grid, 256, 0, c->stream>>>(c->table.p, c->chunks.as<kc::ExportChunk>(), ch.size(),
-                                                          g.min_count, g.max_count, rcd, rcd + nbk);
-    }
-    std::vector<uint64_t> rc_h(nbk + 1);
-    CK(cudaMemcpyAsync(rc_h.data(), rcd, (nbk + 1) * sizeof(uint64_t), cudaMemcpyDeviceToHost, c->stream));
-    CK(cudaStreamSynchronize(c->stream));
+    std::vector<uint64_t> rc_h;
+    if ((rc = run_export<NW>(c, ch, nbk, rc_h))) return rc;
     std::vector<uint64_t> rstart(nbk);
     uint64_t R = 0;
     for (uint64_t b = 0; b < nbk; ++b) {
         rstart[b] = R;
         R += rc_h[b];
     }
-    CK(c->roots.ensure(std::max<uint64_t>(R, 1) * c->record_bytes));
-    CK(cudaMemcpyAsync(c->root_cursor.p, rstart.data(), nbk * sizeof(uint64_t), cudaMemcpyHostToDevice, c->stream));
-    {
-        Stage st(c, KC_STAGE_EXPORT);
-        kc::export_write<NW><<<grid, 256, 0, c->stream>>>(c->table.p, c->chunks.as<kc::ExportChunk>(), ch.size(),
-                                                          g.min_count, g.max_count, c->root_cursor.as<unsigned long long>(),
-                                                          c->roots.as<uint8_t>());
-    }
-    CK(cudaGetLastError());
     CK(cudaStreamSynchronize(c->stream));
 
     // per-set results; per-set table keys from the live table regions

@@ -832,6 +832,8 @@ __global__ void __launch_bounds__(CNT_THREADS, 4) count_routed(CountArgs a) {
         for (int j = 0; j < ITEMS; ++j) {
             const uint32_t idx = (uint32_t)(j * 32 + lane);
             mult[j] = idx < n_in ? 1u : 0u;
+            if constexpr (NW == 1) it[j] = EMPTY;
+            else it[j] = Key2{EMPTY, EMPTY};
             if (mult[j]) {
                 it[j] = keys[base + idx];
                 if constexpr (NW == 1) mult[j] = it[j] != EMPTY;
@@ -840,9 +842,23 @@ __global__ void __launch_bounds__(CNT_THREADS, 4) count_routed(CountArgs a) {
         }
         __syncwarp();  // every read of the segment precedes any in-place write
 
-        // merge equal keys: the lowest lane of a group carries the multiplicity
+        // merge equal keys: the lowest lane of a group carries the multiplicity.
+        // Equal keys inside one segment arrive in runs (a hot k-mer repeated
+        // along a read lands in consecutive routed slots), so the full match
+        // runs only when some lane's key equals its neighbour's; otherwise the
+        // warp goes on with one atomic per key, which is exact either way.
 #pragma unroll
         for (int j = 0; j < ITEMS; ++j) {
+            bool eq_next;
+            if constexpr (NW == 1) {
+                const uint64_t nx = __shfl_down_sync(0xffffffffu, it[j], 1);
+                eq_next = nx == it[j];
+            } else {
+                const uint64_t n0 = __shfl_down_sync(0xffffffffu, it[j].w0, 1);
+                const uint64_t n1 = __shfl_down_sync(0xffffffffu, it[j].w1, 1);
+                eq_next = n0 == it[j].w0 && n1 == it[j].w1;
+            }
+            if (!__any_sync(0xffffffffu, eq_next && lane < 31 && mult[j] != 0)) continue;  // warp-uniform
             const uint32_t active = __ballot_sync(0xffffffffu, mult[j] != 0);
             if (mult[j]) {
                 uint32_t same;
@@ -1025,111 +1041,136 @@ struct ExportChunk {
     uint32_t root;        // root file id of the bucket
 };
 
-// Count slots passing the filter min <= count <= max per root id
-// (src/NewKmerTree.h:1159-1168) and occupied slots overall.
 template <int NW>
-__global__ void export_count(const void* table, const ExportChunk* chunks, uint64_t n_chunks, uint32_t min_c,
-                             uint32_t max_c, unsigned long long* root_count, unsigned long long* occupied) {
+__device__ __forceinline__ bool slot_used(const typename SlotOf<NW>::T& s) {
+    if constexpr (NW == 1) return s.key != EMPTY;
+    else return !(s.w0 == EMPTY && s.w1 == EMPTY);
+}
+
+constexpr int EXP_THREADS = 256;
+constexpr int EXP_ITEMS = 4;  // slots per thread per round (strided by EXP_THREADS)
+
+// Count slots passing the filter min <= count <= max per export chunk and per
+// root id (src/NewKmerTree.h:1159-1168), and occupied slots overall.  The
+// per-chunk counts, scanned in chunk order, are the chunks' output offsets:
+// chunks are listed root by root, so each root's records are contiguous.
+template <int NW>
+__global__ void __launch_bounds__(EXP_THREADS) export_count(const void* table, const ExportChunk* chunks,
+                                                            uint64_t n_chunks, uint32_t min_c, uint32_t max_c,
+                                                            uint32_t* chunk_pass, unsigned long long* root_count,
+                                                            unsigned long long* occupied) {
     using S = typename SlotOf<NW>::T;
-    __shared__ uint32_t s_pass, s_occ;
+    __shared__ uint32_t s_pass[EXP_THREADS / 32], s_occ[EXP_THREADS / 32];
     const S* tab = reinterpret_cast<const S*>(table);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     for (uint64_t c = blockIdx.x; c < n_chunks; c += gridDim.x) {
-        if (threadIdx.x == 0) {
-            s_pass = 0;
-            s_occ = 0;
-        }
-        __syncthreads();
         const ExportChunk ch = chunks[c];
         uint32_t pass = 0, occ = 0;
-        for (uint32_t i = threadIdx.x; i < ch.n_slots; i += blockDim.x) {
-            const S s = tab[ch.slot_begin + i];
-            bool used;
-            if constexpr (NW == 1) used = s.key != EMPTY;
-            else used = !(s.w0 == EMPTY && s.w1 == EMPTY);
-            occ += used;
-            pass += used && s.count >= min_c && s.count <= max_c;
+        for (uint32_t i0 = 0; i0 < ch.n_slots; i0 += EXP_THREADS * EXP_ITEMS) {
+            S v[EXP_ITEMS];
+#pragma unroll
+            for (int j = 0; j < EXP_ITEMS; ++j) {
+                const uint32_t i = i0 + j * EXP_THREADS + threadIdx.x;
+                if (i < ch.n_slots) v[j] = tab[ch.slot_begin + i];
+            }
+#pragma unroll
+            for (int j = 0; j < EXP_ITEMS; ++j) {
+                const uint32_t i = i0 + j * EXP_THREADS + threadIdx.x;
+                if (i < ch.n_slots && slot_used<NW>(v[j])) {
+                    ++occ;
+                    pass += v[j].count >= min_c && v[j].count <= max_c;
+                }
+            }
         }
         for (int o = 16; o; o >>= 1) {
             pass += __shfl_xor_sync(0xffffffffu, pass, o);
             occ += __shfl_xor_sync(0xffffffffu, occ, o);
         }
-        if ((threadIdx.x & 31) == 0) {
-            atomicAdd(&s_pass, pass);
-            atomicAdd(&s_occ, occ);
+        if (lane == 0) {
+            s_pass[warp] = pass;
+            s_occ[warp] = occ;
         }
         __syncthreads();
         if (threadIdx.x == 0) {
-            if (s_pass) atomicAdd(root_count + ch.root, (unsigned long long)s_pass);
-            if (s_occ) atomicAdd(occupied, (unsigned long long)s_occ);
+            uint32_t tp = 0, to = 0;
+            for (int w = 0; w < EXP_THREADS / 32; ++w) {
+                tp += s_pass[w];
+                to += s_occ[w];
+            }
+            chunk_pass[c] = tp;
+            if (tp) atomicAdd(root_count + ch.root, (unsigned long long)tp);
+            if (to) atomicAdd(occupied, (unsigned long long)to);
         }
         __syncthreads();
     }
 }
 
-// Write ExportRecord<N> {key words, count, pad = 0} into each root's segment.
+// Write ExportRecord<N> {key words, count, pad = 0} of every passing slot,
+// one read of the table: chunk c's records start at chunk_off[c] and follow
+// table order (rounds of EXP_THREADS x EXP_ITEMS slots; inside a round, by
+// thread, then item).  No atomics decide positions, so the record order is a
+// function of the table alone.
 template <int NW>
-__global__ void export_write(const void* table, const ExportChunk* chunks, uint64_t n_chunks, uint32_t min_c,
-                             uint32_t max_c, unsigned long long* root_cursor, uint8_t* records) {
+__global__ void __launch_bounds__(EXP_THREADS) export_write(const void* table, const ExportChunk* chunks,
+                                                            uint64_t n_chunks, uint32_t min_c, uint32_t max_c,
+                                                            const uint64_t* chunk_off, uint8_t* records) {
     using S = typename SlotOf<NW>::T;
-    __shared__ uint32_t s_n;
-    __shared__ unsigned long long s_base;
+    __shared__ uint32_t s_warp[EXP_THREADS / 32];
     const S* tab = reinterpret_cast<const S*>(table);
-    const int lane = threadIdx.x & 31;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     for (uint64_t c = blockIdx.x; c < n_chunks; c += gridDim.x) {
         const ExportChunk ch = chunks[c];
-        // pass 1: count, reserve
-        if (threadIdx.x == 0) s_n = 0;
-        __syncthreads();
-        uint32_t pass = 0;
-        for (uint32_t i = threadIdx.x; i < ch.n_slots; i += blockDim.x) {
-            const S s = tab[ch.slot_begin + i];
-            bool used;
-            if constexpr (NW == 1) used = s.key != EMPTY;
-            else used = !(s.w0 == EMPTY && s.w1 == EMPTY);
-            pass += used && s.count >= min_c && s.count <= max_c;
-        }
-        for (int o = 16; o; o >>= 1) pass += __shfl_xor_sync(0xffffffffu, pass, o);
-        if (lane == 0 && pass) atomicAdd(&s_n, pass);
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            s_base = s_n ? atomicAdd(root_cursor + ch.root, (unsigned long long)s_n) : 0ull;
-            s_n = 0;
-        }
-        __syncthreads();
-        // pass 2: place
-        for (uint32_t i0 = 0; i0 < ch.n_slots; i0 += blockDim.x) {
-            const uint32_t i = i0 + threadIdx.x;
-            bool keep = false;
-            S s;
-            if (i < ch.n_slots) {
-                s = tab[ch.slot_begin + i];
-                bool used;
-                if constexpr (NW == 1) used = s.key != EMPTY;
-                else used = !(s.w0 == EMPTY && s.w1 == EMPTY);
-                keep = used && s.count >= min_c && s.count <= max_c;
-            }
-            const uint32_t m = __ballot_sync(0xffffffffu, keep);
-            uint32_t wb = 0;
-            if (lane == 0 && m) wb = atomicAdd(&s_n, __popc(m));
-            wb = __shfl_sync(0xffffffffu, wb, 0);
-            if (keep) {
-                const unsigned long long r = s_base + wb + __popc(m & ((1u << lane) - 1u));
-                if constexpr (NW == 1) {
-                    uint4 v;
-                    v.x = (uint32_t)s.key;
-                    v.y = (uint32_t)(s.key >> 32);
-                    v.z = s.count;
-                    v.w = 0;
-                    reinterpret_cast<uint4*>(records)[r] = v;
-                } else {
-                    uint64_t* d = reinterpret_cast<uint64_t*>(records + r * 24);
-                    d[0] = s.w0;
-                    d[1] = s.w1;
-                    d[2] = (uint64_t)s.count;
+        uint64_t out = chunk_off[c];
+        for (uint32_t i0 = 0; i0 < ch.n_slots; i0 += EXP_THREADS * EXP_ITEMS) {
+            S v[EXP_ITEMS];
+            uint32_t keep = 0;
+#pragma unroll
+            for (int j = 0; j < EXP_ITEMS; ++j) {
+                const uint32_t i = i0 + j * EXP_THREADS + threadIdx.x;
+                if (i < ch.n_slots) {
+                    v[j] = tab[ch.slot_begin + i];
+                    if (slot_used<NW>(v[j]) && v[j].count >= min_c && v[j].count <= max_c) keep |= 1u << j;
                 }
             }
+            // block-wide exclusive scan of the per-thread keep counts
+            const uint32_t mine = __popc(keep);
+            uint32_t incl = mine;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+                if (lane >= o) incl += y;
+            }
+            if (lane == 31) s_warp[warp] = incl;
+            __syncthreads();
+            uint32_t before = 0, total = 0;
+#pragma unroll
+            for (int w = 0; w < EXP_THREADS / 32; ++w) {
+                const uint32_t t = s_warp[w];
+                before += w < warp ? t : 0u;
+                total += t;
+            }
+            __syncthreads();  // s_warp is rewritten next round
+            uint64_t r = out + before + incl - mine;
+#pragma unroll
+            for (int j = 0; j < EXP_ITEMS; ++j) {
+                if (!((keep >> j) & 1u)) continue;
+                if constexpr (NW == 1) {
+                    uint4 w;
+                    w.x = (uint32_t)v[j].key;
+                    w.y = (uint32_t)(v[j].key >> 32);
+                    w.z = v[j].count;
+                    w.w = 0;
+                    reinterpret_cast<uint4*>(records)[r] = w;
+                } else {
+                    uint64_t* d = reinterpret_cast<uint64_t*>(records + r * 24);
+                    d[0] = v[j].w0;
+                    d[1] = v[j].w1;
+                    d[2] = (uint64_t)v[j].count;
+                }
+                ++r;
+            }
+            out += total;
         }
-        __syncthreads();
     }
 }
 

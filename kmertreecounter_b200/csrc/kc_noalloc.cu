@@ -95,7 +95,9 @@ int run(const kc_config* g, const uint8_t* d_fastq, uint64_t n, uint8_t* d_low, 
     uint32_t* overflow = cv.take<uint32_t>(NB);
     kc::BucketMeta* meta = cv.take<kc::BucketMeta>(NB);
     unsigned long long* rcount = cv.take<unsigned long long>(257);
-    unsigned long long* rcursor = cv.take<unsigned long long>(256);
+    constexpr uint64_t MAX_CHUNKS = 1024;
+    uint32_t* chunk_pass = cv.take<uint32_t>(MAX_CHUNKS);
+    uint64_t* chunk_off = cv.take<uint64_t>(MAX_CHUNKS);
     if (!cv.ok) return err(KC_ERR_OVERFLOW, "no-alloc scratch exhausted (fixed part)");
     NK(cudaMemsetAsync(scal, 0, 16 * sizeof(uint64_t), st));
 
@@ -229,12 +231,12 @@ int run(const kc_config* g, const uint8_t* d_fastq, uint64_t n, uint8_t* d_low, 
                                                                                        nsegs, k, d_low, 0);
 
     // root records grouped by root id
-    kc::ExportChunk h_chunks[1024];
+    kc::ExportChunk h_chunks[MAX_CHUNKS];
     uint64_t nch = 0;
     const uint64_t CH = std::max<uint64_t>(16384, cdiv(ts, 700));
     for (int b = 0; b < NB; ++b) {
         const uint64_t slots = h_meta[b].tab_mask + 1;
-        for (uint64_t s = 0; s < slots && nch < 1024; s += CH)
+        for (uint64_t s = 0; s < slots && nch < MAX_CHUNKS; s += CH)
             h_chunks[nch++] = kc::ExportChunk{h_meta[b].tab_off + s, (uint32_t)std::min<uint64_t>(CH, slots - s), (uint32_t)b};
     }
     kc::ExportChunk* chunks = reinterpret_cast<kc::ExportChunk*>(table + ts);
@@ -242,21 +244,28 @@ int run(const kc_config* g, const uint8_t* d_fastq, uint64_t n, uint8_t* d_low, 
         return err(KC_ERR_OVERFLOW, "no-alloc scratch exhausted at export");
     NK(cudaMemcpyAsync(chunks, h_chunks, nch * sizeof(kc::ExportChunk), cudaMemcpyHostToDevice, st));
     NK(cudaMemsetAsync(rcount, 0, 257 * sizeof(uint64_t), st));
-    kc::export_count<NW><<<std::min<uint64_t>(nch, 148 * 4), 256, 0, st>>>(table, chunks, nch, g->min_count,
-                                                                             g->max_count, rcount, rcount + 256);
+    const uint64_t egrid = std::max<uint64_t>(1, std::min<uint64_t>(nch, 148 * 4));
+    if (nch)
+        kc::export_count<NW><<<egrid, kc::EXP_THREADS, 0, st>>>(table, chunks, nch, g->min_count, g->max_count,
+                                                                chunk_pass, rcount, rcount + 256);
     uint64_t h_r[257];
+    uint32_t h_pass[MAX_CHUNKS];
     NK(cudaMemcpyAsync(h_r, rcount, sizeof h_r, cudaMemcpyDeviceToHost, st));
+    if (nch) NK(cudaMemcpyAsync(h_pass, chunk_pass, nch * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
     NK(cudaStreamSynchronize(st));
-    uint64_t rstart[256], R = 0;
-    for (int r = 0; r < 256; ++r) {
-        rstart[r] = R;
-        R += h_r[r];
+    uint64_t R = 0;
+    for (int r = 0; r < 256; ++r) R += h_r[r];
+    uint64_t h_off[MAX_CHUNKS];
+    for (uint64_t i = 0, o = 0; i < nch; ++i) {
+        h_off[i] = o;
+        o += h_pass[i];
     }
     const uint64_t rec = kc_record_bytes(k);
     if (R * rec > roots_cap) return err(KC_ERR_INVALID, "root output buffer too small");
-    NK(cudaMemcpyAsync(rcursor, rstart, sizeof rstart, cudaMemcpyHostToDevice, st));
-    kc::export_write<NW><<<std::min<uint64_t>(nch, 148 * 4), 256, 0, st>>>(table, chunks, nch, g->min_count,
-                                                                             g->max_count, rcursor, d_roots);
+    if (nch) NK(cudaMemcpyAsync(chunk_off, h_off, nch * sizeof(uint64_t), cudaMemcpyHostToDevice, st));
+    if (nch && R)
+        kc::export_write<NW><<<egrid, kc::EXP_THREADS, 0, st>>>(table, chunks, nch, g->min_count, g->max_count,
+                                                                chunk_off, d_roots);
     NK(cudaGetLastError());
     NK(cudaStreamSynchronize(st));
     if (stats) {

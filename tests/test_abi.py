@@ -39,11 +39,37 @@ def test_sizes():
 
 
 @pytest.mark.parametrize("field,value", [("k", 0), ("k", 65), ("canonical", 0), ("n_buckets", 100),
-                                         ("table_load", 0.99), ("batch_bytes", 1000)])
+                                         ("table_load", 0.99), ("batch_bytes", 1000),
+                                         ("device_batch_bytes", 4096)])
 def test_invalid_config_rejected_before_device(field, value):
     with pytest.raises(kc.KcError) as e:
         kc.Counter(kc.default_config(**{field: value}))
     assert e.value.code == kc.KC_ERR_INVALID
+
+
+def test_struct_layout_matches_header(tmp_path):
+    """Every ctypes mirror of a header struct has the C compiler's size and
+    field offsets."""
+    structs = {"kc_config": _native.KcConfig, "kc_stats": _native.KcStats,
+               "kc_set_desc": _native.KcSetDesc, "kc_set_result": _native.KcSetResult}
+    lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "kmer_count.h"', "int main(void) {"]
+    for cname, py in structs.items():
+        lines.append(f'printf("{cname} size %zu\\n", sizeof({cname}));')
+        for f in py._fields_:
+            lines.append(f'printf("{cname} {f[0]} %zu\\n", offsetof({cname}, {f[0]}));')
+    lines.append("return 0; }")
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines))
+    exe = tmp_path / "layout"
+    subprocess.check_call(["gcc", "-std=c11", "-I", os.path.join(ROOT, "include"), "-o", str(exe), str(src)])
+    got = {}
+    for line in subprocess.check_output([str(exe)], text=True).splitlines():
+        s, f, v = line.split()
+        got[(s, f)] = int(v)
+    for cname, py in structs.items():
+        assert got[(cname, "size")] == C.sizeof(py), cname
+        for f in py._fields_:
+            assert got[(cname, f[0])] == getattr(py, f[0]).offset, (cname, f[0])
 
 
 def test_min_max_order_rejected():
