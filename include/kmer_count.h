@@ -91,12 +91,16 @@ typedef struct kc_stats {
     double wall_ms;
     uint64_t table_slots;     /* repeat-table slots in use at the end (after any growth) */
     uint64_t filter_words;    /* 64-bit words of the first-occurrence filter */
+    uint64_t overflow_keys;   /* keys routed past their estimated bucket region */
+    uint64_t reroutes;        /* batches routed again from an exact histogram */
 } kc_stats;
 
 typedef struct kc_context kc_context;
 
 /* Defaults: k=31, canonical=1, min=1, max=UINT32_MAX, 256 buckets, sampled
- * sizing, device 0, unsorted roots, 256 MiB chunks, 1 GiB batches. */
+ * sizing, device 0, unsorted roots, 256 MiB chunks, 1 GiB host batches,
+ * 8 GiB device batches, 5 filter bits per k-mer, table load 0.7, repeat
+ * ratio 0.125. */
 void kc_config_default(kc_config* cfg);
 
 /* Thread-local message for the last failing call on this thread. */

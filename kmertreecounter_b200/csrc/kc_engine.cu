@@ -146,7 +146,7 @@ struct kc_context {
     // batch pipeline
     DevBuf stage;        // [HALO | batch | pad] for host input
     DevBuf tile_nl, tile_line;
-    DevBuf bucket_count, bucket_cursor;
+    DevBuf bucket_count, bucket_cursor, region_end, region_fill;
     DevBuf routed;
     DevBuf tile_low, tile_fail, tile_low_prefix;
     DevBuf scan_sums, scalars;
@@ -171,6 +171,7 @@ struct kc_context {
     uint64_t last_batch_low = 0;
     uint64_t K = 0;
     uint64_t rehashes = 0, batches = 0, input_bytes = 0;
+    uint64_t overflow_keys = 0, reroutes = 0;  // estimated bucket regions (kc_stats)
     bool have_result = false;
     bool batch_result = false;   // last result came from kc_count_sets
     uint64_t batch_low_bytes = 0;
@@ -386,9 +387,13 @@ int rehash_loop(kc_context* c, uint64_t n_keys) {
     }
 }
 
+// mode HIST: per-bucket totals over every `stride`-th tile.  mode SCATTER:
+// keys into the bucket regions (estimated regions with an overflow area when
+// `estimated`, else exact).
 template <int NW>
-int launch_extract(kc_context* c, const uint8_t* buf, uint64_t n, int has_halo, int mode) {
-    const uint64_t tiles = ceil_div(n, kc::EXT_TILE);
+int launch_extract(kc_context* c, const uint8_t* buf, uint64_t n, int has_halo, int mode, uint32_t stride = 1,
+                   bool estimated = false, uint64_t overflow_start = 0, uint64_t overflow_end = 0) {
+    const uint64_t tiles = ceil_div(ceil_div(n, kc::EXT_TILE), std::max<uint32_t>(stride, 1));
     if (!tiles) return KC_OK;
     kc::ExtractArgs a{};
     a.buf = buf;
@@ -402,6 +407,14 @@ int launch_extract(kc_context* c, const uint8_t* buf, uint64_t n, int has_halo, 
     a.bucket_cursor = c->bucket_cursor.as<unsigned long long>();
     a.routed = c->routed.p;
     a.error = c->scalars.as<uint32_t>() + 12;
+    a.tile_stride = stride;
+    if (estimated) {
+        a.region_end = c->region_end.as<unsigned long long>();
+        a.region_fill = c->region_fill.as<unsigned long long>();
+        a.overflow_cursor = reinterpret_cast<unsigned long long*>(c->scalars.as<uint64_t>() + 2);
+        a.overflow_start = overflow_start;
+        a.overflow_end = overflow_end;
+    }
     Stage st(c, mode == kc::HIST ? KC_STAGE_EXTRACT_HIST : KC_STAGE_EXTRACT_SCATTER);
     if (mode == kc::HIST)
         kc::extract_kernel<NW, kc::HIST>
@@ -437,48 +450,107 @@ int process_batch(kc_context* c, const uint8_t* buf, uint64_t n, int has_halo) {
 
     CK(c->bucket_count.ensure(nb * sizeof(uint64_t)));
     CK(c->bucket_cursor.ensure(nb * sizeof(uint64_t)));
-    CK(cudaMemsetAsync(c->bucket_count.p, 0, nb * sizeof(uint64_t), c->stream));
-    if ((rc = launch_extract<NW>(c, buf, n, has_halo, kc::HIST))) return rc;
+    CK(c->region_end.ensure(nb * sizeof(uint64_t)));
+    CK(c->region_fill.ensure(nb * sizeof(uint64_t)));
 
-    c->h_bucket_count.resize(nb);
-    uint64_t line_end = 0;
-    CK(cudaMemcpyAsync(c->h_bucket_count.data(), c->bucket_count.p, nb * sizeof(uint64_t), cudaMemcpyDeviceToHost,
-                       c->stream));
-    CK(cudaMemcpyAsync(&line_end, d_scal + 0, sizeof(uint64_t), cudaMemcpyDeviceToHost, c->stream));
-    CK(cudaStreamSynchronize(c->stream));
-    c->line_base = line_end;
-
-    uint64_t kb = 0;
-    std::vector<uint64_t> start(nb);
-    for (uint32_t b = 0; b < nb; ++b) {
-        start[b] = kb;
-        kb += c->h_bucket_count[b];
-    }
-    c->K += kb;
-    if (!c->sized) {
-        double scale = 1.0;
-        if (c->expected_total_bytes > n && n > 0) scale = (double)c->expected_total_bytes / (double)n;
-        if ((rc = size_structures(c, c->h_bucket_count, scale))) return rc;
-    }
-    if (!kb) return KC_OK;
-
+    // Bucket regions.  A large batch takes them from a histogram of every
+    // EST_STRIDE-th tile: region = estimate x 1.02 + 4 standard deviations +
+    // 256 keys, and a CTA's keys past its region go to an overflow area after
+    // the regions (counted like the rest; the unfilled region tails hold EMPTY
+    // keys, which the count kernel skips).  If the overflow area itself fills,
+    // the batch is routed again from an exact histogram of every tile.
     constexpr int CT = kc::count_tile<NW>();
     constexpr int SEG = kc::count_seg<NW>();
-    const uint64_t ctiles = ceil_div(kb, CT);
-    const uint64_t nsegs = ceil_div(kb, SEG);
-    CK(c->routed.ensure(ctiles * CT * (uint64_t)(8 * NW)));
-    CK(c->tile_low.ensure(ctiles * (CT / SEG) * sizeof(uint32_t)));
-    CK(c->tile_fail.ensure(ctiles * (CT / SEG) * sizeof(uint32_t)));
-    CK(c->tile_low_prefix.ensure(ctiles * (CT / SEG) * sizeof(uint64_t)));
-    CK(cudaMemcpyAsync(c->bucket_cursor.p, start.data(), nb * sizeof(uint64_t), cudaMemcpyHostToDevice, c->stream));
-    if ((rc = launch_extract<NW>(c, buf, n, has_halo, kc::SCATTER))) return rc;
+    bool est = nb <= 256 && tiles >= kc::EST_MIN_TILES;
+    std::vector<uint64_t> start(nb), end(nb), cursor(nb);
+    uint64_t n_keys = 0, kb = 0;
+    for (int attempt = 0;; ++attempt) {
+        const uint32_t stride = est ? kc::EST_STRIDE : 1u;
+        CK(cudaMemsetAsync(c->bucket_count.p, 0, nb * sizeof(uint64_t), c->stream));
+        if ((rc = launch_extract<NW>(c, buf, n, has_halo, kc::HIST, stride))) return rc;
+        c->h_bucket_count.resize(nb);
+        uint64_t line_end = 0;
+        CK(cudaMemcpyAsync(c->h_bucket_count.data(), c->bucket_count.p, nb * sizeof(uint64_t), cudaMemcpyDeviceToHost,
+                           c->stream));
+        CK(cudaMemcpyAsync(&line_end, d_scal + 0, sizeof(uint64_t), cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
+        if (attempt == 0) c->line_base = line_end;
+
+        std::vector<uint64_t> kest(nb);
+        uint64_t total_cap = 0;
+        const double f = est ? (double)tiles / (double)ceil_div(tiles, stride) : 1.0;
+        for (uint32_t b = 0; b < nb; ++b) {
+            const double e = (double)c->h_bucket_count[b] * f;
+            kest[b] = (uint64_t)e;
+            const uint64_t cap = est ? (uint64_t)(e * 1.02 + 4.0 * std::sqrt(e) + 256.0) : c->h_bucket_count[b];
+            start[b] = total_cap;
+            total_cap += cap;
+            end[b] = total_cap;
+        }
+        // at least 65536 keys: one CTA's run of a bucket (<= 8192 keys) always fits
+        const uint64_t ovf_cap = est ? std::max<uint64_t>(1ull << 16, total_cap / 32) : 0;
+        if (!c->sized) {
+            double scale = 1.0;
+            if (c->expected_total_bytes > n && n > 0) scale = (double)c->expected_total_bytes / (double)n;
+            if ((rc = size_structures(c, kest, scale))) return rc;
+        }
+        if (!total_cap) return KC_OK;  // no k-mers in this batch
+
+        const uint64_t cap_keys = total_cap + ovf_cap;
+        const uint64_t ctiles = ceil_div(cap_keys, CT);
+        CK(c->routed.ensure(ctiles * CT * (uint64_t)(8 * NW)));
+        CK(c->tile_low.ensure(ctiles * (CT / SEG) * sizeof(uint32_t)));
+        CK(c->tile_fail.ensure(ctiles * (CT / SEG) * sizeof(uint32_t)));
+        CK(c->tile_low_prefix.ensure(ctiles * (CT / SEG) * sizeof(uint64_t)));
+        CK(cudaMemcpyAsync(c->bucket_cursor.p, start.data(), nb * sizeof(uint64_t), cudaMemcpyHostToDevice, c->stream));
+        if (est) {
+            CK(cudaMemcpyAsync(c->region_end.p, end.data(), nb * sizeof(uint64_t), cudaMemcpyHostToDevice, c->stream));
+            CK(cudaMemcpyAsync(d_scal + 2, &total_cap, sizeof(uint64_t), cudaMemcpyHostToDevice, c->stream));
+            CK(cudaMemsetAsync(c->region_fill.p, 0xFF, nb * sizeof(uint64_t), c->stream));
+        }
+        if ((rc = launch_extract<NW>(c, buf, n, has_halo, kc::SCATTER, 1, est, total_cap, cap_keys))) return rc;
+        if (!est) {
+            n_keys = kb = total_cap;
+            break;
+        }
+        uint64_t ovf_used = 0;
+        uint32_t flags = 0;
+        CK(cudaMemcpyAsync(cursor.data(), c->bucket_cursor.p, nb * sizeof(uint64_t), cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaMemcpyAsync(&ovf_used, d_scal + 2, sizeof(uint64_t), cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaMemcpyAsync(&flags, c->scalars.as<uint32_t>() + 12, sizeof(uint32_t), cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
+        if (flags & 2u) {  // overflow area full: route this batch again, exactly
+            CK(cudaMemsetAsync(c->scalars.as<uint32_t>() + 12, 0, sizeof(uint32_t), c->stream));
+            est = false;
+            ++c->reroutes;
+            continue;
+        }
+        c->overflow_keys += ovf_used - total_cap;
+        kb = 0;
+        for (uint32_t b = 0; b < nb; ++b) {
+            c->h_bucket_count[b] = cursor[b] - start[b];
+            kb += c->h_bucket_count[b];
+        }
+        n_keys = ovf_used;  // regions, then the used part of the overflow area
+        {
+            Stage st(c, KC_STAGE_EXTRACT_SCATTER);
+            if (nb)
+                kc::fill_region_gaps<NW><<<nb, 256, 0, c->stream>>>(
+                    c->routed.p, c->bucket_cursor.as<unsigned long long>(), c->region_fill.as<unsigned long long>(),
+                    c->region_end.as<unsigned long long>(), nb);
+            CK(cudaGetLastError());
+        }
+        break;
+    }
+    c->K += kb;
     if (c->after_scatter) CK(cudaEventRecord(c->after_scatter, c->stream));
     uint32_t ext_err = 0;
     CK(cudaMemcpyAsync(&ext_err, c->scalars.as<uint32_t>() + 12, sizeof(uint32_t), cudaMemcpyDeviceToHost, c->stream));
 
-    launch_count<NW>(c, kb, 1);
+    const uint64_t nsegs = ceil_div(n_keys, SEG);
+    launch_count<NW>(c, n_keys, 1);
     CK(cudaGetLastError());
-    if ((rc = rehash_loop<NW>(c, kb))) return rc;
+    if ((rc = rehash_loop<NW>(c, n_keys))) return rc;
 
     // first occurrences -> packed low.bin bytes
     if ((rc = device_scan<uint32_t, uint64_t>(c, c->tile_low.as<uint32_t>(), nsegs,
@@ -603,6 +675,8 @@ int begin_run(kc_context* c, uint64_t total_bytes) {
     c->low_total = 0;
     c->K = 0;
     c->rehashes = 0;
+    c->overflow_keys = 0;
+    c->reroutes = 0;
     c->batches = 0;
     c->input_bytes = 0;
     c->sized = false;
@@ -669,6 +743,8 @@ void fill_stats(kc_context* c, kc_stats* s, double dev_ms, double wall_ms) {
     for (const auto& m : c->h_meta) live += m.tab_mask + 1;
     s->table_slots = live;
     s->filter_words = c->bloom_words;
+    s->overflow_keys = c->overflow_keys;
+    s->reroutes = c->reroutes;
 }
 
 // Deliver completed device->host pieces in order; `all` waits for every one.
@@ -840,7 +916,7 @@ void kc_destroy(kc_context* c) {
     if (!c) return;
     cudaSetDevice(c->device);
     if (c->stream) cudaStreamSynchronize(c->stream);
-    DevBuf* bufs[] = {&c->stage,  &c->tile_nl,   &c->tile_line, &c->bucket_count, &c->bucket_cursor, &c->routed,
+    DevBuf* bufs[] = {&c->stage,  &c->tile_nl,   &c->tile_line, &c->bucket_count, &c->bucket_cursor, &c->region_end, &c->region_fill, &c->routed,
                       &c->tile_low, &c->tile_fail, &c->tile_low_prefix, &c->scan_sums, &c->scalars, &c->overflow,
                       &c->meta,   &c->bloom,     &c->table,     &c->low_packed,   &c->roots,         &c->chunks,
                       &c->root_count, &c->chunk_pass, &c->chunk_off, &c->sort_tmp, &c->sort_hist, &c->sort_offs, &c->sort_sums,

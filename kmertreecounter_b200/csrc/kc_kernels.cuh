@@ -52,6 +52,10 @@ constexpr int EXT_THREADS = 256;                     // extraction CTA
 constexpr int EXT_BPT = 32;                          // bytes per thread
 constexpr int EXT_TILE = EXT_THREADS * EXT_BPT;      // 8 KiB per CTA
 constexpr int HALO = 64;                             // bytes kept before a batch
+// Bucket regions of a batch of at least EST_MIN_TILES tiles are sized from a
+// histogram of every EST_STRIDE-th tile instead of all of them.
+constexpr uint32_t EST_STRIDE = 32;
+constexpr uint64_t EST_MIN_TILES = 4096;
 constexpr int CNT_THREADS = 256;                     // count CTA
 constexpr uint64_t EMPTY = ~0ull;                    // never a canonical key
 constexpr int PROBE_LIMIT = 512;                     // linear-probe bound before overflow
@@ -379,7 +383,18 @@ struct ExtractArgs {
     unsigned long long* bucket_count;  // HIST: per-bucket totals (accumulated)
     unsigned long long* bucket_cursor; // SCATTER: next free index per bucket
     void* routed;            // SCATTER: routed key array
-    uint32_t* error;         // set when a key's bucket disagrees with its reservation
+    uint32_t* error;         // bit 0: a key's bucket disagreed with its reservation;
+                             // bit 1: the overflow area was full (keys dropped)
+    uint32_t tile_stride;    // HIST over every tile_stride-th tile only (0 or 1: all)
+    // SCATTER into estimated regions: bucket b owns routed[cursor0[b], region_end[b]).
+    // A CTA's run of bucket b that does not fit whole goes whole to the overflow
+    // area routed[overflow_start, overflow_end) (cursor *overflow_cursor), and
+    // region_fill[b] (atomicMin) records where the region stopped filling.
+    // region_end == nullptr: the regions are exact (no overflow).
+    const unsigned long long* region_end;
+    unsigned long long* region_fill;
+    unsigned long long* overflow_cursor;
+    uint64_t overflow_start, overflow_end;
 };
 
 // Bucket of the canonical key of window (hi:lo) without building the key:
@@ -433,14 +448,13 @@ __host__ __device__ constexpr int stage_keys() {
 // Dynamic shared memory of extract_kernel.
 template <int NW, int MODE>
 __host__ __device__ constexpr size_t extract_smem_bytes(uint32_t n_buckets) {
-    return (size_t)n_buckets * (8 + 4 + 4 + 4) +
-           (MODE == SCATTER ? (size_t)stage_keys<NW>() * (8 * NW + 2) : 0);
+    return (size_t)n_buckets * (8 + 4 + 4 + 4) + (MODE == SCATTER ? (size_t)stage_keys<NW>() * (8 * NW + 2) : 0);
 }
 
 template <int NW, int MODE>
 __global__ void __launch_bounds__(EXT_THREADS) extract_kernel(ExtractArgs a) {
     // dynamic smem: u64 base[nb] | u32 hist[nb] | u32 fill[nb] | u32 loff[nb]
-    //               | K keys[stage] | u16 bucket_of_key[stage]
+    //               | SCATTER: K keys[stage] | u16 bucket_of_key[stage]
     extern __shared__ unsigned long long ext_smem[];
     __shared__ uint64_t seg_codes[EXT_THREADS + 2];
     __shared__ uint32_t seg_bases[EXT_THREADS + 2];
@@ -457,7 +471,8 @@ __global__ void __launch_bounds__(EXT_THREADS) extract_kernel(ExtractArgs a) {
     uint16_t* sbkt = reinterpret_cast<uint16_t*>(skeys + STAGE);
 
     const int tid = threadIdx.x;
-    uint64_t tile_start = (uint64_t)blockIdx.x * EXT_TILE;
+    const uint64_t tile = (uint64_t)blockIdx.x * (a.tile_stride > 1 ? a.tile_stride : 1u);
+    uint64_t tile_start = tile * EXT_TILE;
     uint64_t n_end = a.n;
     bool halo_ok = tile_start > 0 || a.has_halo;
     uint32_t k = a.k;
@@ -497,7 +512,7 @@ __global__ void __launch_bounds__(EXT_THREADS) extract_kernel(ExtractArgs a) {
     uint32_t nl_total;
     const uint32_t nl_before = block_exclusive_scan<EXT_THREADS>(__popc(s.nls), warp_sums, &nl_total);
     (void)nl_total;  // the scan synchronised the block: seg_* are visible
-    const uint32_t line0 = (uint32_t)a.tile_line[blockIdx.x] + nl_before;
+    const uint32_t line0 = (uint32_t)a.tile_line[tile] + nl_before;
 
     uint32_t emit = 0;
     if (s.bases) {
@@ -529,7 +544,23 @@ __global__ void __launch_bounds__(EXT_THREADS) extract_kernel(ExtractArgs a) {
                 const uint32_t b = tid * per + q;
                 if (b < a.n_buckets) {
                     const uint32_t c = hist[b];
-                    bbase[b] = c ? atomicAdd(a.bucket_cursor + bucket_off + b, (unsigned long long)c) : 0ull;
+                    unsigned long long base =
+                        c ? atomicAdd(a.bucket_cursor + bucket_off + b, (unsigned long long)c) : 0ull;
+                    if (a.region_end && c && base + c > a.region_end[b]) {
+                        // the run does not fit the region: it goes whole to the
+                        // overflow area.  If that is full too, the batch is routed
+                        // again (error bit 1) and the run lands, in bounds, at the
+                        // overflow area's start (at least 65536 keys >= one run).
+                        atomicMin(a.region_fill + b, base);
+                        const unsigned long long ob = atomicAdd(a.overflow_cursor, (unsigned long long)c);
+                        if (ob + c <= a.overflow_end) {
+                            base = ob;
+                        } else {
+                            base = a.overflow_start;
+                            atomicOr(a.error, 2u);
+                        }
+                    }
+                    bbase[b] = base;
                     sum += c;
                 }
             }
@@ -1357,6 +1388,22 @@ __global__ void loads_table_pass(const void* table, uint64_t n_slots, unsigned l
             atomicAdd(distinct + (hi >> 52), 1ull);
             atomicAdd(kmers + (hi >> 52), (unsigned long long)s.count);
         }
+    }
+}
+
+// EMPTY keys into the unfilled tail of each estimated bucket region:
+// routed[min(cursor[b], region_fill[b], region_end[b]), region_end[b]).
+template <int NW>
+__global__ void fill_region_gaps(void* routed, const unsigned long long* cursor, const unsigned long long* region_fill,
+                                 const unsigned long long* region_end, uint32_t n_buckets) {
+    using K = typename KeyOf<NW>::T;
+    K* keys = reinterpret_cast<K*>(routed);
+    const uint32_t b = blockIdx.x;
+    if (b >= n_buckets) return;
+    const unsigned long long end = region_end[b];
+    for (unsigned long long i = min(min(cursor[b], region_fill[b]), end) + threadIdx.x; i < end; i += blockDim.x) {
+        if constexpr (NW == 1) keys[i] = EMPTY;
+        else keys[i] = Key2{EMPTY, EMPTY};
     }
 }
 
