@@ -20,7 +20,11 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <condition_variable>
+#include <deque>
+#include <mutex>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include <cuda_runtime.h>
@@ -130,7 +134,8 @@ struct kc_context {
     bool stream_low = false;
     kc_sink_fn sink = nullptr;
     void* sink_user = nullptr;
-    int sink_rc = 0;
+    int sink_rc = 0;        // first non-zero sink return (guarded by pin_mu)
+    bool deliver_err = false;  // a piece's copy failed (guarded by pin_mu)
     static constexpr uint64_t PIN_BYTES = 512ull << 20;
     static constexpr int PIN_SLOTS = 4;
     uint8_t* pin[PIN_SLOTS] = {};
@@ -141,7 +146,14 @@ struct kc_context {
         uint64_t bytes;
         int slot;
     };
-    std::vector<Piece> pending;  // FIFO of in-flight device->host pieces
+    // FIFO of in-flight device->host pieces, delivered to the sink in order by
+    // the `deliverer` thread; slot_busy / pending / flags are guarded by pin_mu
+    std::deque<Piece> pending;
+    bool slot_busy[PIN_SLOTS] = {};
+    bool deliver_stop = false;
+    std::mutex pin_mu;
+    std::condition_variable pin_cv;
+    std::thread deliverer;
 
     // batch pipeline
     DevBuf stage;        // [HALO | batch | pad] for host input
@@ -180,6 +192,19 @@ struct kc_context {
 
     // optional learned sizing hook (per-bucket repeat-key predictions)
     std::vector<double> pred_distinct, pred_table;  // learned sizing, per model bucket (4096)
+
+    // control-path mailbox: mapped pinned memory, [0, MBOX_UP) for uploads and
+    // [MBOX_UP, MBOX_UP + MBOX_DOWN) for readbacks (put / get / sync_stream)
+    static constexpr uint64_t MBOX_UP = 512ull << 10, MBOX_DOWN = 512ull << 10;
+    uint8_t* mbox_h = nullptr;
+    uint8_t* mbox_d = nullptr;
+    uint64_t mbox_up_off = 0, mbox_down_off = 0;
+    cudaEvent_t ev_mbox = nullptr;
+    struct Readback {
+        void* dst;
+        uint64_t off, bytes;
+    };
+    std::vector<Readback> readbacks;
 
     // stage profiling: CUDA event pairs recorded on `stream` around each stage
     bool profiling = false;
@@ -244,6 +269,80 @@ int setup_shape(kc_context* c) {
     return KC_OK;
 }
 
+// Control-path transfers on `stream`.  The copy engines carry the bulk
+// FASTQ batches (h2d stream) and output pieces (d2h stream); a small
+// cudaMemcpyAsync/cudaMemsetAsync on `stream` would queue behind them and
+// hold up the batch it belongs to.  So: fills run as a kernel, uploads are
+// staged in the mapped mailbox and copied in by a kernel, readbacks are
+// copied out to the mailbox by a kernel and land in their host destination
+// at the next sync_stream().  Sizes and addresses must be 4-byte multiples;
+// anything else, or larger than the mailbox, takes cudaMemcpyAsync.
+int fill_dev(kc_context* c, void* dst, uint64_t bytes, uint32_t word) {
+    if (!bytes) return KC_OK;
+    if (bytes % 4 || reinterpret_cast<uintptr_t>(dst) % 4) {
+        CK(cudaMemsetAsync(dst, (int)(word & 0xFF), bytes, c->stream));
+        return KC_OK;
+    }
+    const uint64_t n = bytes / 4;
+    kc::fill_words<<<std::min<uint64_t>(ceil_div(n, 256), (uint64_t)c->sm_count * 16), 256, 0, c->stream>>>(
+        static_cast<uint32_t*>(dst), n, word);
+    CK(cudaGetLastError());
+    return KC_OK;
+}
+
+int put(kc_context* c, void* dst, const void* src, uint64_t bytes) {
+    if (!bytes) return KC_OK;
+    if (bytes % 4 || reinterpret_cast<uintptr_t>(dst) % 4 || bytes > kc_context::MBOX_UP) {
+        CK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, c->stream));
+        return KC_OK;
+    }
+    if (c->mbox_up_off + bytes > kc_context::MBOX_UP) {
+        // wrap: every earlier upload kernel has to have read its bytes
+        CK(cudaEventSynchronize(c->ev_mbox));
+        c->mbox_up_off = 0;
+    }
+    std::memcpy(c->mbox_h + c->mbox_up_off, src, bytes);
+    const uint64_t n = bytes / 4;
+    kc::copy_words<<<std::min<uint64_t>(ceil_div(n, 256), 64), 256, 0, c->stream>>>(
+        reinterpret_cast<const uint32_t*>(c->mbox_d + c->mbox_up_off), static_cast<uint32_t*>(dst), n);
+    CK(cudaGetLastError());
+    CK(cudaEventRecord(c->ev_mbox, c->stream));
+    c->mbox_up_off += (bytes + 15) & ~15ull;
+    return KC_OK;
+}
+
+int get(kc_context* c, void* dst, const void* src, uint64_t bytes) {
+    if (!bytes) return KC_OK;
+    if (bytes % 4 || reinterpret_cast<uintptr_t>(src) % 4 || c->mbox_down_off + bytes > kc_context::MBOX_DOWN) {
+        CK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, c->stream));
+        return KC_OK;
+    }
+    const uint64_t off = kc_context::MBOX_UP + c->mbox_down_off;
+    const uint64_t n = bytes / 4;
+    kc::copy_words<<<std::min<uint64_t>(ceil_div(n, 256), 64), 256, 0, c->stream>>>(
+        static_cast<const uint32_t*>(src), reinterpret_cast<uint32_t*>(c->mbox_d + off), n);
+    CK(cudaGetLastError());
+    c->readbacks.push_back({dst, off, bytes});
+    c->mbox_down_off += (bytes + 15) & ~15ull;
+    return KC_OK;
+}
+
+// Wait for `stream`, then deliver the pending readbacks.
+int sync_stream(kc_context* c) {
+    CK(cudaStreamSynchronize(c->stream));
+    for (const auto& r : c->readbacks) std::memcpy(r.dst, c->mbox_h + r.off, r.bytes);
+    c->readbacks.clear();
+    c->mbox_down_off = 0;
+    c->mbox_up_off = 0;
+    return KC_OK;
+}
+
+#define CKR(x)                   \
+    do {                         \
+        const int r_ = (x);      \
+        if (r_) return r_;       \
+    } while (0)
+
 // Exclusive scan of n values of type TI into TO out[], plus base; optional
 // device total in scalars[slot].
 template <class TI, class TO>
@@ -253,7 +352,7 @@ int device_scan(kc_context* c, const TI* in, uint64_t n, TO* out, uint64_t base,
     Stage st(c, KC_STAGE_SCAN, n ? 3 : 1);
     uint64_t* sums = c->scan_sums.as<uint64_t>();
     if (n) kc::scan_reduce<TI><<<nb, kc::SCAN_BLOCK, 0, c->stream>>>(in, n, sums);
-    else CK(cudaMemsetAsync(sums, 0, sizeof(uint64_t), c->stream));
+    else CKR(fill_dev(c, sums, sizeof(uint64_t), 0));
     kc::scan_sums<<<1, kc::SCAN_BLOCK, 0, c->stream>>>(sums, n ? nb : 1, base, d_total);
     if (n) kc::scan_apply<TI, TO><<<nb, kc::SCAN_BLOCK, 0, c->stream>>>(in, n, sums, out);
     CK(cudaGetLastError());
@@ -297,17 +396,17 @@ int size_structures(kc_context* c, const std::vector<uint64_t>& kb, double scale
     CK(c->bloom.ensure(bw * sizeof(uint64_t)));
     CK(c->table.ensure(ts * c->slot_bytes + ts * c->slot_bytes / 2));
     CK(c->meta.ensure(nb * sizeof(kc::BucketMeta)));
-    CK(cudaMemcpyAsync(c->meta.p, c->h_meta.data(), nb * sizeof(kc::BucketMeta), cudaMemcpyHostToDevice, c->stream));
+    CKR(put(c, c->meta.p, c->h_meta.data(), nb * sizeof(kc::BucketMeta)));
     {
         Stage st(c, KC_STAGE_INIT, 1);
-        CK(cudaMemsetAsync(c->bloom.p, 0, bw * sizeof(uint64_t), c->stream));
+        CKR(fill_dev(c, c->bloom.p, bw * sizeof(uint64_t), 0));
         const int ig = 148 * 8;
         if (c->nw == 1) kc::init_slots<1><<<ig, 256, 0, c->stream>>>(c->table.p, ts);
         else kc::init_slots<2><<<ig, 256, 0, c->stream>>>(c->table.p, ts);
         CK(cudaGetLastError());
     }
     CK(c->overflow.ensure(nb * sizeof(uint32_t)));
-    CK(cudaMemsetAsync(c->overflow.p, 0, nb * sizeof(uint32_t), c->stream));
+    CKR(fill_dev(c, c->overflow.p, nb * sizeof(uint32_t), 0));
     c->h_overflow.assign(nb, 0);
     c->sized = true;
     return KC_OK;
@@ -341,15 +440,14 @@ template <int NW>
 int rehash_loop(kc_context* c, uint64_t n_keys) {
     const uint32_t nb = c->n_buckets;
     for (int round = 0;; ++round) {
-        CK(cudaMemcpyAsync(c->h_overflow.data(), c->overflow.p, nb * sizeof(uint32_t), cudaMemcpyDeviceToHost,
-                           c->stream));
-        CK(cudaStreamSynchronize(c->stream));
+        CKR(get(c, c->h_overflow.data(), c->overflow.p, nb * sizeof(uint32_t)));
+        CKR(sync_stream(c));
         std::vector<uint32_t> grow;
         for (uint32_t b = 0; b < nb; ++b)
             if (c->h_overflow[b]) grow.push_back(b);
         if (grow.empty()) return KC_OK;
         if (round > 24) return fail(KC_ERR_OVERFLOW, "repeat tables kept overflowing after %d growth rounds", round);
-        CK(cudaMemsetAsync(c->overflow.p, 0, nb * sizeof(uint32_t), c->stream));
+        CKR(fill_dev(c, c->overflow.p, nb * sizeof(uint32_t), 0));
         CK(c->scalars.ensure(64));
         uint32_t* d_failed = c->scalars.as<uint32_t>() + 8;
         for (uint32_t b : grow) {
@@ -363,13 +461,13 @@ int rehash_loop(kc_context* c, uint64_t n_keys) {
                 const void* ot = c->table.as<uint8_t>() + c->h_meta[b].tab_off * c->slot_bytes;
                 Stage st(c, KC_STAGE_REHASH, 2);
                 kc::init_slots<NW><<<256, 256, 0, c->stream>>>(nt, new_slots);
-                CK(cudaMemsetAsync(d_failed, 0, sizeof(uint32_t), c->stream));
+                CKR(fill_dev(c, d_failed, sizeof(uint32_t), 0));
                 kc::rehash_bucket<NW><<<std::max<uint64_t>(1, std::min<uint64_t>(1184, ceil_div(old_slots, 256))), 256, 0,
                                         c->stream>>>(ot, old_slots, nt, new_slots - 1, d_failed);
                 CK(cudaGetLastError());
                 uint32_t h_failed = 0;
-                CK(cudaMemcpyAsync(&h_failed, d_failed, sizeof(uint32_t), cudaMemcpyDeviceToHost, c->stream));
-                CK(cudaStreamSynchronize(c->stream));
+                CKR(get(c, &h_failed, d_failed, sizeof(uint32_t)));
+                CKR(sync_stream(c));
                 c->table_slots_used += new_slots;
                 if (!h_failed) {
                     c->h_meta[b].tab_off = off;
@@ -380,8 +478,7 @@ int rehash_loop(kc_context* c, uint64_t n_keys) {
             }
             ++c->rehashes;
         }
-        CK(cudaMemcpyAsync(c->meta.p, c->h_meta.data(), nb * sizeof(kc::BucketMeta), cudaMemcpyHostToDevice,
-                           c->stream));
+        CKR(put(c, c->meta.p, c->h_meta.data(), nb * sizeof(kc::BucketMeta)));
         launch_count<NW>(c, n_keys, 0);
         CK(cudaGetLastError());
     }
@@ -438,7 +535,7 @@ int process_batch(kc_context* c, const uint8_t* buf, uint64_t n, int has_halo) {
     CK(c->tile_line.ensure(std::max<uint64_t>(tiles, 1) * sizeof(uint64_t)));
     CK(c->scalars.ensure(64));
     uint64_t* d_scal = c->scalars.as<uint64_t>();
-    CK(cudaMemsetAsync(c->scalars.as<uint32_t>() + 12, 0, sizeof(uint32_t), c->stream));
+    CKR(fill_dev(c, c->scalars.as<uint32_t>() + 12, sizeof(uint32_t), 0));
     if (tiles) {
         Stage st(c, KC_STAGE_LINES);
         kc::lines_per_tile<<<tiles, kc::EXT_THREADS, 0, c->stream>>>(buf, n, c->tile_nl.as<uint32_t>());
@@ -466,14 +563,13 @@ int process_batch(kc_context* c, const uint8_t* buf, uint64_t n, int has_halo) {
     uint64_t n_keys = 0, kb = 0;
     for (int attempt = 0;; ++attempt) {
         const uint32_t stride = est ? kc::EST_STRIDE : 1u;
-        CK(cudaMemsetAsync(c->bucket_count.p, 0, nb * sizeof(uint64_t), c->stream));
+        CKR(fill_dev(c, c->bucket_count.p, nb * sizeof(uint64_t), 0));
         if ((rc = launch_extract<NW>(c, buf, n, has_halo, kc::HIST, stride))) return rc;
         c->h_bucket_count.resize(nb);
         uint64_t line_end = 0;
-        CK(cudaMemcpyAsync(c->h_bucket_count.data(), c->bucket_count.p, nb * sizeof(uint64_t), cudaMemcpyDeviceToHost,
-                           c->stream));
-        CK(cudaMemcpyAsync(&line_end, d_scal + 0, sizeof(uint64_t), cudaMemcpyDeviceToHost, c->stream));
-        CK(cudaStreamSynchronize(c->stream));
+        CKR(get(c, c->h_bucket_count.data(), c->bucket_count.p, nb * sizeof(uint64_t)));
+        CKR(get(c, &line_end, d_scal + 0, sizeof(uint64_t)));
+        CKR(sync_stream(c));
         if (attempt == 0) c->line_base = line_end;
 
         std::vector<uint64_t> kest(nb);
@@ -502,11 +598,11 @@ int process_batch(kc_context* c, const uint8_t* buf, uint64_t n, int has_halo) {
         CK(c->tile_low.ensure(ctiles * (CT / SEG) * sizeof(uint32_t)));
         CK(c->tile_fail.ensure(ctiles * (CT / SEG) * sizeof(uint32_t)));
         CK(c->tile_low_prefix.ensure(ctiles * (CT / SEG) * sizeof(uint64_t)));
-        CK(cudaMemcpyAsync(c->bucket_cursor.p, start.data(), nb * sizeof(uint64_t), cudaMemcpyHostToDevice, c->stream));
+        CKR(put(c, c->bucket_cursor.p, start.data(), nb * sizeof(uint64_t)));
         if (est) {
-            CK(cudaMemcpyAsync(c->region_end.p, end.data(), nb * sizeof(uint64_t), cudaMemcpyHostToDevice, c->stream));
-            CK(cudaMemcpyAsync(d_scal + 2, &total_cap, sizeof(uint64_t), cudaMemcpyHostToDevice, c->stream));
-            CK(cudaMemsetAsync(c->region_fill.p, 0xFF, nb * sizeof(uint64_t), c->stream));
+            CKR(put(c, c->region_end.p, end.data(), nb * sizeof(uint64_t)));
+            CKR(put(c, d_scal + 2, &total_cap, sizeof(uint64_t)));
+            CKR(fill_dev(c, c->region_fill.p, nb * sizeof(uint64_t), 0xFFFFFFFFu));
         }
         if ((rc = launch_extract<NW>(c, buf, n, has_halo, kc::SCATTER, 1, est, total_cap, cap_keys))) return rc;
         if (!est) {
@@ -515,12 +611,12 @@ int process_batch(kc_context* c, const uint8_t* buf, uint64_t n, int has_halo) {
         }
         uint64_t ovf_used = 0;
         uint32_t flags = 0;
-        CK(cudaMemcpyAsync(cursor.data(), c->bucket_cursor.p, nb * sizeof(uint64_t), cudaMemcpyDeviceToHost, c->stream));
-        CK(cudaMemcpyAsync(&ovf_used, d_scal + 2, sizeof(uint64_t), cudaMemcpyDeviceToHost, c->stream));
-        CK(cudaMemcpyAsync(&flags, c->scalars.as<uint32_t>() + 12, sizeof(uint32_t), cudaMemcpyDeviceToHost, c->stream));
-        CK(cudaStreamSynchronize(c->stream));
+        CKR(get(c, cursor.data(), c->bucket_cursor.p, nb * sizeof(uint64_t)));
+        CKR(get(c, &ovf_used, d_scal + 2, sizeof(uint64_t)));
+        CKR(get(c, &flags, c->scalars.as<uint32_t>() + 12, sizeof(uint32_t)));
+        CKR(sync_stream(c));
         if (flags & 2u) {  // overflow area full: route this batch again, exactly
-            CK(cudaMemsetAsync(c->scalars.as<uint32_t>() + 12, 0, sizeof(uint32_t), c->stream));
+            CKR(fill_dev(c, c->scalars.as<uint32_t>() + 12, sizeof(uint32_t), 0));
             est = false;
             ++c->reroutes;
             continue;
@@ -545,7 +641,7 @@ int process_batch(kc_context* c, const uint8_t* buf, uint64_t n, int has_halo) {
     c->K += kb;
     if (c->after_scatter) CK(cudaEventRecord(c->after_scatter, c->stream));
     uint32_t ext_err = 0;
-    CK(cudaMemcpyAsync(&ext_err, c->scalars.as<uint32_t>() + 12, sizeof(uint32_t), cudaMemcpyDeviceToHost, c->stream));
+    CKR(get(c, &ext_err, c->scalars.as<uint32_t>() + 12, sizeof(uint32_t)));
 
     const uint64_t nsegs = ceil_div(n_keys, SEG);
     launch_count<NW>(c, n_keys, 1);
@@ -557,8 +653,8 @@ int process_batch(kc_context* c, const uint8_t* buf, uint64_t n, int has_halo) {
                                               c->tile_low_prefix.as<uint64_t>(), 0, d_scal + 1)))
         return rc;
     uint64_t nlow = 0;
-    CK(cudaMemcpyAsync(&nlow, d_scal + 1, sizeof(uint64_t), cudaMemcpyDeviceToHost, c->stream));
-    CK(cudaStreamSynchronize(c->stream));
+    CKR(get(c, &nlow, d_scal + 1, sizeof(uint64_t)));
+    CKR(sync_stream(c));
     if (ext_err) return fail(KC_ERR_DEVICE, "internal error: routing bucket disagreed with its reservation");
     uint8_t* low_dst;
     uint64_t low_base;
@@ -605,9 +701,8 @@ int run_export(kc_context* c, const std::vector<kc::ExportChunk>& ch, uint64_t n
     CK(c->chunk_pass.ensure(std::max<uint64_t>(nch, 1) * sizeof(uint32_t)));
     CK(c->chunk_off.ensure(std::max<uint64_t>(nch, 1) * sizeof(uint64_t)));
     CK(c->root_count.ensure((n_groups + 1) * sizeof(uint64_t)));
-    if (nch)
-        CK(cudaMemcpyAsync(c->chunks.p, ch.data(), nch * sizeof(kc::ExportChunk), cudaMemcpyHostToDevice, c->stream));
-    CK(cudaMemsetAsync(c->root_count.p, 0, (n_groups + 1) * sizeof(uint64_t), c->stream));
+    if (nch) CKR(put(c, c->chunks.p, ch.data(), nch * sizeof(kc::ExportChunk)));
+    CKR(fill_dev(c, c->root_count.p, (n_groups + 1) * sizeof(uint64_t), 0));
     unsigned long long* rcd = c->root_count.as<unsigned long long>();
     const uint64_t grid = std::min<uint64_t>(std::max<uint64_t>(nch, 1), (uint64_t)c->sm_count * 8);
     if (nch) {
@@ -622,8 +717,8 @@ int run_export(kc_context* c, const std::vector<kc::ExportChunk>& ch, uint64_t n
                                               nullptr)))
         return rc;
     totals.assign(n_groups + 1, 0);
-    CK(cudaMemcpyAsync(totals.data(), rcd, (n_groups + 1) * sizeof(uint64_t), cudaMemcpyDeviceToHost, c->stream));
-    CK(cudaStreamSynchronize(c->stream));
+    CKR(get(c, totals.data(), rcd, (n_groups + 1) * sizeof(uint64_t)));
+    CKR(sync_stream(c));
     uint64_t R = 0;
     for (uint64_t g = 0; g < n_groups; ++g) R += totals[g];
     CK(c->roots.ensure(std::max<uint64_t>(R, 1) * c->record_bytes));
@@ -674,6 +769,8 @@ int begin_run(kc_context* c, uint64_t total_bytes) {
     c->line_base = 0;
     c->low_total = 0;
     c->K = 0;
+    c->readbacks.clear();  // a failed earlier call may have left some behind
+    c->mbox_up_off = c->mbox_down_off = 0;
     c->rehashes = 0;
     c->overflow_keys = 0;
     c->reroutes = 0;
@@ -721,7 +818,7 @@ int finish_run(kc_context* c) {
         rc = kc_sort_roots(c->roots.p, c->root_total, c->record_bytes, c->cfg.k, w, c->stream);
         if (rc) return fail(rc, "root record sort failed: %s", kc_sort_error());
     }
-    CK(cudaStreamSynchronize(c->stream));
+    CKR(sync_stream(c));
     c->have_result = true;
     return KC_OK;
 }
@@ -747,53 +844,83 @@ void fill_stats(kc_context* c, kc_stats* s, double dev_ms, double wall_ms) {
     s->reroutes = c->reroutes;
 }
 
-// Deliver completed device->host pieces in order; `all` waits for every one.
-int drain_pieces(kc_context* c, bool all) {
-    size_t done = 0;
-    for (; done < c->pending.size(); ++done) {
-        const kc_context::Piece& p = c->pending[done];
-        if (!all && cudaEventQuery(c->ev_pin[p.slot]) == cudaErrorNotReady) break;
-        CK(cudaEventSynchronize(c->ev_pin[p.slot]));
-        if (!c->sink_rc) c->sink_rc = c->sink(c->sink_user, p.kind, p.root, c->pin[p.slot], p.bytes);
+// Output delivery thread: waits for each device->host piece in FIFO order and
+// hands it to the sink, so that the thread issuing the counting work never
+// waits for a copy it does not need.  A piece with slot -1 is an empty root
+// file (sink called with no bytes).  Pieces still queued at stop are drained.
+void deliver_loop(kc_context* c) {
+    cudaSetDevice(c->device);
+    std::unique_lock<std::mutex> lk(c->pin_mu);
+    for (;;) {
+        c->pin_cv.wait(lk, [&] { return c->deliver_stop || !c->pending.empty(); });
+        if (c->pending.empty()) return;
+        const kc_context::Piece p = c->pending.front();
+        const bool skip = c->sink_rc || c->deliver_err;
+        lk.unlock();
+        bool copy_ok = true;
+        int r = 0;
+        if (p.slot >= 0) copy_ok = cudaEventSynchronize(c->ev_pin[p.slot]) == cudaSuccess;
+        if (copy_ok && !skip) r = c->sink(c->sink_user, p.kind, p.root, p.slot >= 0 ? c->pin[p.slot] : nullptr, p.bytes);
+        lk.lock();
+        if (!copy_ok) c->deliver_err = true;
+        if (r && !c->sink_rc) c->sink_rc = r;
+        c->pending.pop_front();
+        if (p.slot >= 0) c->slot_busy[p.slot] = false;
+        c->pin_cv.notify_all();
     }
-    c->pending.erase(c->pending.begin(), c->pending.begin() + done);
+}
+
+int sink_status(kc_context* c) {
+    std::lock_guard<std::mutex> lk(c->pin_mu);
+    if (c->deliver_err) return fail(KC_ERR_DEVICE, "device->host copy of an output piece failed");
     if (c->sink_rc) return fail(KC_ERR_IO, "output sink returned %d", c->sink_rc);
     return KC_OK;
 }
 
-// Copy `bytes` from device `src` to the caller through the pinned ring, in
-// pieces, after event `ready` on the compute stream.
+// Wait until every queued piece was delivered.
+int drain_pieces(kc_context* c) {
+    {
+        std::unique_lock<std::mutex> lk(c->pin_mu);
+        c->pin_cv.wait(lk, [&] { return c->pending.empty(); });
+    }
+    return sink_status(c);
+}
+
+// Copy `bytes` at device `src` (ready once `ready` fires on `stream`) out
+// through the pinned slots, PIN_BYTES at a time.
 int stream_piece(kc_context* c, int kind, uint32_t root, const uint8_t* src, uint64_t bytes, cudaEvent_t ready) {
     if (bytes == 0) {
         if (kind == KC_SINK_ROOT) {
-            int rc = drain_pieces(c, true);
-            if (rc) return rc;
-            if (!c->sink_rc) c->sink_rc = c->sink(c->sink_user, kind, root, nullptr, 0);
-            if (c->sink_rc) return fail(KC_ERR_IO, "output sink returned %d", c->sink_rc);
+            std::lock_guard<std::mutex> lk(c->pin_mu);
+            c->pending.push_back({kind, root, 0, -1});
+            c->pin_cv.notify_all();
         }
-        return KC_OK;
+        return sink_status(c);
     }
     CK(cudaStreamWaitEvent(c->d2h, ready, 0));
     for (uint64_t off = 0; off < bytes; off += kc_context::PIN_BYTES) {
         const uint64_t m = std::min<uint64_t>(kc_context::PIN_BYTES, bytes - off);
-        // a slot is reusable once its previous piece was delivered
         int slot = -1;
-        for (;;) {
-            bool busy[kc_context::PIN_SLOTS] = {};
-            for (const auto& p : c->pending) busy[p.slot] = true;
-            for (int q = 0; q < kc_context::PIN_SLOTS && slot < 0; ++q)
-                if (!busy[q]) slot = q;
-            if (slot >= 0) break;
-            // deliver the oldest piece to free its slot
-            CK(cudaEventSynchronize(c->ev_pin[c->pending.front().slot]));
-            int rc = drain_pieces(c, false);
-            if (rc) return rc;
+        {
+            std::unique_lock<std::mutex> lk(c->pin_mu);
+            c->pin_cv.wait(lk, [&] {
+                for (int q = 0; q < kc_context::PIN_SLOTS; ++q)
+                    if (!c->slot_busy[q]) {
+                        slot = q;
+                        return true;
+                    }
+                return c->sink_rc != 0 || c->deliver_err;
+            });
+            if (slot < 0) break;  // the sink failed: stop producing
+            c->slot_busy[slot] = true;
         }
         CK(cudaMemcpyAsync(c->pin[slot], src + off, m, cudaMemcpyDeviceToHost, c->d2h));
         CK(cudaEventRecord(c->ev_pin[slot], c->d2h));
+        std::lock_guard<std::mutex> lk(c->pin_mu);
         c->pending.push_back({kind, root, m, slot});
+        c->pin_cv.notify_all();
     }
-    return drain_pieces(c, false);
+    return sink_status(c);
 }
 
 int stream_out_low(kc_context* c) {
@@ -895,6 +1022,13 @@ int kc_create(const kc_config* cfg, kc_context** out) {
     }
     for (int i = 0; i < kc_context::PIN_SLOTS; ++i) cudaEventCreateWithFlags(&c->ev_pin[i], cudaEventDisableTiming);
     cudaEventCreateWithFlags(&c->ev_pack, cudaEventDisableTiming);
+    cudaEventCreateWithFlags(&c->ev_mbox, cudaEventDisableTiming);
+    if ((e = cudaHostAlloc(reinterpret_cast<void**>(&c->mbox_h), kc_context::MBOX_UP + kc_context::MBOX_DOWN,
+                           cudaHostAllocMapped | cudaHostAllocPortable)) != cudaSuccess ||
+        (e = cudaHostGetDevicePointer(reinterpret_cast<void**>(&c->mbox_d), c->mbox_h, 0)) != cudaSuccess) {
+        kc_destroy(c);
+        return fail(KC_ERR_DEVICE, "mapped control mailbox allocation failed: %s", cudaGetErrorString(e));
+    }
     // 4096-bucket extraction and the scatter staging area exceed 48 KiB.
     cudaFuncSetAttribute(kc::extract_kernel<1, kc::HIST>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)kc::extract_smem_bytes<1, kc::HIST>(4096));
@@ -935,6 +1069,8 @@ void kc_destroy(kc_context* c) {
         if (c->pin[i]) cudaFreeHost(c->pin[i]);
     }
     if (c->ev_pack) cudaEventDestroy(c->ev_pack);
+    if (c->ev_mbox) cudaEventDestroy(c->ev_mbox);
+    if (c->mbox_h) cudaFreeHost(c->mbox_h);
     c->stage2.release();
     if (c->h2d) cudaStreamDestroy(c->h2d);
     if (c->d2h) cudaStreamDestroy(c->d2h);
@@ -989,6 +1125,31 @@ int kc_count_device(kc_context* c, const uint8_t* d_fastq, uint64_t n, kc_stats*
     return KC_OK;
 }
 
+// Batch lengths of a host input: batch_bytes B each, except that a long
+// input (at least 4 B, B >= 64 MiB) ramps up over its first batches (B/8,
+// B/4, B/2) and down over its last ones, so that the first output leaves
+// early and the last batch is counted soon after its bytes arrived.
+std::vector<uint64_t> plan_batches(uint64_t n, uint64_t B) {
+    std::vector<uint64_t> v;
+    if (!n) return v;
+    const uint64_t T = kc::EXT_TILE;
+    auto al = [&](uint64_t x) { return std::max<uint64_t>(T, x & ~(T - 1)); };
+    if (n < 4 * B || B < (64ull << 20)) {
+        for (uint64_t off = 0; off < n; off += B) v.push_back(std::min<uint64_t>(B, n - off));
+        return v;
+    }
+    const uint64_t ramp[3] = {al(B / 8), al(B / 4), al(B / 2)};
+    const uint64_t ends = 2 * (ramp[0] + ramp[1] + ramp[2]);
+    const uint64_t mid = n - ends;  // > 2 B
+    const uint64_t k = ceil_div(mid, B);
+    const uint64_t each = al(mid / k);
+    v.assign(ramp, ramp + 3);
+    for (uint64_t i = 0; i + 1 < k; ++i) v.push_back(each);
+    v.push_back(mid - (k - 1) * each);
+    for (int i = 2; i >= 0; --i) v.push_back(ramp[i]);
+    return v;
+}
+
 // Host input, double-buffered: batch i+1 is copied host->device on its own
 // stream (chunk_bytes pieces) while batch i is counted.  Staging buffers are
 // [HALO | batch | pad]; the HALO bytes before a batch are copied from the
@@ -996,15 +1157,21 @@ int kc_count_device(kc_context* c, const uint8_t* d_fastq, uint64_t n, kc_stats*
 // reference reader's k-1 overlap does (src/FastqReader.h:338-365).
 int host_pipeline(kc_context* c, const uint8_t* fastq, uint64_t n) {
     const uint64_t B = std::max<uint64_t>(kc::EXT_TILE, c->cfg.batch_bytes & ~(uint64_t)(kc::EXT_TILE - 1));
-    const uint64_t cap = std::min<uint64_t>(B, std::max<uint64_t>(n, 1));
-    const uint64_t nbatch = n ? ceil_div(n, cap) : 0;
+    const std::vector<uint64_t> plan = plan_batches(n, B);
+    const uint64_t nbatch = plan.size();
+    std::vector<uint64_t> offs(nbatch);
+    uint64_t cap = 1;
+    for (uint64_t i = 0, o = 0; i < nbatch; o += plan[i], ++i) {
+        offs[i] = o;
+        cap = std::max<uint64_t>(cap, plan[i]);
+    }
     CK(c->stage.ensure(kc::HALO + cap + kc::EXT_TILE));
     if (nbatch > 1) CK(c->stage2.ensure(kc::HALO + cap + kc::EXT_TILE));
     uint8_t* slots[2] = {c->stage.as<uint8_t>(), c->stage2.as<uint8_t>()};
     const uint64_t chunk = std::max<uint64_t>(c->cfg.chunk_bytes, 1 << 20);
     auto enqueue_copy = [&](uint64_t i) -> int {
         const int slot = (int)(i & 1);
-        const uint64_t off = i * cap, len = std::min<uint64_t>(cap, n - off);
+        const uint64_t off = offs[i], len = plan[i];
         uint8_t* dst = slots[slot];
         if (i >= 2) CK(cudaStreamWaitEvent(c->h2d, c->ev_free[slot], 0));
         if (off >= (uint64_t)kc::HALO) CK(cudaMemcpyAsync(dst, fastq + off - kc::HALO, kc::HALO, cudaMemcpyHostToDevice, c->h2d));
@@ -1019,10 +1186,9 @@ int host_pipeline(kc_context* c, const uint8_t* fastq, uint64_t n) {
     for (uint64_t i = 0; i < nbatch; ++i) {
         if (i + 1 < nbatch && (rc = enqueue_copy(i + 1))) return rc;
         const int slot = (int)(i & 1);
-        const uint64_t off = i * cap, len = std::min<uint64_t>(cap, n - off);
         CK(cudaStreamWaitEvent(c->stream, c->ev_h2d[slot], 0));
         c->after_scatter = c->ev_free[slot];
-        rc = run_batch(c, slots[slot] + kc::HALO, len, off > 0);
+        rc = run_batch(c, slots[slot] + kc::HALO, plan[i], offs[i] > 0);
         c->after_scatter = nullptr;
         if (rc) return rc;
         if (c->stream_low && (rc = stream_out_low(c))) return rc;
@@ -1064,20 +1230,44 @@ int kc_count_host_stream(kc_context* c, const uint8_t* fastq, uint64_t n, kc_sin
                 return fail(KC_ERR_NOMEM, "pinned staging allocation failed");
             }
         }
-        CK(cudaEventRecord(c->ev_pin[i], c->d2h));
     }
     for (int i = 0; i < 2; ++i) CK(cudaEventRecord(c->ev_lowfree[i], c->d2h));
     c->stream_low = true;
     c->sink = sink;
     c->sink_user = user;
-    c->sink_rc = 0;
-    c->pending.clear();
+    {
+        std::lock_guard<std::mutex> lk(c->pin_mu);
+        c->sink_rc = 0;
+        c->deliver_err = false;
+        c->deliver_stop = false;
+        c->pending.clear();
+        for (bool& b : c->slot_busy) b = false;
+    }
+    try {
+        c->deliverer = std::thread(deliver_loop, c);
+    } catch (...) {
+        c->stream_low = false;
+        return fail(KC_ERR_NOMEM, "could not start the output delivery thread");
+    }
+    // stops the delivery thread on every exit path, after it delivered (or,
+    // once the sink failed, skipped) every queued piece
+    struct StopDelivery {
+        kc_context* c;
+        ~StopDelivery() {
+            {
+                std::lock_guard<std::mutex> lk(c->pin_mu);
+                c->deliver_stop = true;
+            }
+            c->pin_cv.notify_all();
+            if (c->deliverer.joinable()) c->deliverer.join();
+            c->stream_low = false;
+        }
+    } stop{c};
     CK(cudaEventRecord(c->ev0, c->stream));
     rc = host_pipeline(c, fastq, n);
     if (!rc) rc = finish_run(c);
     if (!rc) rc = stream_out_roots(c);
-    const int drc = drain_pieces(c, true);
-    c->stream_low = false;
+    const int drc = drain_pieces(c);
     if (rc) return rc;
     if (drc) return drc;
     CK(cudaEventRecord(c->ev1, c->stream));

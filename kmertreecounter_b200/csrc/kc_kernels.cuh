@@ -203,6 +203,23 @@ __device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t v, uint32_t* s
     return r;
 }
 
+// ------------------------------------------------ control-path transfers
+//
+// Counts, cursors and flags move between host and device as kernels that
+// read or write mapped pinned memory, and small fills run as kernels: the
+// copy engines are kept for the bulk FASTQ and output copies, behind which a
+// few-byte copy would otherwise wait.
+
+static __global__ void copy_words(const uint32_t* __restrict__ src, uint32_t* __restrict__ dst, uint64_t n) {
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+        dst[i] = src[i];
+}
+
+static __global__ void fill_words(uint32_t* __restrict__ dst, uint64_t n, uint32_t v) {
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+        dst[i] = v;
+}
+
 // ------------------------------------------------------- FASTQ line split
 
 // '\n' count per 8 KiB tile of the batch buf[0..n) (16-byte vector reads,
