@@ -131,8 +131,10 @@ void kc_destroy(kc_context* ctx);
 int kc_count_host(kc_context* ctx, const uint8_t* fastq, uint64_t n, kc_stats* stats);
 
 /* Streaming form of kc_count_host for large inputs: results are handed to
- * `sink` on the calling thread as they reach host memory, so device->host
- * copies overlap the counting of later batches.
+ * `sink` as they reach host memory, so device->host copies overlap the
+ * counting of later batches.  The sink runs on a delivery thread the library
+ * starts for the call and joins before returning (one call at a time, in
+ * the order below); it must not call back into this context.
  *   kind KC_SINK_LOW   packed low.bin bytes, in file order (first
  *                      occurrences of a batch are final when emitted)
  *   kind KC_SINK_ROOT  ExportRecord<N> bytes of root file `root`, roots in

@@ -52,6 +52,10 @@ constexpr int EXT_THREADS = 256;                     // extraction CTA
 constexpr int EXT_BPT = 32;                          // bytes per thread
 constexpr int EXT_TILE = EXT_THREADS * EXT_BPT;      // 8 KiB per CTA
 constexpr int HALO = 64;                             // bytes kept before a batch
+// The 256-bucket scatter staging area holds extraction to 4 CTAs per SM;
+// telling the compiler so lets it use up to 64 registers (measured 6% faster
+// than its default of 32).
+constexpr int EXT_MIN_CTAS = 4;
 // Bucket regions of a batch of at least EST_MIN_TILES tiles are sized from a
 // histogram of every EST_STRIDE-th tile instead of all of them.
 constexpr uint32_t EST_STRIDE = 32;
@@ -469,7 +473,7 @@ __host__ __device__ constexpr size_t extract_smem_bytes(uint32_t n_buckets) {
 }
 
 template <int NW, int MODE>
-__global__ void __launch_bounds__(EXT_THREADS) extract_kernel(ExtractArgs a) {
+__global__ void __launch_bounds__(EXT_THREADS, EXT_MIN_CTAS) extract_kernel(ExtractArgs a) {
     // dynamic smem: u64 base[nb] | u32 hist[nb] | u32 fill[nb] | u32 loff[nb]
     //               | SCATTER: K keys[stage] | u16 bucket_of_key[stage]
     extern __shared__ unsigned long long ext_smem[];

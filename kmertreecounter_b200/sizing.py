@@ -3,23 +3,32 @@
 The reference sizes its per-prefix Bloom filters from a Stage-0 sample of up
 to 256 MB (src/main.cpp:88-108) and never sizes its tree, which grows from a
 memory pool.  Here the open-addressing tables must be sized up front; the
-plain rule (`KC_SIZING_SAMPLED`) takes each bucket's exact k-mer total of the
-first batch and a fixed ratio of table keys per k-mer, and grows a table x4
-(rehash) when it overflows.  The learned rule predicts each bucket's distinct
-keys and table keys from a 1% read prefix with a small MLP:
+plain rule (`KC_SIZING_SAMPLED`) takes each bucket's k-mer total and a fixed
+ratio of table keys per k-mer, and grows a table x4 (rehash) when it
+overflows.  The learned rule predicts, per model bucket (4096 = the top six
+bases of the canonical key), the ratios that the plain rule fixes:
 
-  input  (4102) log1p 6-mer-prefix histogram of the prefix's k-mers (4096
-         buckets = top six bases of the canonical key) / 16, k/64, read
-         length/300, ln(FASTQ bytes)/25, and three totals of the prefix counted
-         exactly on the GPU: ln(1+k-mers), ln(1+distinct), ln(1+table keys), /25
+  input  (4104) the 6-mer-prefix histogram of the first 1% of the reads,
+         log1p(4096 x bucket share) / 4; k/64, read length/300, ln(FASTQ
+         bytes)/25, ln(1 + prefix k-mers)/25; and three rates of the prefix
+         counted exactly on the GPU: distinct keys per k-mer, table keys per
+         k-mer and its square root; ln(bytes / prefix bytes)/10
   hidden 512 -> 512, ReLU, BF16 weights, FP32 accumulation
-  output (8192) ln(1+distinct keys)/20 and ln(1+table keys)/20 per bucket
+  output (8192) per bucket, ln(ratio + 1e-4)/10 + 1 of distinct keys per
+         k-mer and of table keys per k-mer
 
-It is trained by the library's own kernels (kc_mlp_train_step) on exact loads
-that the counter itself measures (kc_bucket_loads) on seeded synthetic
-genomes.  The plain rule stays the fallback: a table that overflows under a
-learned size is grown exactly as under the plain rule, so counts stay exact
-either way; rehashes avoided or incurred are reported by kc_stats.
+so that predicted loads are ratio x the bucket's k-mer total (the prefix's
+total scaled by the file size).  Every input and output is a rate, not a
+size: a 100 Mbp genome looks like the small training genomes of the same
+coverage, error and repeat structure.  Table keys are multiplied by a margin
+calibrated on held-out training sets (a quantile of measured / predicted),
+so that few tables overflow; a table that does is grown exactly as under the
+plain rule, so counts stay exact either way, and kc_stats reports the
+rehashes avoided or incurred.
+
+It is trained by the library's own kernels (kc_mlp_train_step) on exact
+loads that the counter itself measures (kc_bucket_loads) on seeded synthetic
+genomes.
 """
 import ctypes as C
 import math
@@ -31,11 +40,12 @@ from . import _native
 from ._native import check, lib
 
 MODEL_BUCKETS = 4096
-N_IN = MODEL_BUCKETS + 6
+N_IN = MODEL_BUCKETS + 8
 N_HID = 512
 N_OUT = 2 * MODEL_BUCKETS
 IN_SCALE = 25.0
-OUT_SCALE = 20.0
+RATIO_FLOOR = 1e-4
+RATIO_LOG = 10.0
 PREFIX_FRACTION = 0.01
 MODEL_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "sizing_mlp.npz")
 
@@ -130,21 +140,27 @@ class MLP:
         _mcheck(lib.kc_mlp_train_step(self._m, _fp(x), _fp(t), x.shape[0], lr, C.byref(loss)))
         return loss.value
 
+    margin = 1.0  # table-key multiplier applied by predict (calibrated after training)
+
     def save(self, path=MODEL_PATH, meta=None):
-        """Weights as float16 (the forward pass runs in BF16 anyway), biases fp32."""
+        """Weights as float16 (the forward pass runs in BF16 anyway), biases
+        fp32, the calibrated margin, and a free-form report."""
         arrs = {}
         for l in range(3):
             w, b = self.get_layer(l)
             arrs[f"w{l}"] = w.astype(np.float16)
             arrs[f"b{l}"] = b
-        np.savez_compressed(path, **arrs, meta=np.array(str(meta or {})))
+        np.savez_compressed(path, **arrs, margin=np.float64(self.margin), meta=np.array(str(meta or {})))
 
     @classmethod
     def load(cls, path=MODEL_PATH, max_batch=8):
         z = np.load(path, allow_pickle=False)
+        if z["w0"].shape[0] != N_IN:
+            raise ValueError(f"{path}: model input width {z['w0'].shape[0]} != {N_IN} (features changed; retrain)")
         m = cls(n_in=z["w0"].shape[0], n_hid=z["w0"].shape[1], n_out=z["w2"].shape[1], max_batch=max_batch)
         for l in range(3):
             m.set_layer(l, z[f"w{l}"].astype(np.float32), z[f"b{l}"].astype(np.float32))
+        m.margin = float(z["margin"]) if "margin" in z.files else 1.0
         return m
 
 
@@ -161,51 +177,89 @@ def bucket_loads(counter):
     return d, t, km
 
 
+def prefix_len(n, fraction=PREFIX_FRACTION):
+    return max(1, int(n * fraction))
+
+
 def prefix_bytes(data, fraction=PREFIX_FRACTION):
-    n = max(1, int(len(data) * fraction))
-    return data[:n]
+    return data[:prefix_len(len(data), fraction)]
 
 
-def features(prefix_loads, k, read_len, fastq_bytes):
+def features(prefix_loads, k, read_len, fastq_bytes, prefix_nbytes):
     """Model input from the prefix's per-bucket loads (distinct, table, kmers)."""
-    d, t, km = prefix_loads
-    x = np.empty(N_IN, np.float32)
-    x[:MODEL_BUCKETS] = np.log1p(km.astype(np.float64)) / 16.0
+    d, t, km = (np.asarray(a, np.float64) for a in prefix_loads)
+    Kp, Dp, Tp = km.sum(), d.sum(), t.sum()
+    x = np.zeros(N_IN, np.float32)
+    if Kp > 0:
+        x[:MODEL_BUCKETS] = np.log1p(MODEL_BUCKETS * km / Kp) / 4.0
     x[MODEL_BUCKETS + 0] = k / 64.0
     x[MODEL_BUCKETS + 1] = read_len / 300.0
     x[MODEL_BUCKETS + 2] = math.log(max(fastq_bytes, 1)) / IN_SCALE
-    x[MODEL_BUCKETS + 3] = math.log1p(float(km.sum())) / IN_SCALE
-    x[MODEL_BUCKETS + 4] = math.log1p(float(d.sum())) / IN_SCALE
-    x[MODEL_BUCKETS + 5] = math.log1p(float(t.sum())) / IN_SCALE
+    x[MODEL_BUCKETS + 3] = math.log1p(Kp) / IN_SCALE
+    x[MODEL_BUCKETS + 4] = Dp / Kp if Kp > 0 else 1.0
+    x[MODEL_BUCKETS + 5] = Tp / Kp if Kp > 0 else 0.0
+    x[MODEL_BUCKETS + 6] = math.sqrt(Tp / Kp) if Kp > 0 else 0.0
+    x[MODEL_BUCKETS + 7] = math.log(max(fastq_bytes, 1) / max(prefix_nbytes, 1)) / 10.0
     return x
 
 
+def _to_y(ratio):
+    return np.log(np.asarray(ratio, np.float64) + RATIO_FLOOR) / RATIO_LOG + 1.0
+
+
+def _from_y(y):
+    return np.clip(np.exp((np.clip(y, 0.0, 1.2) - 1.0) * RATIO_LOG) - RATIO_FLOOR, 0.0, 1.0)
+
+
 def targets(full_loads):
-    d, t, _ = full_loads
+    """Per bucket: distinct keys per k-mer and table keys per k-mer, encoded."""
+    d, t, km = (np.asarray(a, np.float64) for a in full_loads)
+    den = np.maximum(km, 1.0)
     y = np.empty(N_OUT, np.float32)
-    y[:MODEL_BUCKETS] = np.log1p(d.astype(np.float64)) / OUT_SCALE
-    y[MODEL_BUCKETS:] = np.log1p(t.astype(np.float64)) / OUT_SCALE
+    y[:MODEL_BUCKETS] = _to_y(d / den)
+    y[MODEL_BUCKETS:] = _to_y(t / den)
     return y
 
 
-def decode(y):
-    """Model output -> (predicted distinct, predicted table keys) per bucket."""
-    y = np.clip(np.asarray(y, np.float64), 0.0, 1.6)
-    return np.expm1(y[:MODEL_BUCKETS] * OUT_SCALE), np.expm1(y[MODEL_BUCKETS:] * OUT_SCALE)
+def decode(y, kmers_est):
+    """Model output + estimated k-mers per bucket -> (distinct, table keys)."""
+    y = np.asarray(y, np.float64)
+    kest = np.asarray(kmers_est, np.float64)
+    return _from_y(y[:MODEL_BUCKETS]) * kest, _from_y(y[MODEL_BUCKETS:]) * kest
 
 
-def profile_prefix(data, k, device=0):
-    """Count the first 1% of the FASTQ exactly; return its per-bucket loads."""
-    from ._native import Counter
-    with Counter(k=k, n_buckets=256, device=device) as c:
-        c.count_host(prefix_bytes(data))
-        return bucket_loads(c)
+def predict_on(counter, model, k, read_len, total_bytes, run_prefix):
+    """Profile a prefix on `counter` (plain rule), predict the full run's
+    per-bucket loads, hand them to `counter` (KC_SIZING_LEARNED) for its next
+    count.  run_prefix() counts the prefix and returns its byte length.
+    Returns (distinct, table keys) as handed over (margin applied)."""
+    check(lib.kc_set_predicted_loads(counter._ctx, None, None))
+    pbytes = run_prefix()
+    loads = bucket_loads(counter)
+    x = features(loads, k, read_len, total_bytes, pbytes)
+    scale = total_bytes / max(pbytes, 1)
+    d, t = decode(model.forward(x[None, :])[0], loads[2].astype(np.float64) * scale)
+    t = t * model.margin
+    apply(counter, (d, t))
+    return d, t
 
 
-def predict_loads(model, data, k, read_len, device=0):
-    """Predicted (distinct, table keys) per model bucket for FASTQ bytes."""
-    x = features(profile_prefix(data, k, device), k, read_len, len(data))
-    return decode(model.forward(x[None, :])[0])
+def predict_host(counter, model, data, k, read_len):
+    """predict_on for host FASTQ bytes (the prefix is copied and counted)."""
+    def run():
+        p = prefix_bytes(data)
+        counter.count_host(p)
+        return len(p)
+    return predict_on(counter, model, k, read_len, len(data), run)
+
+
+def predict_device(counter, model, dptr, n, k, read_len):
+    """predict_on for FASTQ already in device memory."""
+    def run():
+        pn = prefix_len(n)
+        counter.count_device(dptr, pn)
+        return pn
+    return predict_on(counter, model, k, read_len, n, run)
 
 
 def apply(counter, pred):

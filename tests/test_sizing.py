@@ -113,3 +113,19 @@ def test_trained_model_beats_plain_rule():
     s = summarise(evaluate(model, range(990000, 990008), gmin=3e5, gmax=1.2e7))
     assert s["all_exact"]
     assert s["median_rel_err_table_learned"] < s["median_rel_err_table_sampled"]
+
+
+@pytest.mark.skipif(not os.path.exists(sizing.MODEL_PATH), reason="trained sizing model not present")
+def test_learned_sizing_avoids_rehashes_beyond_training_scale():
+    """Held-out 53 Mbp genome at 5.3x coverage (training genomes stop at
+    12 Mbp): the plain rule's fixed 0.125 table keys per k-mer is too small at
+    this coverage and its tables overflow and grow; the rate-based prediction
+    sizes them big enough the first time (here it over-predicts: its median
+    per-bucket error is not the point of this case, the overflow is).  Counts
+    identical under both rules."""
+    from kmertreecounter_b200.train_sizing import evaluate
+    model = sizing.MLP.load()
+    (r,) = evaluate(model, [950001], 1e7, 1e8, max_bytes=4e9)
+    print(r)
+    assert r["exact_match"]
+    assert r["rehash_sampled"] > 0 and r["rehash_learned"] == 0
