@@ -484,12 +484,14 @@ int rehash_loop(kc_context* c, uint64_t n_keys) {
     }
 }
 
-// mode HIST: per-bucket totals over every `stride`-th tile.  mode SCATTER:
-// keys into the bucket regions (estimated regions with an overflow area when
-// `estimated`, else exact).
+// mode HIST: totals of `bins` buckets (the top log2(bins) key bits) over
+// every `stride`-th tile.  mode SCATTER: keys into the regions of `bins`
+// routing buckets (estimated regions with an overflow area when `estimated`,
+// else exact).
 template <int NW>
-int launch_extract(kc_context* c, const uint8_t* buf, uint64_t n, int has_halo, int mode, uint32_t stride = 1,
-                   bool estimated = false, uint64_t overflow_start = 0, uint64_t overflow_end = 0) {
+int launch_extract(kc_context* c, const uint8_t* buf, uint64_t n, int has_halo, int mode, uint32_t bins,
+                   uint32_t stride = 1, bool estimated = false, uint64_t overflow_start = 0,
+                   uint64_t overflow_end = 0) {
     const uint64_t tiles = ceil_div(ceil_div(n, kc::EXT_TILE), std::max<uint32_t>(stride, 1));
     if (!tiles) return KC_OK;
     kc::ExtractArgs a{};
@@ -498,8 +500,8 @@ int launch_extract(kc_context* c, const uint8_t* buf, uint64_t n, int has_halo, 
     a.has_halo = has_halo;
     a.tile_line = c->tile_line.as<uint64_t>();
     a.k = c->cfg.k;
-    a.bucket_shift = c->bucket_shift;
-    a.n_buckets = c->n_buckets;
+    a.bucket_shift = 64 - (bins == 4096 ? 12 : 8);
+    a.n_buckets = bins;
     a.bucket_count = c->bucket_count.as<unsigned long long>();
     a.bucket_cursor = c->bucket_cursor.as<unsigned long long>();
     a.routed = c->routed.p;
@@ -515,10 +517,10 @@ int launch_extract(kc_context* c, const uint8_t* buf, uint64_t n, int has_halo, 
     Stage st(c, mode == kc::HIST ? KC_STAGE_EXTRACT_HIST : KC_STAGE_EXTRACT_SCATTER);
     if (mode == kc::HIST)
         kc::extract_kernel<NW, kc::HIST>
-            <<<tiles, kc::EXT_THREADS, kc::extract_smem_bytes<NW, kc::HIST>(c->n_buckets), c->stream>>>(a);
+            <<<tiles, kc::EXT_THREADS, kc::extract_smem_bytes<NW, kc::HIST>(bins), c->stream>>>(a);
     else
         kc::extract_kernel<NW, kc::SCATTER>
-            <<<tiles, kc::EXT_THREADS, kc::extract_smem_bytes<NW, kc::SCATTER>(c->n_buckets), c->stream>>>(a);
+            <<<tiles, kc::EXT_THREADS, kc::extract_smem_bytes<NW, kc::SCATTER>(bins), c->stream>>>(a);
     CK(cudaGetLastError());
     return KC_OK;
 }
@@ -556,15 +558,23 @@ int process_batch(kc_context* c, const uint8_t* buf, uint64_t n, int has_halo) {
     // the regions (counted like the rest; the unfilled region tails hold EMPTY
     // keys, which the count kernel skips).  If the overflow area itself fills,
     // the batch is routed again from an exact histogram of every tile.
+    //
+    // Keys are routed by their top 8 bits (rb = 256 routing buckets) whatever
+    // the table partition: with 4096 table buckets, the 16 that share a
+    // routing bucket are adjacent in the filter and table arenas, so a routed
+    // region still touches one contiguous working set, and the scatter keeps
+    // its 256-bucket shared-memory footprint.  The histogram counts all nb
+    // table buckets (sizing is per table bucket).
     constexpr int CT = kc::count_tile<NW>();
     constexpr int SEG = kc::count_seg<NW>();
-    bool est = nb <= 256 && tiles >= kc::EST_MIN_TILES;
-    std::vector<uint64_t> start(nb), end(nb), cursor(nb);
+    const uint32_t rb = std::min<uint32_t>(nb, 256), per = nb / rb;
+    bool est = tiles >= kc::EST_MIN_TILES;
+    std::vector<uint64_t> start(rb), end(rb), cursor(rb);
     uint64_t n_keys = 0, kb = 0;
     for (int attempt = 0;; ++attempt) {
         const uint32_t stride = est ? kc::EST_STRIDE : 1u;
         CKR(fill_dev(c, c->bucket_count.p, nb * sizeof(uint64_t), 0));
-        if ((rc = launch_extract<NW>(c, buf, n, has_halo, kc::HIST, stride))) return rc;
+        if ((rc = launch_extract<NW>(c, buf, n, has_halo, kc::HIST, nb, stride))) return rc;
         c->h_bucket_count.resize(nb);
         uint64_t line_end = 0;
         CKR(get(c, c->h_bucket_count.data(), c->bucket_count.p, nb * sizeof(uint64_t)));
@@ -575,13 +585,15 @@ int process_batch(kc_context* c, const uint8_t* buf, uint64_t n, int has_halo) {
         std::vector<uint64_t> kest(nb);
         uint64_t total_cap = 0;
         const double f = est ? (double)tiles / (double)ceil_div(tiles, stride) : 1.0;
-        for (uint32_t b = 0; b < nb; ++b) {
-            const double e = (double)c->h_bucket_count[b] * f;
-            kest[b] = (uint64_t)e;
-            const uint64_t cap = est ? (uint64_t)(e * 1.02 + 4.0 * std::sqrt(e) + 256.0) : c->h_bucket_count[b];
-            start[b] = total_cap;
+        for (uint32_t b = 0; b < nb; ++b) kest[b] = (uint64_t)((double)c->h_bucket_count[b] * f);
+        for (uint32_t r = 0; r < rb; ++r) {
+            uint64_t exact = 0;
+            for (uint32_t q = 0; q < per; ++q) exact += c->h_bucket_count[r * per + q];
+            const double e = (double)exact * f;
+            const uint64_t cap = est ? (uint64_t)(e * 1.02 + 4.0 * std::sqrt(e) + 256.0) : exact;
+            start[r] = total_cap;
             total_cap += cap;
-            end[b] = total_cap;
+            end[r] = total_cap;
         }
         // at least 65536 keys: one CTA's run of a bucket (<= 8192 keys) always fits
         const uint64_t ovf_cap = est ? std::max<uint64_t>(1ull << 16, total_cap / 32) : 0;
@@ -598,20 +610,20 @@ int process_batch(kc_context* c, const uint8_t* buf, uint64_t n, int has_halo) {
         CK(c->tile_low.ensure(ctiles * (CT / SEG) * sizeof(uint32_t)));
         CK(c->tile_fail.ensure(ctiles * (CT / SEG) * sizeof(uint32_t)));
         CK(c->tile_low_prefix.ensure(ctiles * (CT / SEG) * sizeof(uint64_t)));
-        CKR(put(c, c->bucket_cursor.p, start.data(), nb * sizeof(uint64_t)));
+        CKR(put(c, c->bucket_cursor.p, start.data(), rb * sizeof(uint64_t)));
         if (est) {
-            CKR(put(c, c->region_end.p, end.data(), nb * sizeof(uint64_t)));
+            CKR(put(c, c->region_end.p, end.data(), rb * sizeof(uint64_t)));
             CKR(put(c, d_scal + 2, &total_cap, sizeof(uint64_t)));
-            CKR(fill_dev(c, c->region_fill.p, nb * sizeof(uint64_t), 0xFFFFFFFFu));
+            CKR(fill_dev(c, c->region_fill.p, rb * sizeof(uint64_t), 0xFFFFFFFFu));
         }
-        if ((rc = launch_extract<NW>(c, buf, n, has_halo, kc::SCATTER, 1, est, total_cap, cap_keys))) return rc;
+        if ((rc = launch_extract<NW>(c, buf, n, has_halo, kc::SCATTER, rb, 1, est, total_cap, cap_keys))) return rc;
         if (!est) {
             n_keys = kb = total_cap;
             break;
         }
         uint64_t ovf_used = 0;
         uint32_t flags = 0;
-        CKR(get(c, cursor.data(), c->bucket_cursor.p, nb * sizeof(uint64_t)));
+        CKR(get(c, cursor.data(), c->bucket_cursor.p, rb * sizeof(uint64_t)));
         CKR(get(c, &ovf_used, d_scal + 2, sizeof(uint64_t)));
         CKR(get(c, &flags, c->scalars.as<uint32_t>() + 12, sizeof(uint32_t)));
         CKR(sync_stream(c));
@@ -623,17 +635,13 @@ int process_batch(kc_context* c, const uint8_t* buf, uint64_t n, int has_halo) {
         }
         c->overflow_keys += ovf_used - total_cap;
         kb = 0;
-        for (uint32_t b = 0; b < nb; ++b) {
-            c->h_bucket_count[b] = cursor[b] - start[b];
-            kb += c->h_bucket_count[b];
-        }
+        for (uint32_t r = 0; r < rb; ++r) kb += cursor[r] - start[r];
         n_keys = ovf_used;  // regions, then the used part of the overflow area
         {
             Stage st(c, KC_STAGE_EXTRACT_SCATTER);
-            if (nb)
-                kc::fill_region_gaps<NW><<<nb, 256, 0, c->stream>>>(
-                    c->routed.p, c->bucket_cursor.as<unsigned long long>(), c->region_fill.as<unsigned long long>(),
-                    c->region_end.as<unsigned long long>(), nb);
+            kc::fill_region_gaps<NW><<<rb, 256, 0, c->stream>>>(
+                c->routed.p, c->bucket_cursor.as<unsigned long long>(), c->region_fill.as<unsigned long long>(),
+                c->region_end.as<unsigned long long>(), rb);
             CK(cudaGetLastError());
         }
         break;
