@@ -54,7 +54,7 @@ extern "C" {
  * (src/main.cpp:314-374); n_thread, mem_gb and map_capacity have no meaning on
  * the device and are accepted and ignored by the CLI. */
 typedef struct kc_config {
-    uint32_t k;            /* 1..64; key words N = 1 for k<=32, 2 for k<=64 */
+    uint32_t k;            /* 1..128; key words N = 1 for k<=32, 2 for k<=64, 4 for k<=128 */
     uint32_t canonical;    /* must be 1: the reference always counts canonical */
     uint32_t min_count;    /* root-record filter, inclusive (src/NewKmerTree.h:1159-1168) */
     uint32_t max_count;

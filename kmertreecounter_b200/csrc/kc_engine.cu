@@ -250,7 +250,7 @@ struct Stage {
 
 int setup_shape(kc_context* c) {
     const kc_config& g = c->cfg;
-    if (g.k < 1 || g.k > 64) return fail(KC_ERR_INVALID, "k=%u out of range: this build supports 1..64", g.k);
+    if (g.k < 1 || g.k > 128) return fail(KC_ERR_INVALID, "k=%u out of range: 1..128", g.k);
     if (g.canonical != 1) return fail(KC_ERR_INVALID, "only canonical counting is supported (the reference has no other mode)");
     if (g.max_count < g.min_count) return fail(KC_ERR_INVALID, "max_count < min_count");
     if (g.n_buckets != 256 && g.n_buckets != 4096) return fail(KC_ERR_INVALID, "n_buckets must be 256 or 4096");
@@ -259,11 +259,11 @@ int setup_shape(kc_context* c) {
     if (g.batch_bytes < (1ull << 20)) return fail(KC_ERR_INVALID, "batch_bytes must be at least 1 MiB");
     if (g.device_batch_bytes && g.device_batch_bytes < (1ull << 20))
         return fail(KC_ERR_INVALID, "device_batch_bytes must be 0 or at least 1 MiB");
-    c->nw = g.k <= 32 ? 1 : 2;
+    c->nw = g.k <= 32 ? 1 : (g.k <= 64 ? 2 : 4);
     c->n_buckets = g.n_buckets;
     c->bucket_bits = g.n_buckets == 256 ? 8 : 12;
     c->bucket_shift = 64 - c->bucket_bits;
-    c->slot_bytes = c->nw == 1 ? sizeof(kc::Slot1) : sizeof(kc::Slot2);
+    c->slot_bytes = c->nw == 1 ? sizeof(kc::Slot1) : (c->nw == 2 ? sizeof(kc::Slot2) : sizeof(kc::Slot4));
     c->record_bytes = kc_record_bytes(g.k);
     c->packed_bytes = kc_packed_bytes(g.k);
     return KC_OK;
@@ -402,7 +402,8 @@ int size_structures(kc_context* c, const std::vector<uint64_t>& kb, double scale
         CKR(fill_dev(c, c->bloom.p, bw * sizeof(uint64_t), 0));
         const int ig = 148 * 8;
         if (c->nw == 1) kc::init_slots<1><<<ig, 256, 0, c->stream>>>(c->table.p, ts);
-        else kc::init_slots<2><<<ig, 256, 0, c->stream>>>(c->table.p, ts);
+        else if (c->nw == 2) kc::init_slots<2><<<ig, 256, 0, c->stream>>>(c->table.p, ts);
+        else kc::init_slots<4><<<ig, 256, 0, c->stream>>>(c->table.p, ts);
         CK(cudaGetLastError());
     }
     CK(c->overflow.ensure(nb * sizeof(uint32_t)));
@@ -427,6 +428,7 @@ void launch_count(kc_context* c, uint64_t n_keys, int use_filter) {
     a.seg_low = c->tile_low.as<uint32_t>();
     a.seg_fail = c->tile_fail.as<uint32_t>();
     a.bucket_overflow = c->overflow.as<uint32_t>();
+    a.error = c->scalars.as<uint32_t>() + 13;
     a.bucket_shift = c->bucket_shift;
     a.n_buckets = c->n_buckets;
     a.use_filter = use_filter;
@@ -537,7 +539,7 @@ int process_batch(kc_context* c, const uint8_t* buf, uint64_t n, int has_halo) {
     CK(c->tile_line.ensure(std::max<uint64_t>(tiles, 1) * sizeof(uint64_t)));
     CK(c->scalars.ensure(64));
     uint64_t* d_scal = c->scalars.as<uint64_t>();
-    CKR(fill_dev(c, c->scalars.as<uint32_t>() + 12, sizeof(uint32_t), 0));
+    CKR(fill_dev(c, c->scalars.as<uint32_t>() + 12, 2 * sizeof(uint32_t), 0));  // extraction and count error words
     if (tiles) {
         Stage st(c, KC_STAGE_LINES);
         kc::lines_per_tile<<<tiles, kc::EXT_THREADS, 0, c->stream>>>(buf, n, c->tile_nl.as<uint32_t>());
@@ -661,9 +663,12 @@ int process_batch(kc_context* c, const uint8_t* buf, uint64_t n, int has_halo) {
                                               c->tile_low_prefix.as<uint64_t>(), 0, d_scal + 1)))
         return rc;
     uint64_t nlow = 0;
+    uint32_t cnt_err = 0;
     CKR(get(c, &nlow, d_scal + 1, sizeof(uint64_t)));
+    CKR(get(c, &cnt_err, c->scalars.as<uint32_t>() + 13, sizeof(uint32_t)));
     CKR(sync_stream(c));
     if (ext_err) return fail(KC_ERR_DEVICE, "internal error: routing bucket disagreed with its reservation");
+    if (cnt_err) return fail(KC_ERR_DEVICE, "internal error: a 256-bit table slot was never published");
     uint8_t* low_dst;
     uint64_t low_base;
     if (c->stream_low) {
@@ -812,7 +817,7 @@ int finish_run(kc_context* c) {
         std::vector<uint64_t> zero(c->n_buckets, 0);
         if ((rc = size_structures(c, zero, 1.0))) return rc;
     }
-    rc = c->nw == 1 ? export_tables<1>(c) : export_tables<2>(c);
+    rc = c->nw == 1 ? export_tables<1>(c) : (c->nw == 2 ? export_tables<2>(c) : export_tables<4>(c));
     if (rc) return rc;
     if (c->cfg.sort_output && c->root_total > 1) {
         uint64_t bt, bh, bo, bs;
@@ -957,7 +962,9 @@ int stream_out_roots(kc_context* c) {
 int run_batch(kc_context* c, const uint8_t* buf, uint64_t n, int has_halo) {
     c->batches++;
     c->input_bytes += n;
-    return c->nw == 1 ? process_batch<1>(c, buf, n, has_halo) : process_batch<2>(c, buf, n, has_halo);
+    if (c->nw == 1) return process_batch<1>(c, buf, n, has_halo);
+    if (c->nw == 2) return process_batch<2>(c, buf, n, has_halo);
+    return process_batch<4>(c, buf, n, has_halo);
 }
 
 }  // namespace
@@ -1046,6 +1053,10 @@ int kc_create(const kc_config* cfg, kc_context** out) {
                          (int)kc::extract_smem_bytes<2, kc::HIST>(4096));
     cudaFuncSetAttribute(kc::extract_kernel<2, kc::SCATTER>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)kc::extract_smem_bytes<2, kc::SCATTER>(4096));
+    cudaFuncSetAttribute(kc::extract_kernel<4, kc::HIST>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)kc::extract_smem_bytes<4, kc::HIST>(4096));
+    cudaFuncSetAttribute(kc::extract_kernel<4, kc::SCATTER>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)kc::extract_smem_bytes<4, kc::SCATTER>(4096));
     if ((e = cudaGetLastError()) != cudaSuccess) {
         delete c;
         return fail(KC_ERR_DEVICE, "kernel attribute setup failed: %s", cudaGetErrorString(e));
@@ -1288,6 +1299,49 @@ int kc_count_host_stream(kc_context* c, const uint8_t* fastq, uint64_t n, kc_sin
     return KC_OK;
 }
 
+}  // extern "C"
+
+namespace {
+
+// Merged-count histogram kernels: low.bin keys looked up (and marked) in
+// their tables, then every unmarked key of each live bucket table (regions
+// left behind by a rehash are stale copies and are not walked).
+template <int NW>
+void histogram_kernels(kc_context* c, uint32_t min_freq, uint32_t max_freq, unsigned long long* d, uint64_t bins) {
+    const int grid = c->sm_count * 8;
+    kc::hist_clear_marks<NW><<<grid, 256, 0, c->stream>>>(c->table.p, c->table_slots_used);
+    kc::hist_low_pass<NW><<<grid, 256, 0, c->stream>>>(c->low_packed.as<uint8_t>(), c->low_total, c->cfg.k,
+                                                       c->meta.as<kc::BucketMeta>(), c->bucket_shift, c->table.p,
+                                                       min_freq, max_freq, d);
+    for (uint32_t b = 0; b < c->n_buckets; ++b) {
+        const uint64_t n = c->h_meta[b].tab_mask + 1;
+        uint8_t* t = c->table.as<uint8_t>() + c->h_meta[b].tab_off * c->slot_bytes;
+        const int g = (int)std::min<uint64_t>(grid, ceil_div(n, 256));
+        kc::hist_table_pass<NW><<<g, 256, 0, c->stream>>>(t, n, min_freq, max_freq, d, d + bins);
+    }
+}
+
+// Per model bucket loads: dd[0..4096) distinct, [4096..8192) table keys,
+// [8192..12288) k-mer occurrences.
+template <int NW>
+void loads_kernels(kc_context* c, unsigned long long* dd) {
+    const int grid = c->sm_count * 8;
+    kc::hist_clear_marks<NW><<<grid, 256, 0, c->stream>>>(c->table.p, c->table_slots_used);
+    kc::loads_low_pass<NW><<<grid, 256, 0, c->stream>>>(c->low_packed.as<uint8_t>(), c->low_total, c->cfg.k,
+                                                        c->meta.as<kc::BucketMeta>(), c->bucket_shift, c->table.p, dd,
+                                                        dd + 2 * KC_MODEL_BUCKETS);
+    for (uint32_t b = 0; b < c->n_buckets; ++b) {
+        const uint64_t n = c->h_meta[b].tab_mask + 1;
+        uint8_t* t = c->table.as<uint8_t>() + c->h_meta[b].tab_off * c->slot_bytes;
+        const int g = (int)std::min<uint64_t>(grid, ceil_div(n, 256));
+        kc::loads_table_pass<NW><<<g, 256, 0, c->stream>>>(t, n, dd, dd + KC_MODEL_BUCKETS, dd + 2 * KC_MODEL_BUCKETS);
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
 // Merged count histogram and distinct keys of the last device-held result.
 int kc_histogram(kc_context* c, uint32_t min_freq, uint32_t max_freq, uint64_t* hist, uint64_t* distinct) {
     if (!c) return fail(KC_ERR_INVALID, "null context");
@@ -1301,28 +1355,9 @@ int kc_histogram(kc_context* c, uint32_t min_freq, uint32_t max_freq, uint64_t* 
     CK(gh.ensure((bins + 1) * sizeof(unsigned long long)));
     unsigned long long* d = gh.as<unsigned long long>();
     CK(cudaMemsetAsync(d, 0, (bins + 1) * sizeof(unsigned long long), c->stream));
-    const int grid = c->sm_count * 8;
-    const uint64_t slots = c->table_slots_used;
-    if (c->nw == 1) {
-        kc::hist_clear_marks<1><<<grid, 256, 0, c->stream>>>(c->table.p, slots);
-        kc::hist_low_pass<1><<<grid, 256, 0, c->stream>>>(c->low_packed.as<uint8_t>(), c->low_total, c->cfg.k,
-                                                          c->meta.as<kc::BucketMeta>(), c->bucket_shift, c->table.p,
-                                                          min_freq, max_freq, d);
-    } else {
-        kc::hist_clear_marks<2><<<grid, 256, 0, c->stream>>>(c->table.p, slots);
-        kc::hist_low_pass<2><<<grid, 256, 0, c->stream>>>(c->low_packed.as<uint8_t>(), c->low_total, c->cfg.k,
-                                                          c->meta.as<kc::BucketMeta>(), c->bucket_shift, c->table.p,
-                                                          min_freq, max_freq, d);
-    }
-    // only slots that belong to a live bucket table (regions left by a rehash
-    // are stale copies) -- walk each bucket's region
-    for (uint32_t b = 0; b < c->n_buckets; ++b) {
-        const uint64_t n = c->h_meta[b].tab_mask + 1;
-        uint8_t* t = c->table.as<uint8_t>() + c->h_meta[b].tab_off * c->slot_bytes;
-        const int g = (int)std::min<uint64_t>(grid, ceil_div(n, 256));
-        if (c->nw == 1) kc::hist_table_pass<1><<<g, 256, 0, c->stream>>>(t, n, min_freq, max_freq, d, d + bins);
-        else kc::hist_table_pass<2><<<g, 256, 0, c->stream>>>(t, n, min_freq, max_freq, d, d + bins);
-    }
+    if (c->nw == 1) histogram_kernels<1>(c, min_freq, max_freq, d, bins);
+    else if (c->nw == 2) histogram_kernels<2>(c, min_freq, max_freq, d, bins);
+    else histogram_kernels<4>(c, min_freq, max_freq, d, bins);
     CK(cudaGetLastError());
     std::vector<unsigned long long> h(bins + 1);
     CK(cudaMemcpyAsync(h.data(), d, (bins + 1) * sizeof(unsigned long long), cudaMemcpyDeviceToHost, c->stream));
@@ -1420,27 +1455,9 @@ extern "C" int kc_bucket_loads(kc_context* c, uint64_t* distinct, uint64_t* tabl
     CK(d.ensure(3 * KC_MODEL_BUCKETS * sizeof(unsigned long long)));
     unsigned long long* dd = d.as<unsigned long long>();
     CK(cudaMemsetAsync(dd, 0, 3 * KC_MODEL_BUCKETS * sizeof(unsigned long long), c->stream));
-    const int grid = c->sm_count * 8;
-    if (c->nw == 1) {
-        kc::hist_clear_marks<1><<<grid, 256, 0, c->stream>>>(c->table.p, c->table_slots_used);
-        kc::loads_low_pass<1><<<grid, 256, 0, c->stream>>>(c->low_packed.as<uint8_t>(), c->low_total, c->cfg.k,
-                                                           c->meta.as<kc::BucketMeta>(), c->bucket_shift, c->table.p,
-                                                           dd, dd + 2 * KC_MODEL_BUCKETS);
-    } else {
-        kc::hist_clear_marks<2><<<grid, 256, 0, c->stream>>>(c->table.p, c->table_slots_used);
-        kc::loads_low_pass<2><<<grid, 256, 0, c->stream>>>(c->low_packed.as<uint8_t>(), c->low_total, c->cfg.k,
-                                                           c->meta.as<kc::BucketMeta>(), c->bucket_shift, c->table.p,
-                                                           dd, dd + 2 * KC_MODEL_BUCKETS);
-    }
-    for (uint32_t b = 0; b < c->n_buckets; ++b) {
-        const uint64_t n = c->h_meta[b].tab_mask + 1;
-        uint8_t* t = c->table.as<uint8_t>() + c->h_meta[b].tab_off * c->slot_bytes;
-        const int g = (int)std::min<uint64_t>(grid, ceil_div(n, 256));
-        if (c->nw == 1)
-            kc::loads_table_pass<1><<<g, 256, 0, c->stream>>>(t, n, dd, dd + KC_MODEL_BUCKETS, dd + 2 * KC_MODEL_BUCKETS);
-        else
-            kc::loads_table_pass<2><<<g, 256, 0, c->stream>>>(t, n, dd, dd + KC_MODEL_BUCKETS, dd + 2 * KC_MODEL_BUCKETS);
-    }
+    if (c->nw == 1) loads_kernels<1>(c, dd);
+    else if (c->nw == 2) loads_kernels<2>(c, dd);
+    else loads_kernels<4>(c, dd);
     CK(cudaGetLastError());
     std::vector<unsigned long long> h(3 * KC_MODEL_BUCKETS);
     CK(cudaMemcpyAsync(h.data(), dd, h.size() * sizeof(unsigned long long), cudaMemcpyDeviceToHost, c->stream));

@@ -51,7 +51,8 @@ KC_HD uint64_t brev64(uint64_t x) {
 constexpr int EXT_THREADS = 256;                     // extraction CTA
 constexpr int EXT_BPT = 32;                          // bytes per thread
 constexpr int EXT_TILE = EXT_THREADS * EXT_BPT;      // 8 KiB per CTA
-constexpr int HALO = 64;                             // bytes kept before a batch
+constexpr int HALO = 128;                            // bytes kept before a batch (k - 1 <= 127)
+constexpr int HALO_SEGS = HALO / 32;                 // extraction segments of halo
 // The 256-bucket scatter staging area holds extraction to 4 CTAs per SM;
 // telling the compiler so lets it use up to 64 registers (measured 6% faster
 // than its default of 32).
@@ -68,6 +69,10 @@ constexpr int PROBE_LIMIT = 512;                     // linear-probe bound befor
 // (most significant, first bases), w1 = data[1].
 struct Key2 {
     uint64_t w0, w1;
+};
+// 256-bit key (k = 65..128), kmer<4> order: w0 most significant.
+struct Key4 {
+    uint64_t w0, w1, w2, w3;
 };
 
 // One extraction tile of a multi-set batch: bytes [start, min(start + 8 KiB,
@@ -94,6 +99,18 @@ struct __align__(16) Slot1 {
     uint32_t count;
     uint32_t pad;
 };
+// 256-bit keys have no CAS of their width: a slot is claimed by a CAS of
+// `state` (SLOT_EMPTY -> SLOT_WRITING); the owner writes the key and the first
+// count and publishes them with a release of state = SLOT_READY.  A thread
+// that meets a SLOT_WRITING slot waits for it (bounded) before comparing.
+constexpr uint32_t SLOT_EMPTY = 0, SLOT_WRITING = 1, SLOT_READY = 2;
+constexpr uint32_t PUBLISH_WAIT_LIMIT = 1u << 22;  // polls before a wait counts as a device error
+struct __align__(16) Slot4 {
+    uint64_t w0, w1, w2, w3;
+    uint32_t count;
+    uint32_t state;
+    uint64_t mark;  // merged-histogram mark (hist_* kernels)
+};
 struct __align__(32) Slot2 {
     uint64_t w0, w1;
     uint32_t count;
@@ -114,6 +131,9 @@ __device__ __forceinline__ uint64_t mix64(uint64_t x) {
 __device__ __forceinline__ uint64_t hash_key(uint64_t k) { return mix64(k); }
 __device__ __forceinline__ uint64_t hash_key(const Key2& k) {
     return mix64(k.w0 ^ mix64(k.w1 + 0x9e3779b97f4a7c15ull));
+}
+__device__ __forceinline__ uint64_t hash_key(const Key4& k) {
+    return mix64(k.w0 ^ mix64(k.w1 ^ mix64(k.w2 ^ mix64(k.w3 + 0x9e3779b97f4a7c15ull))));
 }
 
 // Reverse the order of the 32 two-bit bases of a word (base p -> 31-p).
@@ -139,9 +159,14 @@ template <>
 struct KeyOf<2> {
     using T = Key2;
 };
+template <>
+struct KeyOf<4> {
+    using T = Key4;
+};
 
 __device__ __forceinline__ uint64_t key_hi(uint64_t k) { return k; }
 __device__ __forceinline__ uint64_t key_hi(const Key2& k) { return k.w0; }
+__device__ __forceinline__ uint64_t key_hi(const Key4& k) { return k.w0; }
 
 // Canonical key of the window W (the last k bases, oldest base in the high
 // bits of the 2k-bit value, newest in bits 1..0).
@@ -173,6 +198,51 @@ KC_HD Key2 canonical2(uint64_t Whi, uint64_t Wlo, uint32_t k) {
         C.w1 = nlo << s;
     }
     const bool f_less = (F.w0 < C.w0) || (F.w0 == C.w0 && F.w1 < C.w1);
+    return f_less ? F : C;
+}
+
+// k = 65..128: the window is the 256-bit W3:W2:W1:W0 (W0 = the newest 32
+// bases, oldest base highest), of which the low 2k bits are the k bases.
+// F = base-reverse of all 256 bits (left-aligned by the reversal itself);
+// C = (~W masked to 2k bits) << (256 - 2k); key = the lexicographic min.
+KC_HD Key4 canonical4(uint64_t W0, uint64_t W1, uint64_t W2, uint64_t W3, uint32_t k) {
+    const uint32_t kb = 2 * k;  // 130..256
+    if (kb <= 192) {
+        W3 = 0;
+        if (kb < 192) W2 &= (1ull << (kb - 128)) - 1ull;
+    } else if (kb < 256) {
+        W3 &= (1ull << (kb - 192)) - 1ull;
+    }
+    const Key4 F{rev_bases(W0), rev_bases(W1), rev_bases(W2), rev_bases(W3)};
+    // ~W restricted to the 2k bits
+    uint64_t n0 = ~W0, n1 = ~W1, n2 = ~W2, n3 = ~W3;
+    if (kb <= 192) {
+        n3 = 0;
+        if (kb < 192) n2 &= (1ull << (kb - 128)) - 1ull;
+    } else if (kb < 256) {
+        n3 &= (1ull << (kb - 192)) - 1ull;
+    }
+    // shift left by sh = 256 - 2k (0..126): whole words first, then bits
+    const uint32_t sh = 256 - kb;
+    if (sh >= 64) {
+        n3 = n2;
+        n2 = n1;
+        n1 = n0;
+        n0 = 0;
+    }
+    const uint32_t r = sh & 63;
+    if (r) {
+        n3 = (n3 << r) | (n2 >> (64 - r));
+        n2 = (n2 << r) | (n1 >> (64 - r));
+        n1 = (n1 << r) | (n0 >> (64 - r));
+        n0 = n0 << r;
+    }
+    const Key4 C{n3, n2, n1, n0};
+    bool f_less;
+    if (F.w0 != C.w0) f_less = F.w0 < C.w0;
+    else if (F.w1 != C.w1) f_less = F.w1 < C.w1;
+    else if (F.w2 != C.w2) f_less = F.w2 < C.w2;
+    else f_less = F.w3 < C.w3;
     return f_less ? F : C;
 }
 
@@ -353,6 +423,35 @@ __device__ __forceinline__ u128 runs_at_least(u128 X, uint32_t k) {
     return R;
 }
 
+// The same over five segments' base bits (b0 oldest .. b4 current, 160 bits)
+// for k = 65..128: bit j of the result = the k bytes ending at byte j of b4
+// are all bases.
+KC_HD uint32_t runs_at_least5(uint32_t b0, uint32_t b1, uint32_t b2, uint32_t b3, uint32_t b4, uint32_t k) {
+    uint64_t x0 = (uint64_t)b0 | ((uint64_t)b1 << 32), x1 = (uint64_t)b2 | ((uint64_t)b3 << 32), x2 = b4;
+    auto and_shifted = [&](uint32_t n) {  // X &= X << n, 1 <= n <= 64
+        uint64_t y0, y1, y2;
+        if (n == 64) {
+            y2 = x1;
+            y1 = x0;
+            y0 = 0;
+        } else {
+            y2 = (x2 << n) | (x1 >> (64 - n));
+            y1 = (x1 << n) | (x0 >> (64 - n));
+            y0 = x0 << n;
+        }
+        x0 &= y0;
+        x1 &= y1;
+        x2 &= y2;
+    };
+    uint32_t have = 1;
+    while (2 * have <= k) {
+        and_shifted(have);
+        have *= 2;
+    }
+    if (have < k) and_shifted(k - have);
+    return (uint32_t)x2;
+}
+
 // Bits of the 32 bytes that lie on sequence lines (line index = 1 mod 4),
 // line0 = line index of byte 0, nls = newline bits.
 __device__ __forceinline__ uint32_t sequence_mask(uint32_t line0, uint32_t nls) {
@@ -389,6 +488,24 @@ KC_HD void window_at(uint64_t s0, uint64_t s1, uint64_t s2, uint32_t j, uint64_t
     } else {
         lo = (s2 >> sh) | (s1 << (64 - sh));
         hi = (s1 >> sh) | (s0 << (64 - sh));
+    }
+}
+
+// The 256-bit window of the last 128 bases ending at byte j of segment s4
+// (segments s0..s3 precede it): W0 = the newest 32 bases.
+KC_HD void window_at4(uint64_t s0, uint64_t s1, uint64_t s2, uint64_t s3, uint64_t s4, uint32_t j, uint64_t& W0,
+                      uint64_t& W1, uint64_t& W2, uint64_t& W3) {
+    const uint32_t sh = 2 * (31 - j);
+    if (sh == 0) {
+        W0 = s4;
+        W1 = s3;
+        W2 = s2;
+        W3 = s1;
+    } else {
+        W0 = (s4 >> sh) | (s3 << (64 - sh));
+        W1 = (s3 >> sh) | (s2 << (64 - sh));
+        W2 = (s2 >> sh) | (s1 << (64 - sh));
+        W3 = (s1 >> sh) | (s0 << (64 - sh));
     }
 }
 
@@ -463,7 +580,7 @@ KC_HD uint32_t bucket_of_window(uint64_t lo, uint64_t hi, uint32_t k, uint32_t B
 // they are written out as contiguous runs; keys beyond this go out directly.
 template <int NW>
 __host__ __device__ constexpr int stage_keys() {
-    return NW == 1 ? 4096 : 2048;
+    return NW == 1 ? 4096 : (NW == 2 ? 2048 : 1024);
 }
 
 // Dynamic shared memory of extract_kernel.
@@ -477,8 +594,10 @@ __global__ void __launch_bounds__(EXT_THREADS, EXT_MIN_CTAS) extract_kernel(Extr
     // dynamic smem: u64 base[nb] | u32 hist[nb] | u32 fill[nb] | u32 loff[nb]
     //               | SCATTER: K keys[stage] | u16 bucket_of_key[stage]
     extern __shared__ unsigned long long ext_smem[];
-    __shared__ uint64_t seg_codes[EXT_THREADS + 2];
-    __shared__ uint32_t seg_bases[EXT_THREADS + 2];
+    // segment t of the tile is seg_*[t + HALO_SEGS]; the HALO_SEGS before it
+    // hold the halo bytes (zero where there is nothing to read)
+    __shared__ uint64_t seg_codes[EXT_THREADS + HALO_SEGS];
+    __shared__ uint32_t seg_bases[EXT_THREADS + HALO_SEGS];
     __shared__ uint32_t seg_emit[EXT_THREADS];
     __shared__ uint32_t warp_sums[EXT_THREADS / 32];
     __shared__ uint32_t tile_any;
@@ -515,14 +634,14 @@ __global__ void __launch_bounds__(EXT_THREADS, EXT_MIN_CTAS) extract_kernel(Extr
     }
     if (tid == 0) tile_any = 0;
 
-    // ---- phase A: classify own segment (+ the two halo segments)
+    // ---- phase A: classify own segment (+ the halo segments)
     uint32_t w[8];
     const uint64_t valid = seg_start < n_end ? n_end - seg_start : 0;
     load32(a.buf + seg_start, valid, w);
     const Seg s = classify(w, valid);
-    seg_codes[tid + 2] = s.codes;
-    seg_bases[tid + 2] = s.bases;
-    if (tid < 2) {
+    seg_codes[tid + HALO_SEGS] = s.codes;
+    seg_bases[tid + HALO_SEGS] = s.bases;
+    if (tid < HALO_SEGS) {
         uint32_t hw[8];
         const bool readable = halo_ok;
         load32(a.buf + (int64_t)tile_start - HALO + 32 * tid, readable ? 32 : 0, hw);
@@ -539,8 +658,13 @@ __global__ void __launch_bounds__(EXT_THREADS, EXT_MIN_CTAS) extract_kernel(Extr
     if (s.bases) {
         const uint32_t seq = sequence_mask(line0, s.nls);
         if (seq & s.bases) {
-            const u128 X = ((u128)s.bases << 64) | ((u128)seg_bases[tid + 1] << 32) | (u128)seg_bases[tid];
-            emit = (uint32_t)(runs_at_least(X, k) >> 64) & seq;
+            const uint32_t* sb = seg_bases + tid + HALO_SEGS;  // sb[0] = this segment
+            if constexpr (NW == 4) {
+                emit = runs_at_least5(sb[-4], sb[-3], sb[-2], sb[-1], s.bases, k) & seq;
+            } else {
+                const u128 X = ((u128)s.bases << 64) | ((u128)sb[-1] << 32) | (u128)sb[-2];
+                emit = (uint32_t)(runs_at_least(X, k) >> 64) & seq;
+            }
         }
     }
     seg_emit[tid] = emit;
@@ -601,9 +725,15 @@ __global__ void __launch_bounds__(EXT_THREADS, EXT_MIN_CTAS) extract_kernel(Extr
             const uint32_t em = seg_emit[t];
             if (!em) continue;  // warp-uniform
             if (!((em >> lane) & 1u)) continue;
-            uint64_t lo, hi;
-            window_at(seg_codes[t], seg_codes[t + 1], seg_codes[t + 2], (uint32_t)lane, lo, hi);
-            if (pass == 0) {
+            const uint64_t* sc = seg_codes + t + HALO_SEGS;  // sc[0] = segment t
+            uint64_t lo, hi, w2 = 0, w3 = 0;
+            if constexpr (NW == 4) window_at4(sc[-4], sc[-3], sc[-2], sc[-1], sc[0], (uint32_t)lane, lo, hi, w2, w3);
+            else window_at(sc[-2], sc[-1], sc[0], (uint32_t)lane, lo, hi);
+            if (pass == 0 && NW == 4) {
+                // 256-bit keys: the bucket from the full canonical key
+                const Key4 key4 = canonical4(lo, hi, w2, w3, k);
+                atomicAdd(hist + (uint32_t)(key4.w0 >> a.bucket_shift), 1u);
+            } else if (pass == 0) {
                 if (NW == 1) {
                     const uint64_t km = k >= 32 ? ~0ull : ((1ull << (2 * k)) - 1ull);
                     lo &= km;
@@ -619,10 +749,13 @@ __global__ void __launch_bounds__(EXT_THREADS, EXT_MIN_CTAS) extract_kernel(Extr
                     const uint64_t km = k >= 32 ? ~0ull : ((1ull << (2 * k)) - 1ull);
                     key = canonical1(lo & km, k);
                     bucket = (uint32_t)(key >> a.bucket_shift);
-                } else {
+                } else if constexpr (NW == 2) {
                     const uint32_t hb = 2 * k - 64;
                     const uint64_t hmask = hb >= 64 ? ~0ull : ((1ull << hb) - 1ull);
                     key = canonical2(hi & hmask, lo, k);
+                    bucket = (uint32_t)(key.w0 >> a.bucket_shift);
+                } else {
+                    key = canonical4(lo, hi, w2, w3, k);
                     bucket = (uint32_t)(key.w0 >> a.bucket_shift);
                 }
                 const uint32_t rnk = atomicAdd(fill + bucket, 1u);
@@ -722,12 +855,53 @@ static __device__ __noinline__ bool table_add_slow(Slot2* __restrict__ tab, uint
     return false;
 }
 
+// Insert `add` occurrences of a 256-bit key, probing from (h >> 17) & mask.
+// Returns 1 when added, 0 when the probe limit was hit (the bucket
+// overflows), -1 when a slot stayed SLOT_WRITING for PUBLISH_WAIT_LIMIT polls.
+static __device__ __noinline__ int table_add4(Slot4* __restrict__ tab, uint64_t mask, uint64_t h, const Key4& key,
+                                              uint32_t add) {
+    const uint64_t i = (h >> 17) & mask;
+    const int limit = (int)min((uint64_t)PROBE_LIMIT, mask + 1);
+    for (int p = 0; p < limit; ++p) {
+        Slot4* s = tab + ((i + p) & mask);
+        volatile uint32_t* state = &s->state;
+        uint32_t st = *state;
+        if (st == SLOT_EMPTY) {
+            st = atomicCAS(&s->state, SLOT_EMPTY, SLOT_WRITING);
+            if (st == SLOT_EMPTY) {  // claimed: key and first count, then publish
+                s->w0 = key.w0;
+                s->w1 = key.w1;
+                s->w2 = key.w2;
+                s->w3 = key.w3;
+                s->count = add;
+                __threadfence();
+                atomicExch(&s->state, SLOT_READY);
+                return 1;
+            }
+        }
+        for (uint32_t n = 0; st == SLOT_WRITING; ++n) {
+            if (n >= PUBLISH_WAIT_LIMIT) return -1;
+            st = *state;
+        }
+        __threadfence();  // pairs with the owner's fence: its key words are visible
+        const Key4 have{__ldcg(&s->w0), __ldcg(&s->w1), __ldcg(&s->w2), __ldcg(&s->w3)};
+        if (have.w0 == key.w0 && have.w1 == key.w1 && have.w2 == key.w2 && have.w3 == key.w3) {
+            atomicAdd(&s->count, add);
+            return 1;
+        }
+    }
+    return 0;
+}
+
 // Full insert (used by the table rehash).
 __device__ __forceinline__ bool table_add(Slot1* tab, uint64_t mask, uint64_t h, uint64_t key, uint32_t add) {
     return table_add_slow(tab, mask, h, key, add, 0);
 }
 __device__ __forceinline__ bool table_add(Slot2* tab, uint64_t mask, uint64_t h, const Key2& key, uint32_t add) {
     return table_add_slow(tab, mask, h, key, add, 0);
+}
+__device__ __forceinline__ bool table_add(Slot4* tab, uint64_t mask, uint64_t h, const Key4& key, uint32_t add) {
+    return table_add4(tab, mask, h, key, add) > 0;
 }
 
 // First probe already read (`seen`): settle the common cases inline -- the
@@ -754,6 +928,9 @@ __device__ __forceinline__ bool table_add_first(Slot2* tab, uint64_t mask, uint6
 
 __device__ __forceinline__ bool key_eq(uint64_t a, uint64_t b) { return a == b; }
 __device__ __forceinline__ bool key_eq(const Key2& a, const Key2& b) { return a.w0 == b.w0 && a.w1 == b.w1; }
+__device__ __forceinline__ bool key_eq(const Key4& a, const Key4& b) {
+    return a.w0 == b.w0 && a.w1 == b.w1 && a.w2 == b.w2 && a.w3 == b.w3;
+}
 
 template <int NW>
 struct SlotOf;
@@ -765,10 +942,14 @@ template <>
 struct SlotOf<2> {
     using T = Slot2;
 };
+template <>
+struct SlotOf<4> {
+    using T = Slot4;
+};
 
 template <int NW>
 __host__ __device__ constexpr int count_items() {
-    return NW == 1 ? 4 : 2;
+    return NW == 1 ? 4 : (NW == 2 ? 2 : 1);
 }
 // Keys owned by one warp of the count kernel (a contiguous segment).
 template <int NW>
@@ -789,6 +970,7 @@ struct CountArgs {
     uint32_t* seg_low;            // per warp segment: first occurrences kept at its front
     uint32_t* seg_fail;           // per warp segment: overflowed keys kept at its back
     uint32_t* bucket_overflow;    // set to 1 for a bucket whose table overflowed
+    uint32_t* error;              // 256-bit keys: set when a slot was never published
     uint32_t bucket_shift;
     uint32_t n_buckets;
     int use_filter;               // 0: retry pass (table only, no filter)
@@ -826,7 +1008,10 @@ template <int NW>
 __global__ void __launch_bounds__(CNT_THREADS, 4) count_routed(CountArgs a) {
     using K = typename KeyOf<NW>::T;
     using S = typename SlotOf<NW>::T;
-    using Seen = typename std::conditional<NW == 1, uint64_t, ulonglong2>::type;
+    // first table slot read ahead of the filter result (not for 256-bit keys,
+    // whose slots are read under the publish protocol of table_add4)
+    using Seen = typename std::conditional<NW == 1, uint64_t,
+                                           typename std::conditional<NW == 2, ulonglong2, uint32_t>::type>::type;
     constexpr int ITEMS = count_items<NW>();
     constexpr int SEG = count_seg<NW>();
     __shared__ MetaS sm[META_SMEM_BUCKETS];
@@ -885,11 +1070,13 @@ __global__ void __launch_bounds__(CNT_THREADS, 4) count_routed(CountArgs a) {
             const uint32_t idx = (uint32_t)(j * 32 + lane);
             mult[j] = idx < n_in ? 1u : 0u;
             if constexpr (NW == 1) it[j] = EMPTY;
-            else it[j] = Key2{EMPTY, EMPTY};
+            else if constexpr (NW == 2) it[j] = Key2{EMPTY, EMPTY};
+            else it[j] = Key4{EMPTY, EMPTY, EMPTY, EMPTY};
             if (mult[j]) {
                 it[j] = keys[base + idx];
                 if constexpr (NW == 1) mult[j] = it[j] != EMPTY;
-                else mult[j] = !(it[j].w0 == EMPTY && it[j].w1 == EMPTY);
+                else if constexpr (NW == 2) mult[j] = !(it[j].w0 == EMPTY && it[j].w1 == EMPTY);
+                else mult[j] = !(it[j].w0 == EMPTY && it[j].w1 == EMPTY && it[j].w2 == EMPTY && it[j].w3 == EMPTY);
             }
         }
         __syncwarp();  // every read of the segment precedes any in-place write
@@ -905,17 +1092,26 @@ __global__ void __launch_bounds__(CNT_THREADS, 4) count_routed(CountArgs a) {
             if constexpr (NW == 1) {
                 const uint64_t nx = __shfl_down_sync(0xffffffffu, it[j], 1);
                 eq_next = nx == it[j];
-            } else {
+            } else if constexpr (NW == 2) {
                 const uint64_t n0 = __shfl_down_sync(0xffffffffu, it[j].w0, 1);
                 const uint64_t n1 = __shfl_down_sync(0xffffffffu, it[j].w1, 1);
                 eq_next = n0 == it[j].w0 && n1 == it[j].w1;
+            } else {
+                const uint64_t n0 = __shfl_down_sync(0xffffffffu, it[j].w0, 1);
+                const uint64_t n1 = __shfl_down_sync(0xffffffffu, it[j].w1, 1);
+                const uint64_t n2 = __shfl_down_sync(0xffffffffu, it[j].w2, 1);
+                const uint64_t n3 = __shfl_down_sync(0xffffffffu, it[j].w3, 1);
+                eq_next = n0 == it[j].w0 && n1 == it[j].w1 && n2 == it[j].w2 && n3 == it[j].w3;
             }
             if (!__any_sync(0xffffffffu, eq_next && lane < 31 && mult[j] != 0)) continue;  // warp-uniform
             const uint32_t active = __ballot_sync(0xffffffffu, mult[j] != 0);
             if (mult[j]) {
                 uint32_t same;
                 if constexpr (NW == 1) same = __match_any_sync(active, it[j]);
-                else same = __match_any_sync(active, it[j].w0) & __match_any_sync(active, it[j].w1);
+                else if constexpr (NW == 2) same = __match_any_sync(active, it[j].w0) & __match_any_sync(active, it[j].w1);
+                else
+                    same = __match_any_sync(active, it[j].w0) & __match_any_sync(active, it[j].w1) &
+                           __match_any_sync(active, it[j].w2) & __match_any_sync(active, it[j].w3);
                 mult[j] = ((__ffs(same) - 1) == lane) ? (uint32_t)__popc(same) : 0u;
             }
         }
@@ -932,7 +1128,8 @@ __global__ void __launch_bounds__(CNT_THREADS, 4) count_routed(CountArgs a) {
                 if (a.use_filter) old[j] = __ldcg(a.bloom + m.bloom_off + (h[j] & m.bloom_mask));
                 const S* slot = table + m.tab_off + ((h[j] >> 17) & m.tab_mask);
                 if constexpr (NW == 1) seen[j] = __ldcg(&slot->key);
-                else seen[j] = __ldcg(reinterpret_cast<const ulonglong2*>(slot));
+                else if constexpr (NW == 2) seen[j] = __ldcg(reinterpret_cast<const ulonglong2*>(slot));
+                else seen[j] = 0;
             }
         }
         uint32_t first_bits = 0;  // bit j: item j is a first occurrence
@@ -957,7 +1154,15 @@ __global__ void __launch_bounds__(CNT_THREADS, 4) count_routed(CountArgs a) {
             if (mult[j] && reps) {
                 const uint32_t b = set_bucket0 + (uint32_t)(key_hi(it[j]) >> a.bucket_shift);
                 const MetaS m = meta_of(b);
-                if (!table_add_first(table + m.tab_off, m.tab_mask, h[j], it[j], reps, seen[j])) {
+                bool added;
+                if constexpr (NW == 4) {
+                    const int r = table_add4(table + m.tab_off, m.tab_mask, h[j], it[j], reps);
+                    if (r < 0) atomicOr(a.error, 1u);  // a slot was never published: reported, not retried
+                    added = r != 0;
+                } else {
+                    added = table_add_first(table + m.tab_off, m.tab_mask, h[j], it[j], reps, seen[j]);
+                }
+                if (!added) {
                     fail_bits |= 1u << j;
                     mult[j] = reps;  // keep the count that still has to be added
                     a.bucket_overflow[b] = 1u;
@@ -1010,9 +1215,13 @@ __global__ void rehash_bucket(const void* old_tab, uint64_t old_slots, void* new
         if constexpr (NW == 1) {
             if (s.key == EMPTY) continue;
             if (!table_add(dst, new_mask, hash_key(s.key), s.key, s.count)) atomicExch(failed, 1u);
-        } else {
+        } else if constexpr (NW == 2) {
             if (s.w0 == EMPTY && s.w1 == EMPTY) continue;
             const Key2 k{s.w0, s.w1};
+            if (!table_add(dst, new_mask, hash_key(k), k, s.count)) atomicExch(failed, 1u);
+        } else {
+            if (s.state != SLOT_READY) continue;
+            const Key4 k{s.w0, s.w1, s.w2, s.w3};
             if (!table_add(dst, new_mask, hash_key(k), k, s.count)) atomicExch(failed, 1u);
         }
     }
@@ -1029,11 +1238,16 @@ __global__ void init_slots(void* tab, uint64_t n) {
             s.key = EMPTY;
             s.count = 0;
             s.pad = 0;
-        } else {
+        } else if constexpr (NW == 2) {
             s.w0 = EMPTY;
             s.w1 = EMPTY;
             s.count = 0;
             s.pad[0] = s.pad[1] = s.pad[2] = 0;
+        } else {
+            s.w0 = s.w1 = s.w2 = s.w3 = 0;
+            s.count = 0;
+            s.state = SLOT_EMPTY;
+            s.mark = 0;
         }
         t[i] = s;
     }
@@ -1060,27 +1274,34 @@ __global__ void pack_low(const void* routed, const uint32_t* seg_low, const uint
         const uint64_t o = out_base + seg_low_prefix[sg];
         for (uint32_t i = lane; i < n; i += 32) {
             const K key = keys[sg * (uint64_t)SEG + i];
-            uint64_t w0, w1;
+            uint64_t w[4] = {0, 0, 0, 0};
             if constexpr (NW == 1) {
-                w0 = key;
-                w1 = 0;
+                w[0] = key;
+            } else if constexpr (NW == 2) {
+                w[0] = key.w0;
+                w[1] = key.w1;
             } else {
-                w0 = key.w0;
-                w1 = key.w1;
+                w[0] = key.w0;
+                w[1] = key.w1;
+                w[2] = key.w2;
+                w[3] = key.w3;
             }
             uint8_t* d = out + (o + i) * P;
             if (P == 8) {
-                *reinterpret_cast<uint64_t*>(d) = full ? w0 : (w0 & tmask);
+                *reinterpret_cast<uint64_t*>(d) = full ? w[0] : (w[0] & tmask);
             } else if (P == 16) {
-                reinterpret_cast<uint64_t*>(d)[0] = w0;
-                reinterpret_cast<uint64_t*>(d)[1] = full == 2 ? w1 : (w1 & tmask);
+                reinterpret_cast<uint64_t*>(d)[0] = w[0];
+                reinterpret_cast<uint64_t*>(d)[1] = full == 2 ? w[1] : (w[1] & tmask);
             } else {
+                // k/32 whole words little-endian, then the top tail_bytes bytes
+                // of the masked tail word (src/ExportWriter.h:522-550)
                 uint32_t q = 0;
-                if (full) {
-                    for (uint32_t b = 0; b < 8; ++b) d[q++] = (uint8_t)(w0 >> (8 * b));
+                for (uint32_t f = 0; f < full; ++f)
+                    for (uint32_t b = 0; b < 8; ++b) d[q++] = (uint8_t)(w[f] >> (8 * b));
+                if (tail_bytes) {
+                    const uint64_t tw = w[full] & tmask;
+                    for (uint32_t b = 8 - tail_bytes; b < 8; ++b) d[q++] = (uint8_t)(tw >> (8 * b));
                 }
-                const uint64_t tw = (full ? w1 : w0) & tmask;
-                for (uint32_t b = 8 - tail_bytes; b < 8; ++b) d[q++] = (uint8_t)(tw >> (8 * b));
             }
         }
     }
@@ -1096,7 +1317,8 @@ struct ExportChunk {
 template <int NW>
 __device__ __forceinline__ bool slot_used(const typename SlotOf<NW>::T& s) {
     if constexpr (NW == 1) return s.key != EMPTY;
-    else return !(s.w0 == EMPTY && s.w1 == EMPTY);
+    else if constexpr (NW == 2) return !(s.w0 == EMPTY && s.w1 == EMPTY);
+    else return s.state == SLOT_READY;
 }
 
 constexpr int EXP_THREADS = 256;
@@ -1213,11 +1435,18 @@ __global__ void __launch_bounds__(EXP_THREADS) export_write(const void* table, c
                     w.z = v[j].count;
                     w.w = 0;
                     reinterpret_cast<uint4*>(records)[r] = w;
-                } else {
+                } else if constexpr (NW == 2) {
                     uint64_t* d = reinterpret_cast<uint64_t*>(records + r * 24);
                     d[0] = v[j].w0;
                     d[1] = v[j].w1;
                     d[2] = (uint64_t)v[j].count;
+                } else {
+                    uint64_t* d = reinterpret_cast<uint64_t*>(records + r * 40);
+                    d[0] = v[j].w0;
+                    d[1] = v[j].w1;
+                    d[2] = v[j].w2;
+                    d[3] = v[j].w3;
+                    d[4] = (uint64_t)v[j].count;
                 }
                 ++r;
             }
@@ -1250,9 +1479,12 @@ __device__ __forceinline__ bool table_find(const typename SlotOf<NW>::T* tab, ui
         if constexpr (NW == 1) {
             empty = s.key == EMPTY;
             eq = s.key == key;
-        } else {
+        } else if constexpr (NW == 2) {
             empty = s.w0 == EMPTY && s.w1 == EMPTY;
             eq = s.w0 == key.w0 && s.w1 == key.w1;
+        } else {
+            empty = s.state != SLOT_READY;  // after the count every used slot is ready
+            eq = !empty && s.w0 == key.w0 && s.w1 == key.w1 && s.w2 == key.w2 && s.w3 == key.w3;
         }
         if (eq) {
             *where = i;
@@ -1277,7 +1509,8 @@ __global__ void hist_clear_marks(void* table, uint64_t n_slots) {
     S* t = reinterpret_cast<S*>(table);
     for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n_slots; i += (uint64_t)gridDim.x * blockDim.x) {
         if constexpr (NW == 1) t[i].pad = 0;
-        else t[i].pad[0] = 0;
+        else if constexpr (NW == 2) t[i].pad[0] = 0;
+        else t[i].mark = 0;
     }
 }
 
@@ -1294,13 +1527,14 @@ __global__ void hist_low_pass(const uint8_t* low, uint64_t n_low, uint32_t k, co
     const uint32_t P = full * 8 + tail_bytes;
     for (uint64_t r = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; r < n_low; r += (uint64_t)gridDim.x * blockDim.x) {
         const uint8_t* p = low + r * P;
-        uint64_t w[2] = {0, 0};
+        uint64_t w[4] = {0, 0, 0, 0};
         for (uint32_t f = 0; f < full; ++f)
             for (uint32_t b = 0; b < 8; ++b) w[f] |= (uint64_t)p[8 * f + b] << (8 * b);
         for (uint32_t b = 0; b < tail_bytes; ++b) w[full] |= (uint64_t)p[8 * full + b] << (8 * (8 - tail_bytes + b));
         K key;
         if constexpr (NW == 1) key = w[0];
-        else key = Key2{w[0], w[1]};
+        else if constexpr (NW == 2) key = Key2{w[0], w[1]};
+        else key = Key4{w[0], w[1], w[2], w[3]};
         const BucketMeta m = meta[key_hi(key) >> bucket_shift];
         S* tab = reinterpret_cast<S*>(table) + m.tab_off;
         uint64_t at;
@@ -1308,7 +1542,8 @@ __global__ void hist_low_pass(const uint8_t* low, uint64_t n_low, uint32_t k, co
         if (table_find<NW>(tab, m.tab_mask, hash_key(key), key, &at)) {
             merged = (uint64_t)tab[at].count + 1;
             if constexpr (NW == 1) tab[at].pad = 1;
-            else tab[at].pad[0] = 1;
+            else if constexpr (NW == 2) tab[at].pad[0] = 1;
+            else tab[at].mark = 1;
         }
         hist_add(sh, gh, merged, lo, hi);
     }
@@ -1334,9 +1569,12 @@ __global__ void hist_table_pass(const void* table, uint64_t n_slots, uint32_t lo
         if constexpr (NW == 1) {
             used = s.key != EMPTY;
             marked = s.pad != 0;
-        } else {
+        } else if constexpr (NW == 2) {
             used = !(s.w0 == EMPTY && s.w1 == EMPTY);
             marked = s.pad[0] != 0;
+        } else {
+            used = s.state == SLOT_READY;
+            marked = s.mark != 0;
         }
         if (used && !marked) {
             ++un;
@@ -1364,13 +1602,14 @@ __global__ void loads_low_pass(const uint8_t* low, uint64_t n_low, uint32_t k, c
     const uint32_t P = full * 8 + tail_bytes;
     for (uint64_t r = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; r < n_low; r += (uint64_t)gridDim.x * blockDim.x) {
         const uint8_t* p = low + r * P;
-        uint64_t w[2] = {0, 0};
+        uint64_t w[4] = {0, 0, 0, 0};
         for (uint32_t f = 0; f < full; ++f)
             for (uint32_t b = 0; b < 8; ++b) w[f] |= (uint64_t)p[8 * f + b] << (8 * b);
         for (uint32_t b = 0; b < tail_bytes; ++b) w[full] |= (uint64_t)p[8 * full + b] << (8 * (8 - tail_bytes + b));
         K key;
         if constexpr (NW == 1) key = w[0];
-        else key = Key2{w[0], w[1]};
+        else if constexpr (NW == 2) key = Key2{w[0], w[1]};
+        else key = Key4{w[0], w[1], w[2], w[3]};
         const BucketMeta m = meta[key_hi(key) >> bucket_shift];
         S* tab = reinterpret_cast<S*>(table) + m.tab_off;
         uint64_t at;
@@ -1378,7 +1617,8 @@ __global__ void loads_low_pass(const uint8_t* low, uint64_t n_low, uint32_t k, c
         if (table_find<NW>(tab, m.tab_mask, hash_key(key), key, &at)) {
             occ += tab[at].count;
             if constexpr (NW == 1) tab[at].pad = 1;
-            else tab[at].pad[0] = 1;
+            else if constexpr (NW == 2) tab[at].pad[0] = 1;
+            else tab[at].mark = 1;
         }
         atomicAdd(distinct + (key_hi(key) >> 52), 1ull);
         atomicAdd(kmers + (key_hi(key) >> 52), occ);
@@ -1398,9 +1638,13 @@ __global__ void loads_table_pass(const void* table, uint64_t n_slots, unsigned l
             used = s.key != EMPTY;
             marked = s.pad != 0;
             hi = s.key;
-        } else {
+        } else if constexpr (NW == 2) {
             used = !(s.w0 == EMPTY && s.w1 == EMPTY);
             marked = s.pad[0] != 0;
+            hi = s.w0;
+        } else {
+            used = s.state == SLOT_READY;
+            marked = s.mark != 0;
             hi = s.w0;
         }
         if (!used) continue;
@@ -1424,7 +1668,8 @@ __global__ void fill_region_gaps(void* routed, const unsigned long long* cursor,
     const unsigned long long end = region_end[b];
     for (unsigned long long i = min(min(cursor[b], region_fill[b]), end) + threadIdx.x; i < end; i += blockDim.x) {
         if constexpr (NW == 1) keys[i] = EMPTY;
-        else keys[i] = Key2{EMPTY, EMPTY};
+        else if constexpr (NW == 2) keys[i] = Key2{EMPTY, EMPTY};
+        else keys[i] = Key4{EMPTY, EMPTY, EMPTY, EMPTY};
     }
 }
 
@@ -1439,7 +1684,8 @@ __global__ void fill_set_gaps(void* routed, const uint64_t* set_end_key, const u
     if (s >= n_sets) return;
     for (uint64_t i = set_end_key[s] + threadIdx.x; i < set_next_key[s]; i += blockDim.x) {
         if constexpr (NW == 1) keys[i] = EMPTY;
-        else keys[i] = Key2{EMPTY, EMPTY};
+        else if constexpr (NW == 2) keys[i] = Key2{EMPTY, EMPTY};
+        else keys[i] = Key4{EMPTY, EMPTY, EMPTY, EMPTY};
     }
 }
 

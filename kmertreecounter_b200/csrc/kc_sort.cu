@@ -37,11 +37,17 @@ template <int NW>
 __device__ __forceinline__ uint32_t digit_of(const uint64_t* rec, uint32_t bit) {
     if constexpr (NW == 1) {
         return (uint32_t)(rec[0] >> bit) & 0xFFu;
-    } else {
+    } else if constexpr (NW == 2) {
         // 128-bit key: w0 = rec[0] (high), w1 = rec[1] (low)
         if (bit >= 64) return (uint32_t)(rec[0] >> (bit - 64)) & 0xFFu;
         if (bit + 8 <= 64) return (uint32_t)(rec[1] >> bit) & 0xFFu;
         return (uint32_t)((rec[1] >> bit) | (rec[0] << (64 - bit))) & 0xFFu;
+    } else {
+        // 256-bit key: rec[0] high .. rec[3] low; a digit may straddle two words
+        const uint32_t wi = 3 - (bit >> 6), sh = bit & 63;
+        uint64_t v = rec[wi] >> sh;
+        if (sh > 56 && wi > 0) v |= rec[wi - 1] << (64 - sh);
+        return (uint32_t)v & 0xFFu;
     }
 }
 
@@ -54,6 +60,10 @@ struct Rec<1> {
 template <>
 struct Rec<2> {
     uint64_t w[3];  // key word 0, key word 1, count|pad
+};
+template <>
+struct Rec<4> {
+    uint64_t w[5];  // key words 0..3, count|pad
 };
 
 template <int NW>
@@ -166,6 +176,7 @@ int kc_sort_roots(void* records, uint64_t n, uint64_t record_bytes, uint32_t k, 
     if (n < 2) return KC_OK;
     if (record_bytes == 16 && k <= 32) return sort_impl<1>(records, n, k, w, stream);
     if (record_bytes == 24 && k <= 64) return sort_impl<2>(records, n, k, w, stream);
+    if (record_bytes == 40 && k <= 128) return sort_impl<4>(records, n, k, w, stream);
     g_sort_err = "unsupported record layout";
     return KC_ERR_INVALID;
 }

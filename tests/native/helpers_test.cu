@@ -1,12 +1,14 @@
 // Host-side unit test of the extraction helpers in kc_kernels.cuh
 // (compiled by tests/test_kernel_helpers.py; runs on the CPU).
 //
-// For random base strings and every k in 1..64 and bucket widths 8/12 bits:
+// For random base strings and every k in 1..128 and bucket widths 8/12 bits:
 //   * window_at() returns exactly the last k bases ending at byte j,
 //   * canonical1/canonical2 equal min(F, C) built from the definition in the
 //     reference (src/GetKmer.h:58-82, :181-207): F = bases in reverse order,
 //     C = complemented bases in read order, both left-aligned,
-//   * bucket_of_window() equals the top bits of that canonical key.
+//   * bucket_of_window() equals the top bits of that canonical key (k <= 64),
+//   * for k = 65..128: window_at4() and canonical4() the same way, and
+//     runs_at_least5() marks exactly the bytes that end k consecutive bases.
 #include <cstdio>
 #include <cstdint>
 #include <cstdlib>
@@ -23,6 +25,85 @@ static void pack_left(const std::vector<int>& b, uint64_t out[2]) {
         const int w = (int)(i / 32), pos = 62 - 2 * (int)(i % 32);
         out[w] |= (uint64_t)b[i] << pos;
     }
+}
+
+static void pack_left4(const std::vector<int>& b, uint64_t out[4]) {
+    out[0] = out[1] = out[2] = out[3] = 0;
+    for (size_t i = 0; i < b.size(); ++i) {
+        const int w = (int)(i / 32), pos = 62 - 2 * (int)(i % 32);
+        out[w] |= (uint64_t)b[i] << pos;
+    }
+}
+
+// k = 65..128 over five segments (160 bytes); returns the number of checks
+static long check_long_keys(std::mt19937_64& rng) {
+    long checks = 0;
+    for (int iter = 0; iter < 4000; ++iter) {
+        std::vector<int> bases(160);
+        for (auto& x : bases) x = (int)(rng() & 3);
+        uint64_t seg[5] = {0, 0, 0, 0, 0};
+        for (int s = 0; s < 5; ++s)
+            for (int j = 0; j < 32; ++j) seg[s] |= (uint64_t)bases[32 * s + j] << (62 - 2 * j);
+        const uint32_t j = (uint32_t)(rng() % 32);
+        uint64_t W[4];
+        window_at4(seg[0], seg[1], seg[2], seg[3], seg[4], j, W[0], W[1], W[2], W[3]);
+        for (uint32_t k = 65; k <= 128; ++k) {
+            const int end = 128 + (int)j;
+            std::vector<int> win(bases.begin() + end - k + 1, bases.begin() + end + 1);
+            for (uint32_t i = 0; i < k; ++i) {
+                const uint32_t bit = 2 * (k - 1 - i);
+                if ((int)((W[bit / 64] >> (bit % 64)) & 3) != win[i]) {
+                    std::printf("window4 mismatch k=%u j=%u\n", k, j);
+                    std::exit(1);
+                }
+            }
+            std::vector<int> rf(win.rbegin(), win.rend()), cc(win.size());
+            for (size_t i = 0; i < win.size(); ++i) cc[i] = 3 - win[i];
+            uint64_t F[4], C[4];
+            pack_left4(rf, F);
+            pack_left4(cc, C);
+            int cmp = 0;
+            for (int w = 0; w < 4 && !cmp; ++w) cmp = F[w] < C[w] ? -1 : (F[w] > C[w] ? 1 : 0);
+            const uint64_t* want = cmp <= 0 ? F : C;
+            // bits above the window (from bit 2k up) must not matter
+            uint64_t g2 = W[2], g3 = W[3];
+            const uint32_t kb = 2 * k;
+            if (kb < 192) {
+                g2 |= rng() << (kb - 128);
+                g3 = rng();
+            } else if (kb == 192) {
+                g3 = rng();
+            } else if (kb < 256) {
+                g3 |= rng() << (kb - 192);
+            }
+            const Key4 got = canonical4(W[0], W[1], g2, g3, k);
+            if (got.w0 != want[0] || got.w1 != want[1] || got.w2 != want[2] || got.w3 != want[3]) {
+                std::printf("canonical4 mismatch k=%u\n", k);
+                std::exit(1);
+            }
+            ++checks;
+        }
+        // run mask: random base/non-base bytes
+        uint32_t fl[5];
+        for (auto& f : fl) f = (uint32_t)rng() | (uint32_t)rng() | (uint32_t)rng();  // mostly bases
+        if (iter % 3 == 0) fl[0] = fl[1] = fl[2] = fl[3] = fl[4] = 0xFFFFFFFFu;
+        for (uint32_t k = 65; k <= 128; ++k) {
+            const uint32_t got = runs_at_least5(fl[0], fl[1], fl[2], fl[3], fl[4], k);
+            for (int b = 0; b < 32; ++b) {
+                bool all = true;
+                for (uint32_t q = 0; q < k && all; ++q) {
+                    const int pos = 128 + b - (int)q;
+                    all = (fl[pos / 32] >> (pos % 32)) & 1u;
+                }
+                if (all != (bool)((got >> b) & 1u)) {
+                    std::printf("runs_at_least5 mismatch k=%u byte %d\n", k, b);
+                    std::exit(1);
+                }
+            }
+            ++checks;
+        }
+    }
+    return checks;
 }
 
 int main() {
@@ -85,6 +166,7 @@ int main() {
             ++checks;
         }
     }
+    checks += check_long_keys(rng);
     std::printf("ok %ld\n", checks);
     return 0;
 }

@@ -38,7 +38,7 @@ def test_sizes():
     assert kc.record_dtype(31).itemsize == 16 and kc.record_dtype(63).itemsize == 24
 
 
-@pytest.mark.parametrize("field,value", [("k", 0), ("k", 65), ("canonical", 0), ("n_buckets", 100),
+@pytest.mark.parametrize("field,value", [("k", 0), ("k", 129), ("canonical", 0), ("n_buckets", 100),
                                          ("table_load", 0.99), ("batch_bytes", 1000),
                                          ("device_batch_bytes", 4096)])
 def test_invalid_config_rejected_before_device(field, value):

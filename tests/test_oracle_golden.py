@@ -14,8 +14,8 @@ import pytest
 import inputs
 import oracle
 
-CASES = [(name, k) for name, ks in [("plain_small", [31]), ("plain_small_s7", [21, 32, 33, 63]),
-                                    ("adversarial", [17, 31, 32, 33, 64])] for k in ks]
+CASES = [(name, k) for name, ks in [("plain_small", [31]), ("plain_small_s7", [21, 32, 33, 63, 65, 101, 127, 128]),
+                                    ("adversarial", [17, 31, 32, 33, 64, 65, 100, 128])] for k in ks]
 
 _cache = {}
 
