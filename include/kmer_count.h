@@ -93,6 +93,9 @@ typedef struct kc_stats {
     uint64_t filter_words;    /* 64-bit words of the first-occurrence filter */
     uint64_t overflow_keys;   /* keys routed past their estimated bucket region */
     uint64_t reroutes;        /* batches routed again from an exact histogram */
+    uint64_t max_bucket_filter_words;  /* largest per-bucket filter (the reference's "Max Bloom
+                                        * Filter capacity", src/main.cpp:88-108, in 64-bit words) */
+    uint64_t max_bucket_table_slots;   /* largest per-bucket repeat table */
 } kc_stats;
 
 typedef struct kc_context kc_context;

@@ -55,6 +55,7 @@ class KcStats(C.Structure):
         ("batches", C.c_uint64), ("root_counts", C.c_uint64 * 256), ("device_ms", C.c_double),
         ("wall_ms", C.c_double), ("table_slots", C.c_uint64), ("filter_words", C.c_uint64),
         ("overflow_keys", C.c_uint64), ("reroutes", C.c_uint64),
+        ("max_bucket_filter_words", C.c_uint64), ("max_bucket_table_slots", C.c_uint64),
     ]
 
     def as_dict(self):

@@ -850,7 +850,11 @@ void fill_stats(kc_context* c, kc_stats* s, double dev_ms, double wall_ms) {
     s->device_ms = dev_ms;
     s->wall_ms = wall_ms;
     uint64_t live = 0;
-    for (const auto& m : c->h_meta) live += m.tab_mask + 1;
+    for (const auto& m : c->h_meta) {
+        live += m.tab_mask + 1;
+        s->max_bucket_table_slots = std::max<uint64_t>(s->max_bucket_table_slots, m.tab_mask + 1);
+        s->max_bucket_filter_words = std::max<uint64_t>(s->max_bucket_filter_words, m.bloom_mask + 1);
+    }
     s->table_slots = live;
     s->filter_words = c->bloom_words;
     s->overflow_keys = c->overflow_keys;

@@ -278,6 +278,12 @@ int run(const kc_config* g, const uint8_t* d_fastq, uint64_t n, uint8_t* d_low, 
         stats->rehashes = rehashes;
         stats->batches = 1;
         for (int r = 0; r < 256; ++r) stats->root_counts[r] = h_r[r];
+        for (int b = 0; b < NB; ++b) {
+            stats->table_slots += h_meta[b].tab_mask + 1;
+            stats->max_bucket_table_slots = std::max<uint64_t>(stats->max_bucket_table_slots, h_meta[b].tab_mask + 1);
+            stats->max_bucket_filter_words = std::max<uint64_t>(stats->max_bucket_filter_words, h_meta[b].bloom_mask + 1);
+            stats->filter_words += h_meta[b].bloom_mask + 1;
+        }
     }
     (void)BITS;
     return KC_OK;

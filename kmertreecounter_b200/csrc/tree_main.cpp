@@ -91,6 +91,11 @@ int main(int argc, char* argv[]) {
         std::cerr << kc_last_error() << std::endl;
         return rc == KC_ERR_INVALID ? 1 : 255;
     }
+    // Stage-0 figures of the reference (src/main.cpp:88-108, :186), here
+    // from the exact per-bucket totals instead of a 256 MB sample
+    std::cout << "Average prefix count: " << st.total_kmers / 256 << std::endl;
+    std::cout << "Max Bloom Filter capacity: " << st.max_bucket_filter_words << std::endl;
+    std::cout << "Max repeat table capacity: " << st.max_bucket_table_slots << std::endl;
     std::cout << "Total read k-mer count: " << st.total_kmers << std::endl;
     std::cout << "Low frequency k-mer (low.bin records): " << st.low_records << std::endl;
     std::cout << "Device elapsed ms: " << st.device_ms << std::endl;
