@@ -41,6 +41,10 @@ WORKLOADS = {
     "plain_small": ("plain_small", 31, 256),
     "large_long": ("large_long", 63, 4096),
 }
+# device passes per workload (the 21 GB, k=63 input keeps ~53 GB of packed
+# first occurrences and ~50 GB of tables on the device; 2 GiB passes keep the
+# routed keys at ~9 GB)
+DEVICE_BATCH = {"large_long": 2 << 30}
 
 
 def parse():
@@ -57,6 +61,7 @@ def parse():
     ap.add_argument("--batch-scale", type=float, default=0.05,
                     help="read-set batch comparison: shrink genomes and read counts of the 512 sets")
     ap.add_argument("--no-batched", action="store_true")
+    ap.add_argument("--no-sizing", action="store_true", help="skip the learned-vs-sampled sizing comparison")
     return ap.parse_args()
 
 
@@ -255,7 +260,10 @@ def compare_sizing(args, kc, torch, dev, n, k, buckets):
     hist = {}
     for rule in ("sampled", "learned"):
         mode = kc.KC_SIZING_LEARNED if rule == "learned" else kc.KC_SIZING_SAMPLED
-        with kc.Counter(kc.default_config(k=k, n_buckets=buckets, sizing=mode)) as c:
+        cfg = kc.default_config(k=k, n_buckets=buckets, sizing=mode)
+        if args.workload in DEVICE_BATCH:
+            cfg.device_batch_bytes = DEVICE_BATCH[args.workload]
+        with kc.Counter(cfg) as c:
             def step():
                 if rule == "learned":
                     sizing.predict_device(c, model, dev.data_ptr(), n, k, 150)
@@ -302,6 +310,8 @@ def run_ours(args):
     torch.cuda.synchronize()
 
     cfg = kc.default_config(k=k, n_buckets=buckets, device=local)
+    if args.workload in DEVICE_BATCH:
+        cfg.device_batch_bytes = DEVICE_BATCH[args.workload]
     counter = kc.Counter(cfg)
     stream = torch.cuda.ExternalStream(counter.stream)
 
@@ -340,7 +350,6 @@ def run_ours(args):
         total_ms = float(t.item())
     ms_step = total_ms / args.steps
     _, distinct = counter.histogram(1, 2)  # exact distinct keys (outside the timed region)
-    sizing_cmp = compare_sizing(args, kc, torch, dev, n, k, buckets)
     stats = st.as_dict()
     stats.pop("root_counts", None)
     gpu_launches = int(sum(stage_launch.values()))
@@ -419,10 +428,15 @@ def run_ours(args):
                      "traffic": profile_traffic(args), "per": "step (all count_routed launches of one count)",
                      "dominant_stage": dominant},
         "clocks": clk,
-        "sizing": sizing_cmp,
+        "sizing": None,
     }
+    counter.close()  # its structures go before the sizing comparison builds two more contexts
+    if not args.no_sizing:
+        try:
+            line["sizing"] = compare_sizing(args, kc, torch, dev, n, k, buckets)
+        except kc.KcError as e:
+            line["sizing"] = {"error": str(e)}
     del dev
-    counter.close()
     kc.host_free(host_ptr)
 
     if rank == 0 and not args.no_batched and args.workload == "genome_scale":

@@ -394,7 +394,7 @@ int size_structures(kc_context* c, const std::vector<uint64_t>& kb, double scale
     c->bloom_words = bw;
     c->table_slots_used = ts;
     CK(c->bloom.ensure(bw * sizeof(uint64_t)));
-    CK(c->table.ensure(ts * c->slot_bytes + ts * c->slot_bytes / 2));
+    CK(c->table.ensure(ts * c->slot_bytes + ts * c->slot_bytes / 4));  // room for a few in-place growths
     CK(c->meta.ensure(nb * sizeof(kc::BucketMeta)));
     CKR(put(c, c->meta.p, c->h_meta.data(), nb * sizeof(kc::BucketMeta)));
     {
@@ -683,8 +683,14 @@ int process_batch(kc_context* c, const uint8_t* buf, uint64_t n, int has_halo) {
         low_dst = ring.as<uint8_t>();
         low_base = 0;
     } else {
-        CK(c->low_packed.grow_keep((c->low_total + nlow) * c->packed_bytes + 64, c->low_total * c->packed_bytes,
-                                   c->stream));
+        // first occurrences accumulate over the batches; size the buffer for
+        // the whole input from the share seen so far (+10%), so that it is
+        // reallocated (old and new both live during the copy) about once
+        uint64_t need = (c->low_total + nlow) * c->packed_bytes + 64;
+        if (need > c->low_packed.cap && c->expected_total_bytes > c->input_bytes && c->input_bytes > 0)
+            need = std::max<uint64_t>(need, (uint64_t)((double)need * 1.1 * (double)c->expected_total_bytes /
+                                                       (double)c->input_bytes));
+        CK(c->low_packed.grow_keep(need, c->low_total * c->packed_bytes, c->stream));
         low_dst = c->low_packed.as<uint8_t>();
         low_base = c->low_total;
     }
@@ -1244,6 +1250,9 @@ int kc_count_host_stream(kc_context* c, const uint8_t* fastq, uint64_t n, kc_sin
     const auto t0 = std::chrono::steady_clock::now();
     int rc = begin_run(c, n);
     if (rc) return rc;
+    // a streamed result is never kept on the device: drop the previous
+    // result's packed first occurrences (they can be tens of GB)
+    c->low_packed.release();
     for (int i = 0; i < kc_context::PIN_SLOTS; ++i) {
         if (!c->pin[i]) {
             if (cudaHostAlloc(reinterpret_cast<void**>(&c->pin[i]), kc_context::PIN_BYTES, cudaHostAllocDefault) !=
@@ -1592,7 +1601,7 @@ int count_sets_impl(kc_context* c, const uint8_t* buf, const kc_set_desc* sets, 
     c->bloom_words = bw;
     c->table_slots_used = ts;
     CK(c->bloom.ensure(bw * sizeof(uint64_t)));
-    CK(c->table.ensure(ts * c->slot_bytes + ts * c->slot_bytes / 2));
+    CK(c->table.ensure(ts * c->slot_bytes + ts * c->slot_bytes / 4));  // room for a few in-place growths
     CK(c->meta.ensure(nbk * sizeof(kc::BucketMeta)));
     CK(c->overflow.ensure(nbk * sizeof(uint32_t)));
     const uint64_t nsegs = n_keys / SEG;
