@@ -578,29 +578,31 @@ KC_HD uint32_t bucket_of_window(uint64_t lo, uint64_t hi, uint32_t k, uint32_t B
 // routed[base[bucket] + rank].
 // Keys of one SCATTER tile staged in shared memory (bucket-sorted) before
 // they are written out as contiguous runs; keys beyond this go out directly.
+// (3840 keys for 64-bit keys: an 8 KiB tile of 150 bp FASTQ holds ~3150, and
+// 4 CTAs of the scatter still fit one SM's shared memory)
 template <int NW>
 __host__ __device__ constexpr int stage_keys() {
-    return NW == 1 ? 4096 : (NW == 2 ? 2048 : 1024);
+    return NW == 1 ? 3840 : (NW == 2 ? 2048 : 1024);
 }
 
 // Dynamic shared memory of extract_kernel.
 template <int NW, int MODE>
 __host__ __device__ constexpr size_t extract_smem_bytes(uint32_t n_buckets) {
-    return (size_t)n_buckets * (8 + 4 + 4 + 4) + (MODE == SCATTER ? (size_t)stage_keys<NW>() * (8 * NW + 2) : 0);
+    return (size_t)n_buckets * (8 + 4 + 4 + 4) + (MODE == SCATTER ? (size_t)stage_keys<NW>() * (8 * NW + 2 + 2) : 0);
 }
 
 template <int NW, int MODE>
 __global__ void __launch_bounds__(EXT_THREADS, EXT_MIN_CTAS) extract_kernel(ExtractArgs a) {
     // dynamic smem: u64 base[nb] | u32 hist[nb] | u32 fill[nb] | u32 loff[nb]
-    //               | SCATTER: K keys[stage] | u16 bucket_of_key[stage]
+    //               | SCATTER: K keys[stage] | u16 rank_or_bucket[stage] | u16 order[stage]
     extern __shared__ unsigned long long ext_smem[];
     // segment t of the tile is seg_*[t + HALO_SEGS]; the HALO_SEGS before it
     // hold the halo bytes (zero where there is nothing to read)
     __shared__ uint64_t seg_codes[EXT_THREADS + HALO_SEGS];
     __shared__ uint32_t seg_bases[EXT_THREADS + HALO_SEGS];
     __shared__ uint32_t seg_emit[EXT_THREADS];
+    __shared__ uint32_t seg_first[EXT_THREADS];  // arrival index of the segment's first k-mer
     __shared__ uint32_t warp_sums[EXT_THREADS / 32];
-    __shared__ uint32_t tile_any;
     using K = typename KeyOf<NW>::T;
     constexpr int STAGE = stage_keys<NW>();
     unsigned long long* bbase = ext_smem;
@@ -608,7 +610,8 @@ __global__ void __launch_bounds__(EXT_THREADS, EXT_MIN_CTAS) extract_kernel(Extr
     uint32_t* fill = hist + a.n_buckets;
     uint32_t* loff = fill + a.n_buckets;
     K* skeys = reinterpret_cast<K*>(loff + a.n_buckets + (a.n_buckets & 1));  // 8-byte aligned
-    uint16_t* sbkt = reinterpret_cast<uint16_t*>(skeys + STAGE);
+    uint16_t* sbkt = reinterpret_cast<uint16_t*>(skeys + STAGE);  // two-pass: bucket; one pass: rank
+    uint16_t* sorder = sbkt + STAGE;                               // one pass: arrival index by bucket order
 
     const int tid = threadIdx.x;
     const uint64_t tile = (uint64_t)blockIdx.x * (a.tile_stride > 1 ? a.tile_stride : 1u);
@@ -632,7 +635,6 @@ __global__ void __launch_bounds__(EXT_THREADS, EXT_MIN_CTAS) extract_kernel(Extr
         hist[b] = 0;
         fill[b] = 0;
     }
-    if (tid == 0) tile_any = 0;
 
     // ---- phase A: classify own segment (+ the halo segments)
     uint32_t w[8];
@@ -668,57 +670,128 @@ __global__ void __launch_bounds__(EXT_THREADS, EXT_MIN_CTAS) extract_kernel(Extr
         }
     }
     seg_emit[tid] = emit;
-    if (emit) tile_any = 1;
-    __syncthreads();
-    if (!tile_any) {
+    uint32_t n_tile;  // k-mers of the tile; the scan also publishes seg_emit
+    seg_first[tid] = block_exclusive_scan<EXT_THREADS>(__popc(emit), warp_sums, &n_tile);
+    __syncthreads();  // every segment's seg_first is read by another warp below
+    if (!n_tile) {
         return;  // nothing to count in this tile (HIST adds nothing; SCATTER reserves nothing)
     }
 
     // ---- phase C
     const int lane = tid & 31;
     const int warp = tid >> 5;
+    const uint32_t lt = (1u << lane) - 1u;
+    // canonical key and routing bucket of the window ending at byte `lane` of segment t
+    auto full_key = [&](int t, K& key, uint32_t& bucket) {
+        const uint64_t* sc = seg_codes + t + HALO_SEGS;  // sc[0] = segment t
+        uint64_t lo, hi, w2 = 0, w3 = 0;
+        if constexpr (NW == 4) window_at4(sc[-4], sc[-3], sc[-2], sc[-1], sc[0], (uint32_t)lane, lo, hi, w2, w3);
+        else window_at(sc[-2], sc[-1], sc[0], (uint32_t)lane, lo, hi);
+        if constexpr (NW == 1) {
+            const uint64_t km = k >= 32 ? ~0ull : ((1ull << (2 * k)) - 1ull);
+            key = canonical1(lo & km, k);
+            bucket = (uint32_t)(key >> a.bucket_shift);
+        } else if constexpr (NW == 2) {
+            const uint32_t hb = 2 * k - 64;
+            const uint64_t hmask = hb >= 64 ? ~0ull : ((1ull << hb) - 1ull);
+            key = canonical2(hi & hmask, lo, k);
+            bucket = (uint32_t)(key.w0 >> a.bucket_shift);
+        } else {
+            key = canonical4(lo, hi, w2, w3, k);
+            bucket = (uint32_t)(key.w0 >> a.bucket_shift);
+        }
+    };
+    // reserve each bucket's run in the routed array (bbase) and the local
+    // offsets of the bucket-sorted staging area (loff), from hist
+    auto reserve = [&]() {
+        const uint32_t per = (a.n_buckets + EXT_THREADS - 1) / EXT_THREADS;
+        uint32_t sum = 0;
+        for (uint32_t q = 0; q < per; ++q) {
+            const uint32_t b = tid * per + q;
+            if (b < a.n_buckets) {
+                const uint32_t c = hist[b];
+                unsigned long long base = c ? atomicAdd(a.bucket_cursor + bucket_off + b, (unsigned long long)c) : 0ull;
+                if (a.region_end && c && base + c > a.region_end[b]) {
+                    // the run does not fit the region: it goes whole to the
+                    // overflow area.  If that is full too, the batch is routed
+                    // again (error bit 1) and the run lands, in bounds, at the
+                    // overflow area's start (at least 65536 keys >= one run).
+                    atomicMin(a.region_fill + b, base);
+                    const unsigned long long ob = atomicAdd(a.overflow_cursor, (unsigned long long)c);
+                    if (ob + c <= a.overflow_end) {
+                        base = ob;
+                    } else {
+                        base = a.overflow_start;
+                        atomicOr(a.error, 2u);
+                    }
+                }
+                bbase[b] = base;
+                sum += c;
+            }
+        }
+        uint32_t run = block_exclusive_scan<EXT_THREADS>(sum, warp_sums, nullptr);
+        for (uint32_t q = 0; q < per; ++q) {
+            const uint32_t b = tid * per + q;
+            if (b < a.n_buckets) {
+                loff[b] = run;
+                run += hist[b];
+            }
+        }
+        __syncthreads();
+    };
+
+    if (MODE == SCATTER && n_tile <= (uint32_t)STAGE) {
+        // One extraction pass: the bucket's shared-memory counter gives each
+        // key its rank in the bucket and builds the tile histogram at once;
+        // keys are staged in arrival order, then indexed in bucket order and
+        // written out as contiguous runs.
+#pragma unroll 1
+        for (int r = 0; r < EXT_BPT; ++r) {
+            const int t = r * (EXT_THREADS / 32) + warp;
+            const uint32_t em = seg_emit[t];
+            if (!em) continue;  // warp-uniform
+            if (!((em >> lane) & 1u)) continue;
+            K key;
+            uint32_t bucket;
+            full_key(t, key, bucket);
+            const uint32_t arr = seg_first[t] + __popc(em & lt);
+            if (arr >= n_tile) {  // cannot happen; reported, never written
+                atomicOr(a.error, 1u);
+                continue;
+            }
+            const uint32_t rnk = atomicAdd(hist + bucket, 1u);
+            skeys[arr] = key;
+            sbkt[arr] = (uint16_t)rnk;
+        }
+        __syncthreads();
+        reserve();
+        for (uint32_t i = tid; i < n_tile; i += EXT_THREADS) {
+            const uint32_t b = (uint32_t)(key_hi(skeys[i]) >> a.bucket_shift);
+            const uint32_t pos = loff[b] + sbkt[i];
+            if (sbkt[i] < hist[b] && pos < n_tile) sorder[pos] = (uint16_t)i;
+            else atomicOr(a.error, 1u);
+        }
+        __syncthreads();
+        K* out = reinterpret_cast<K*>(a.routed);
+        for (uint32_t p = tid; p < n_tile; p += EXT_THREADS) {
+            const uint32_t i = sorder[p];
+            if (i >= n_tile) {
+                atomicOr(a.error, 1u);
+                continue;
+            }
+            const K key = skeys[i];
+            const uint32_t b = (uint32_t)(key_hi(key) >> a.bucket_shift);
+            if (p - loff[b] < hist[b]) out[bbase[b] + (p - loff[b])] = key;  // inside the bucket's reservation
+            else atomicOr(a.error, 1u);
+        }
+        return;
+    }
+
+    // Two passes (histogram, then keys; and the HIST kernel's only pass):
+    // tiles with more k-mers than the staging area holds
 #pragma unroll 1
     for (int pass = 0; pass < (MODE == SCATTER ? 2 : 1); ++pass) {
-        if (pass == 1) {
-            // reserve each bucket's run in the routed array; local offsets of
-            // the bucket-sorted staging area (per-thread chunk of buckets +
-            // block scan)
-            const uint32_t per = (a.n_buckets + EXT_THREADS - 1) / EXT_THREADS;
-            uint32_t sum = 0;
-            for (uint32_t q = 0; q < per; ++q) {
-                const uint32_t b = tid * per + q;
-                if (b < a.n_buckets) {
-                    const uint32_t c = hist[b];
-                    unsigned long long base =
-                        c ? atomicAdd(a.bucket_cursor + bucket_off + b, (unsigned long long)c) : 0ull;
-                    if (a.region_end && c && base + c > a.region_end[b]) {
-                        // the run does not fit the region: it goes whole to the
-                        // overflow area.  If that is full too, the batch is routed
-                        // again (error bit 1) and the run lands, in bounds, at the
-                        // overflow area's start (at least 65536 keys >= one run).
-                        atomicMin(a.region_fill + b, base);
-                        const unsigned long long ob = atomicAdd(a.overflow_cursor, (unsigned long long)c);
-                        if (ob + c <= a.overflow_end) {
-                            base = ob;
-                        } else {
-                            base = a.overflow_start;
-                            atomicOr(a.error, 2u);
-                        }
-                    }
-                    bbase[b] = base;
-                    sum += c;
-                }
-            }
-            uint32_t run = block_exclusive_scan<EXT_THREADS>(sum, warp_sums, nullptr);
-            for (uint32_t q = 0; q < per; ++q) {
-                const uint32_t b = tid * per + q;
-                if (b < a.n_buckets) {
-                    loff[b] = run;
-                    run += hist[b];
-                }
-            }
-            __syncthreads();
-        }
+        if (pass == 1) reserve();
 #pragma unroll 1
         for (int r = 0; r < EXT_BPT; ++r) {
             const int t = r * (EXT_THREADS / 32) + warp;  // segment owned by this warp this round
@@ -743,21 +816,9 @@ __global__ void __launch_bounds__(EXT_THREADS, EXT_MIN_CTAS) extract_kernel(Extr
                 }
                 atomicAdd(hist + bucket_of_window(lo, hi, k, B), 1u);
             } else {
-                typename KeyOf<NW>::T key;
+                K key;
                 uint32_t bucket;
-                if constexpr (NW == 1) {
-                    const uint64_t km = k >= 32 ? ~0ull : ((1ull << (2 * k)) - 1ull);
-                    key = canonical1(lo & km, k);
-                    bucket = (uint32_t)(key >> a.bucket_shift);
-                } else if constexpr (NW == 2) {
-                    const uint32_t hb = 2 * k - 64;
-                    const uint64_t hmask = hb >= 64 ? ~0ull : ((1ull << hb) - 1ull);
-                    key = canonical2(hi & hmask, lo, k);
-                    bucket = (uint32_t)(key.w0 >> a.bucket_shift);
-                } else {
-                    key = canonical4(lo, hi, w2, w3, k);
-                    bucket = (uint32_t)(key.w0 >> a.bucket_shift);
-                }
+                full_key(t, key, bucket);
                 const uint32_t rnk = atomicAdd(fill + bucket, 1u);
                 if (rnk < hist[bucket]) {
                     const uint32_t sidx = loff[bucket] + rnk;
