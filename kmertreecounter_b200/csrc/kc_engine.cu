@@ -384,14 +384,24 @@ int size_structures(kc_context* c, const std::vector<uint64_t>& kb, double scale
             words = pow2_at_least(std::max<uint64_t>((uint64_t)(kest * g.bloom_bits / 64.0), 256));
             slots = pow2_at_least(std::max<uint64_t>((uint64_t)(kest * g.repeat_ratio / g.table_load), 256));
         }
-        c->h_meta[b].bloom_off = bw;
-        c->h_meta[b].bloom_mask = words - 1;
+        if (c->nw == 1) {
+            // 64-bit keys: the filter is the 32-bit pad field of the table
+            // cells, at the index of the first table probe, so one read serves
+            // both; cells = the larger of the table's slots and the filter's
+            // 32-bit words.  After a table grows, the old cells stay the filter.
+            slots = std::max<uint64_t>(slots, 2 * words);
+            c->h_meta[b].bloom_off = ts;
+            c->h_meta[b].bloom_mask = slots - 1;
+        } else {
+            c->h_meta[b].bloom_off = bw;
+            c->h_meta[b].bloom_mask = words - 1;
+            bw += words;
+        }
         c->h_meta[b].tab_off = ts;
         c->h_meta[b].tab_mask = slots - 1;
-        bw += words;
         ts += slots;
     }
-    c->bloom_words = bw;
+    c->bloom_words = c->nw == 1 ? ts / 2 : bw;  // in 64-bit words (cells hold 32 filter bits each)
     c->table_slots_used = ts;
     CK(c->bloom.ensure(bw * sizeof(uint64_t)));
     CK(c->table.ensure(ts * c->slot_bytes + ts * c->slot_bytes / 4));  // room for a few in-place growths
@@ -432,6 +442,7 @@ void launch_count(kc_context* c, uint64_t n_keys, int use_filter) {
     a.bucket_shift = c->bucket_shift;
     a.n_buckets = c->n_buckets;
     a.use_filter = use_filter;
+    a.filter_in_table = c->nw == 1;
     Stage st(c, use_filter ? KC_STAGE_COUNT_ROUTED : KC_STAGE_REHASH);
     kc::count_routed<NW><<<tiles, kc::CNT_THREADS, 0, c->stream>>>(a);
 }
@@ -859,7 +870,8 @@ void fill_stats(kc_context* c, kc_stats* s, double dev_ms, double wall_ms) {
     for (const auto& m : c->h_meta) {
         live += m.tab_mask + 1;
         s->max_bucket_table_slots = std::max<uint64_t>(s->max_bucket_table_slots, m.tab_mask + 1);
-        s->max_bucket_filter_words = std::max<uint64_t>(s->max_bucket_filter_words, m.bloom_mask + 1);
+        s->max_bucket_filter_words =
+            std::max<uint64_t>(s->max_bucket_filter_words, c->nw == 1 ? (m.bloom_mask + 1) / 2 : m.bloom_mask + 1);
     }
     s->table_slots = live;
     s->filter_words = c->bloom_words;

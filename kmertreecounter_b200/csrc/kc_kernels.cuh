@@ -869,6 +869,11 @@ __device__ __forceinline__ uint64_t bloom_bits(uint64_t h) {
     // partition depends on this choice, never the merged counts.
     return (1ull << ((h >> 40) & 63)) | (1ull << ((h >> 46) & 63)) | (1ull << ((h >> 52) & 63));
 }
+// Three bit positions in a 32-bit filter word kept in a table cell (64-bit
+// keys); hash bits 0..14, while the cell index uses bits 17 and up.
+__device__ __forceinline__ uint32_t bloom_bits32(uint64_t h) {
+    return (1u << (h & 31)) | (1u << ((h >> 5) & 31)) | (1u << ((h >> 10) & 31));
+}
 
 // Insert `add` occurrences of key into a bucket table starting at slot
 // (h >> 17) & mask; false = probe limit hit.  Linear probing; a slot goes
@@ -1035,6 +1040,9 @@ struct CountArgs {
     uint32_t bucket_shift;
     uint32_t n_buckets;
     int use_filter;               // 0: retry pass (table only, no filter)
+    // 64-bit keys: the filter words are the pad fields of table cells
+    // (bloom_off / bloom_mask count cells of the table arena)
+    uint32_t filter_in_table;
     // multi-set batch: set s owns segments [set_seg_start[s], set_seg_start[s+1])
     // and buckets [s * set_buckets, (s + 1) * set_buckets); EMPTY keys are gaps
     const uint64_t* set_seg_start;
@@ -1186,11 +1194,26 @@ __global__ void __launch_bounds__(CNT_THREADS, 4) count_routed(CountArgs a) {
             if (mult[j]) {
                 h[j] = hash_key(it[j]);
                 const MetaS m = meta_of(set_bucket0 + (uint32_t)(key_hi(it[j]) >> a.bucket_shift));
-                if (a.use_filter) old[j] = __ldcg(a.bloom + m.bloom_off + (h[j] & m.bloom_mask));
                 const S* slot = table + m.tab_off + ((h[j] >> 17) & m.tab_mask);
-                if constexpr (NW == 1) seen[j] = __ldcg(&slot->key);
-                else if constexpr (NW == 2) seen[j] = __ldcg(reinterpret_cast<const ulonglong2*>(slot));
-                else seen[j] = 0;
+                if constexpr (NW == 1) {
+                    if (a.filter_in_table) {
+                        // the filter word is the cell's pad field, at the index
+                        // of the first table probe: one 16-byte read gives key,
+                        // count and filter bits unless the bucket's table has
+                        // moved to a grown region (then the cells are filter only)
+                        const ulonglong2 cv = __ldcg(reinterpret_cast<const ulonglong2*>(
+                            table + m.bloom_off + ((h[j] >> 17) & m.bloom_mask)));
+                        old[j] = cv.y >> 32;
+                        seen[j] = m.bloom_off == m.tab_off ? cv.x : __ldcg(&slot->key);
+                    } else {
+                        if (a.use_filter) old[j] = __ldcg(a.bloom + m.bloom_off + (h[j] & m.bloom_mask));
+                        seen[j] = __ldcg(&slot->key);
+                    }
+                } else {
+                    if (a.use_filter) old[j] = __ldcg(a.bloom + m.bloom_off + (h[j] & m.bloom_mask));
+                    if constexpr (NW == 2) seen[j] = __ldcg(reinterpret_cast<const ulonglong2*>(slot));
+                    else seen[j] = 0;
+                }
             }
         }
         uint32_t first_bits = 0;  // bit j: item j is a first occurrence
@@ -1198,11 +1221,22 @@ __global__ void __launch_bounds__(CNT_THREADS, 4) count_routed(CountArgs a) {
 #pragma unroll
             for (int j = 0; j < ITEMS; ++j) {
                 if (mult[j]) {
-                    const uint64_t bits = bloom_bits(h[j]);
+                    bool in_table = false;
+                    if constexpr (NW == 1) in_table = a.filter_in_table != 0;
+                    const uint64_t bits = in_table ? (uint64_t)bloom_bits32(h[j]) : bloom_bits(h[j]);
                     if ((old[j] & bits) != bits) {
                         const MetaS m = meta_of(set_bucket0 + (uint32_t)(key_hi(it[j]) >> a.bucket_shift));
-                        const uint64_t o = atomicOr(
-                            reinterpret_cast<unsigned long long*>(a.bloom + m.bloom_off + (h[j] & m.bloom_mask)), bits);
+                        uint64_t o;
+                        if constexpr (NW == 1) {
+                            if (in_table)
+                                o = atomicOr(&(table + m.bloom_off + ((h[j] >> 17) & m.bloom_mask))->pad, (uint32_t)bits);
+                            else
+                                o = atomicOr(reinterpret_cast<unsigned long long*>(a.bloom + m.bloom_off +
+                                                                                   (h[j] & m.bloom_mask)), bits);
+                        } else {
+                            o = atomicOr(reinterpret_cast<unsigned long long*>(a.bloom + m.bloom_off + (h[j] & m.bloom_mask)),
+                                         bits);
+                        }
                         if ((o & bits) != bits) first_bits |= 1u << j;
                     }
                 }
