@@ -166,6 +166,7 @@ struct kc_context {
     DevBuf bloom, table;
     DevBuf low_packed;
     DevBuf roots, chunks, chunk_pass, chunk_off, root_count;
+    uint64_t n_chunks = 0;  // entries of `chunks` (live table regions) of the last export
     DevBuf sort_tmp, sort_hist, sort_offs, sort_sums;
     DevBuf set_tiles, tile_prefix, set_info;  // multi-set batches
 
@@ -727,6 +728,7 @@ template <int NW>
 int run_export(kc_context* c, const std::vector<kc::ExportChunk>& ch, uint64_t n_groups,
                std::vector<uint64_t>& totals) {
     const uint64_t nch = ch.size();
+    c->n_chunks = nch;
     CK(c->chunks.ensure(std::max<uint64_t>(nch, 1) * sizeof(kc::ExportChunk)));
     CK(c->chunk_pass.ensure(std::max<uint64_t>(nch, 1) * sizeof(uint32_t)));
     CK(c->chunk_off.ensure(std::max<uint64_t>(nch, 1) * sizeof(uint64_t)));
@@ -1338,12 +1340,10 @@ void histogram_kernels(kc_context* c, uint32_t min_freq, uint32_t max_freq, unsi
     kc::hist_low_pass<NW><<<grid, 256, 0, c->stream>>>(c->low_packed.as<uint8_t>(), c->low_total, c->cfg.k,
                                                        c->meta.as<kc::BucketMeta>(), c->bucket_shift, c->table.p,
                                                        min_freq, max_freq, d);
-    for (uint32_t b = 0; b < c->n_buckets; ++b) {
-        const uint64_t n = c->h_meta[b].tab_mask + 1;
-        uint8_t* t = c->table.as<uint8_t>() + c->h_meta[b].tab_off * c->slot_bytes;
-        const int g = (int)std::min<uint64_t>(grid, ceil_div(n, 256));
-        kc::hist_table_pass<NW><<<g, 256, 0, c->stream>>>(t, n, min_freq, max_freq, d, d + bins);
-    }
+    // the export's chunk list covers exactly the live bucket tables
+    if (c->n_chunks)
+        kc::hist_table_pass<NW><<<std::min<uint64_t>(c->n_chunks, (uint64_t)grid), 256, 0, c->stream>>>(
+            c->table.p, c->chunks.as<kc::ExportChunk>(), c->n_chunks, min_freq, max_freq, d, d + bins);
 }
 
 // Per model bucket loads: dd[0..4096) distinct, [4096..8192) table keys,
@@ -1355,12 +1355,10 @@ void loads_kernels(kc_context* c, unsigned long long* dd) {
     kc::loads_low_pass<NW><<<grid, 256, 0, c->stream>>>(c->low_packed.as<uint8_t>(), c->low_total, c->cfg.k,
                                                         c->meta.as<kc::BucketMeta>(), c->bucket_shift, c->table.p, dd,
                                                         dd + 2 * KC_MODEL_BUCKETS);
-    for (uint32_t b = 0; b < c->n_buckets; ++b) {
-        const uint64_t n = c->h_meta[b].tab_mask + 1;
-        uint8_t* t = c->table.as<uint8_t>() + c->h_meta[b].tab_off * c->slot_bytes;
-        const int g = (int)std::min<uint64_t>(grid, ceil_div(n, 256));
-        kc::loads_table_pass<NW><<<g, 256, 0, c->stream>>>(t, n, dd, dd + KC_MODEL_BUCKETS, dd + 2 * KC_MODEL_BUCKETS);
-    }
+    if (c->n_chunks)
+        kc::loads_table_pass<NW><<<std::min<uint64_t>(c->n_chunks, (uint64_t)grid), 256, 0, c->stream>>>(
+            c->table.p, c->chunks.as<kc::ExportChunk>(), c->n_chunks, dd, dd + KC_MODEL_BUCKETS,
+            dd + 2 * KC_MODEL_BUCKETS);
 }
 
 }  // namespace

@@ -1563,6 +1563,29 @@ __global__ void __launch_bounds__(EXP_THREADS) export_write(const void* table, c
 
 constexpr int HIST_SMEM = 1024;
 
+// Key of low.bin record r (layout of src/ExportWriter.h:522-550, read back as
+// tool/ExportReader.h:355-391 does).  Records of a multiple of 8 bytes
+// (k = 29..32, 61..64, 93..96, 125..128) are read as aligned words.
+template <int NW>
+__device__ __forceinline__ typename KeyOf<NW>::T unpack_low(const uint8_t* low, uint64_t r, uint32_t P, uint32_t full,
+                                                            uint32_t tail_bytes) {
+    const uint8_t* p = low + r * P;
+    uint64_t w[4] = {0, 0, 0, 0};
+    if ((P & 7u) == 0) {
+        const uint64_t* q = reinterpret_cast<const uint64_t*>(p);
+        for (uint32_t f = 0; f < P / 8 && f < (uint32_t)NW; ++f) w[f] = q[f];
+    } else {
+        for (uint32_t f = 0; f < full; ++f)
+            for (uint32_t b = 0; b < 8; ++b) w[f] |= (uint64_t)p[8 * f + b] << (8 * b);
+        for (uint32_t b = 0; b < tail_bytes; ++b) w[full] |= (uint64_t)p[8 * full + b] << (8 * (8 - tail_bytes + b));
+    }
+    typename KeyOf<NW>::T key;
+    if constexpr (NW == 1) key = w[0];
+    else if constexpr (NW == 2) key = Key2{w[0], w[1]};
+    else key = Key4{w[0], w[1], w[2], w[3]};
+    return key;
+}
+
 template <int NW>
 __device__ __forceinline__ bool table_find(const typename SlotOf<NW>::T* tab, uint64_t mask, uint64_t h,
                                            const typename KeyOf<NW>::T& key, uint64_t* where) {
@@ -1621,15 +1644,7 @@ __global__ void hist_low_pass(const uint8_t* low, uint64_t n_low, uint32_t k, co
     const uint32_t full = k / 32, tail_bits = 2 * (k % 32), tail_bytes = (tail_bits + 7) / 8;
     const uint32_t P = full * 8 + tail_bytes;
     for (uint64_t r = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; r < n_low; r += (uint64_t)gridDim.x * blockDim.x) {
-        const uint8_t* p = low + r * P;
-        uint64_t w[4] = {0, 0, 0, 0};
-        for (uint32_t f = 0; f < full; ++f)
-            for (uint32_t b = 0; b < 8; ++b) w[f] |= (uint64_t)p[8 * f + b] << (8 * b);
-        for (uint32_t b = 0; b < tail_bytes; ++b) w[full] |= (uint64_t)p[8 * full + b] << (8 * (8 - tail_bytes + b));
-        K key;
-        if constexpr (NW == 1) key = w[0];
-        else if constexpr (NW == 2) key = Key2{w[0], w[1]};
-        else key = Key4{w[0], w[1], w[2], w[3]};
+        const K key = unpack_low<NW>(low, r, P, full, tail_bytes);
         const BucketMeta m = meta[key_hi(key) >> bucket_shift];
         S* tab = reinterpret_cast<S*>(table) + m.tab_off;
         uint64_t at;
@@ -1648,18 +1663,18 @@ __global__ void hist_low_pass(const uint8_t* low, uint64_t n_low, uint32_t k, co
 }
 
 template <int NW>
-__global__ void hist_table_pass(const void* table, uint64_t n_slots, uint32_t lo, uint32_t hi, unsigned long long* gh,
-                                unsigned long long* unmarked) {
+__global__ void hist_table_pass(const void* table, const ExportChunk* chunks, uint64_t n_chunks, uint32_t lo, uint32_t hi,
+                                unsigned long long* gh, unsigned long long* unmarked) {
     using S = typename SlotOf<NW>::T;
     __shared__ uint32_t sh[HIST_SMEM];
     __shared__ unsigned long long s_un;
     for (int i = threadIdx.x; i < HIST_SMEM; i += blockDim.x) sh[i] = 0;
     if (threadIdx.x == 0) s_un = 0;
     __syncthreads();
-    const S* t = reinterpret_cast<const S*>(table);
     uint32_t un = 0;
-    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n_slots; i += (uint64_t)gridDim.x * blockDim.x) {
-        const S s = t[i];
+    for (uint64_t c = blockIdx.x; c < n_chunks; c += gridDim.x)
+    for (uint32_t q = threadIdx.x; q < chunks[c].n_slots; q += blockDim.x) {
+        const S s = reinterpret_cast<const S*>(table)[chunks[c].slot_begin + q];
         bool used, marked;
         if constexpr (NW == 1) {
             used = s.key != EMPTY;
@@ -1696,15 +1711,7 @@ __global__ void loads_low_pass(const uint8_t* low, uint64_t n_low, uint32_t k, c
     const uint32_t full = k / 32, tail_bits = 2 * (k % 32), tail_bytes = (tail_bits + 7) / 8;
     const uint32_t P = full * 8 + tail_bytes;
     for (uint64_t r = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; r < n_low; r += (uint64_t)gridDim.x * blockDim.x) {
-        const uint8_t* p = low + r * P;
-        uint64_t w[4] = {0, 0, 0, 0};
-        for (uint32_t f = 0; f < full; ++f)
-            for (uint32_t b = 0; b < 8; ++b) w[f] |= (uint64_t)p[8 * f + b] << (8 * b);
-        for (uint32_t b = 0; b < tail_bytes; ++b) w[full] |= (uint64_t)p[8 * full + b] << (8 * (8 - tail_bytes + b));
-        K key;
-        if constexpr (NW == 1) key = w[0];
-        else if constexpr (NW == 2) key = Key2{w[0], w[1]};
-        else key = Key4{w[0], w[1], w[2], w[3]};
+        const K key = unpack_low<NW>(low, r, P, full, tail_bytes);
         const BucketMeta m = meta[key_hi(key) >> bucket_shift];
         S* tab = reinterpret_cast<S*>(table) + m.tab_off;
         uint64_t at;
@@ -1721,12 +1728,12 @@ __global__ void loads_low_pass(const uint8_t* low, uint64_t n_low, uint32_t k, c
 }
 
 template <int NW>
-__global__ void loads_table_pass(const void* table, uint64_t n_slots, unsigned long long* distinct,
-                                 unsigned long long* tkeys, unsigned long long* kmers) {
+__global__ void loads_table_pass(const void* table, const ExportChunk* chunks, uint64_t n_chunks,
+                                 unsigned long long* distinct, unsigned long long* tkeys, unsigned long long* kmers) {
     using S = typename SlotOf<NW>::T;
-    const S* t = reinterpret_cast<const S*>(table);
-    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n_slots; i += (uint64_t)gridDim.x * blockDim.x) {
-        const S s = t[i];
+    for (uint64_t c = blockIdx.x; c < n_chunks; c += gridDim.x)
+    for (uint32_t q = threadIdx.x; q < chunks[c].n_slots; q += blockDim.x) {
+        const S s = reinterpret_cast<const S*>(table)[chunks[c].slot_begin + q];
         uint64_t hi;
         bool used, marked;
         if constexpr (NW == 1) {
