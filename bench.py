@@ -387,8 +387,8 @@ def run_ours(args):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_step = float(t.item())
 
-    # --- roofline of the dominant kernel (count_routed), SURVEY 8(d) units:
-    # 64 B per k-mer (one 32 B filter sector read + write) and 64 B per
+    # --- roofline of the dominant kernel (count_routed), in the fixed units of
+    # the workload definition: 64 B per k-mer (one 32 B filter sector read + write) and 64 B per
     # repeat occurrence (one table sector read + write).
     from measured import peaks
     pk = peaks()

@@ -26,7 +26,8 @@ extern "C" {
 /* Per model bucket of the last device-held count (kc_count_host /
  * kc_count_device): distinct keys, keys held by the repeat tables (the table
  * load) and k-mer occurrences.  The exact loads the model is trained on and
- * judged by; on a 1% read prefix, `kmers` is the model's input histogram.
+ * whose error it is measured against; on a 1% read prefix, `kmers` is the
+ * model's input histogram.
  * Any pointer may be NULL. */
 int kc_bucket_loads(kc_context* ctx, uint64_t* distinct, uint64_t* table_keys, uint64_t* kmers);
 
