@@ -50,13 +50,14 @@ DEVICE_BATCH = {"large_long": 2 << 30}
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="genome_scale", choices=sorted(WORKLOADS))
     ap.add_argument("--scale", type=float, default=1.0, help="shrink genome and reads together")
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-peaks", action="store_true", help="skip the atomic/link microbenchmark")
     ap.add_argument("--sample-scale", type=float, default=0.05, help="CPU sample size, fraction of the workload")
     ap.add_argument("--batch-scale", type=float, default=0.05,
                     help="read-set batch comparison: shrink genomes and read counts of the 512 sets")
@@ -80,21 +81,31 @@ class ClockSampler:
     def __init__(self, index):
         self.index = index
         self.proc = None
-        self.lines = []
+        self.lines = []  # (arrival time, csv line)
+        self.window = (0.0, float("inf"))
 
     def start(self):
+        """Start polling (every 100 ms) and wait for the first sample, so that
+        the timed region that follows is covered from its start."""
         try:
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
+            t_end = time.perf_counter() + 10.0
+            while not self.lines and time.perf_counter() < t_end and self.proc.poll() is None:
+                time.sleep(0.01)
         except Exception:
             self.proc = None
 
     def _read(self):
         for line in self.proc.stdout:
-            self.lines.append(line.strip())
+            self.lines.append((time.perf_counter(), line.strip()))
+
+    def mark(self, t0, t1):
+        """Keep only samples taken between t0 and t1 (perf_counter seconds)."""
+        self.window = (t0, t1)
 
     def stop(self):
         if not self.proc:
@@ -106,7 +117,10 @@ class ClockSampler:
             self.proc.kill()
         sm, mx, reasons = [], None, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
+        t0, t1 = self.window
+        for ts, ln in self.lines:
+            if not (t0 <= ts <= t1):
+                continue
             f = [x.strip() for x in ln.split(",")]
             if len(f) < 9:
                 continue
@@ -189,6 +203,54 @@ def profile_traffic(args):
     except OSError:
         pass
     return None
+
+
+def pipeline_roofline(dev_peaks, pk, F, K, L, R, P, rec, ms_step, count_ms):
+    """The workload's fixed roofline: t_roof = max(bytes_alg / HBM, atomics /
+    atomic rate[, F / H2D for the host path]), with
+    bytes_alg = F + 64 K + 64 (K - L) + L P + R rec (FASTQ read once, one
+    filter sector read + write per k-mer and one table sector read + write per
+    repeat occurrence, low.bin and root records written once) and one filter
+    atomicOr (old value used) per k-mer plus one count atomicAdd (reduction)
+    per repeat occurrence, each at its own measured rate.
+
+    Two atomic rates are measured: on a 4 GiB random footprint (every atomic
+    misses L2) and on a 32 MiB footprint (L2-resident).  Routing keys into
+    buckets before counting keeps one bucket's filter and table words in L2
+    while its keys are counted, so the L2-resident rate is the ceiling this
+    design runs against; `frac` uses it, `frac_random_4gib` the 4 GiB rate."""
+    if not dev_peaks:
+        return {}
+    hbm = pk["hbm_gbs"] * 1e9
+
+    def t_atom(or_rate, add_rate):
+        return K / (or_rate * 1e9) + (K - L) / (add_rate * 1e9)
+
+    t_dram_atom = t_atom(dev_peaks["or_return_gops"], dev_peaks["red_add_gops"])
+    t_l2_atom = t_atom(dev_peaks["l2_or_return_gops"], dev_peaks["l2_red_add_gops"])
+    bytes_alg = F + 64 * K + 64 * (K - L) + L * P + R * rec
+    t_hbm = bytes_alg / hbm
+    t_roof = max(t_hbm, t_l2_atom)
+    t_link = F / (dev_peaks["h2d_gbs"] * 1e9)
+    out = {"pipeline": {
+        "bytes_alg": bytes_alg, "atomics_alg": 2 * K - L, "t_hbm_ms": t_hbm * 1e3,
+        "t_atomic_l2_ms": t_l2_atom * 1e3, "t_atomic_random_4gib_ms": t_dram_atom * 1e3,
+        "t_h2d_ms": t_link * 1e3, "t_roof_ms": t_roof * 1e3, "t_roof_e2e_ms": max(t_roof, t_link) * 1e3,
+        "bound": "hbm" if t_hbm >= t_l2_atom else "atomic", "frac": t_roof * 1e3 / ms_step,
+        "frac_random_4gib": max(t_hbm, t_dram_atom) * 1e3 / ms_step,
+        "peaks": {"hbm_gbs": pk["hbm_gbs"], "hbm_source": pk["source"],
+                  "hbm_copy_gbs_this_gpu": dev_peaks["hbm_copy_gbs"],
+                  "or_return_gops": dev_peaks["or_return_gops"], "red_add_gops": dev_peaks["red_add_gops"],
+                  "l2_or_return_gops": dev_peaks["l2_or_return_gops"],
+                  "l2_red_add_gops": dev_peaks["l2_red_add_gops"], "h2d_gbs": dev_peaks["h2d_gbs"],
+                  "atomic_footprint_bytes": dev_peaks["footprint_bytes"],
+                  "l2_footprint_bytes": dev_peaks["l2_footprint_bytes"], "source": "kc_measure_peaks on this GPU"}}}
+    if count_ms > 0:
+        out["count_routed_atomic"] = {"atomics_alg_per_step": 2 * K - L, "t_atomic_l2_ms": t_l2_atom * 1e3,
+                                      "frac": t_l2_atom * 1e3 / count_ms,
+                                      "t_atomic_random_4gib_ms": t_dram_atom * 1e3,
+                                      "frac_random_4gib": t_dram_atom * 1e3 / count_ms}
+    return out
 
 
 def compare_batched(args, kc, torch):
@@ -298,6 +360,11 @@ def run_ours(args):
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
 
+    # roofline denominators of the atomic and link terms, measured on this
+    # GPU before the workload is resident (random u32 atomics on a 4 GiB
+    # footprint, pinned H2D); the HBM term uses the pool's measured copy
+    dev_peaks = None if args.no_peaks else kc.measure_peaks(local, 4 << 30)
+
     p, k, buckets, bases = make_workload(args.workload, args.scale)
     g = synth.genome(p)
     n = synth.fastq_bytes(p)
@@ -328,9 +395,10 @@ def run_ours(args):
     counter.set_profiling(True)
     stage_ms, stage_launch = {}, {}
     clocks = ClockSampler(local)
+    clocks.start()
     barrier()
     torch.cuda.synchronize()
-    clocks.start()
+    t_clk0 = time.perf_counter()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(stream)
     for _ in range(args.steps):
@@ -340,6 +408,7 @@ def run_ours(args):
             stage_launch[name] = stage_launch.get(name, 0) + ln
     e1.record(stream)
     torch.cuda.synchronize()
+    clocks.mark(t_clk0, time.perf_counter())
     barrier()
     clk = clocks.stop()
     total_ms = e0.elapsed_time(e1)
@@ -397,6 +466,8 @@ def run_ours(args):
     count_ms = stage_ms.get("count", 0.0) / args.steps
     achieved = alg_bytes / (count_ms / 1e3) / 1e9 if count_ms > 0 else None
     dominant = max(stage_ms, key=lambda s: stage_ms[s]) if stage_ms else None
+    roof = pipeline_roofline(dev_peaks, pk, n, K, L, stats["root_records"], kc.packed_bytes(k), kc.record_bytes(k),
+                             ms_step, count_ms)
 
     line = {
         "metric": "FASTQ Gbases/s to exact k-mer counts on 1 B200",
@@ -421,12 +492,14 @@ def run_ours(args):
         "stages_ms_per_step": {s: v / args.steps for s, v in stage_ms.items()},
         "gpu_launches": gpu_launches,
         "e2e": {"value": bases * world / (e2e_step / 1e3) / 1e9, "unit": "Gbases/s", "ms_per_step": e2e_step,
-                "h2d_bytes_per_step": n, "d2h_bytes_per_step": lb + nr * rec},
+                "h2d_bytes_per_step": n, "d2h_bytes_per_step": lb + nr * rec,
+                "roofline_frac": (roof["pipeline"]["t_roof_e2e_ms"] / e2e_step) if roof.get("pipeline") else None},
         "roofline": {"bound": "hbm", "kernel": "count_routed", "achieved": achieved, "peak": pk["hbm_gbs"],
                      "unit": "GB/s", "frac": (achieved / pk["hbm_gbs"]) if achieved else None,
                      "peak_source": pk["source"], "alg_bytes_per_launch": alg_bytes,
                      "traffic": profile_traffic(args), "per": "step (all count_routed launches of one count)",
-                     "dominant_stage": dominant},
+                     "dominant_stage": dominant, "atomic": roof.get("count_routed_atomic")},
+        "pipeline_roofline": roof.get("pipeline"),
         "clocks": clk,
         "sizing": None,
     }

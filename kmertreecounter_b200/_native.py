@@ -74,6 +74,13 @@ class KcSetResult(C.Structure):
                 ("root_counts", C.c_uint64 * 256)]
 
 
+class KcPeaks(C.Structure):
+    _fields_ = [("hbm_copy_gbs", C.c_double), ("red_add_gops", C.c_double), ("or_return_gops", C.c_double),
+                ("h2d_gbs", C.c_double), ("footprint_bytes", C.c_uint64), ("ops", C.c_uint64),
+                ("l2_red_add_gops", C.c_double), ("l2_or_return_gops", C.c_double),
+                ("l2_footprint_bytes", C.c_uint64)]
+
+
 class KcError(RuntimeError):
     def __init__(self, code, msg):
         super().__init__(f"kc error {code}: {msg}")
@@ -112,6 +119,7 @@ def _load():
         "kc_count_host_stream": (i32, [vp, vp, u64, SINK_FN, vp, stp]),
         "kc_histogram": (i32, [vp, u32, u32, C.POINTER(u64), C.POINTER(u64)]),
         "kc_count_sets": (i32, [vp, vp, C.POINTER(KcSetDesc), u32, C.POINTER(KcSetResult), stp]),
+        "kc_measure_peaks": (i32, [i32, u64, C.POINTER(KcPeaks)]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -281,6 +289,15 @@ def count_fastq(path, out_dir, **kw):
     st = KcStats()
     check(lib.kc_count_fastq(C.byref(cfg), str(path).encode(), str(out_dir).encode(), C.byref(st)))
     return st
+
+
+def measure_peaks(device=0, footprint_bytes=4 << 30):
+    """Roofline denominators measured on `device` (include/kmer_peaks.h):
+    HBM copy GB/s, random u32 atomic rates (10^9 ops/s) on a footprint far
+    above L2, and the pinned host->device link."""
+    out = KcPeaks()
+    check(lib.kc_measure_peaks(int(device), int(footprint_bytes), C.byref(out)))
+    return {f: getattr(out, f) for f, _ in KcPeaks._fields_}
 
 
 def host_alloc(nbytes):

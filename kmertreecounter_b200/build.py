@@ -36,13 +36,13 @@ def _stale(target, deps):
 
 def _deps(*names):
     out = [os.path.join(CSRC, n) for n in names]
-    out += [os.path.join(ROOT, "include", h) for h in ("kmer_count.h", "kmer_synth.h", "kmer_sizing.h")]
+    out += [os.path.join(ROOT, "include", h) for h in ("kmer_count.h", "kmer_synth.h", "kmer_sizing.h", "kmer_peaks.h")]
     return out
 
 
 def build(force=False, verbose_ptxas=False):
     os.makedirs(os.path.join(HERE, "bin"), exist_ok=True)
-    srcs = ["kc_engine.cu", "kc_sort.cu", "kc_io.cpp", "kc_noalloc.cu", "kc_mlp.cu"]
+    srcs = ["kc_engine.cu", "kc_sort.cu", "kc_io.cpp", "kc_noalloc.cu", "kc_mlp.cu", "kc_peaks.cu"]
     hdrs = ["kc_kernels.cuh", "kc_scan.cuh", "kc_internal.h"]
     if force or _stale(LIB, _deps(*srcs, *hdrs)):
         cmd = [NVCC, *ARCH, "-lineinfo", "-O3", "-std=c++20", "-Xcompiler", "-fPIC", "-shared",

@@ -120,6 +120,11 @@ struct kc_context {
     int device = 0;
     cudaStream_t stream = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    // table initialisation runs on `side` (high priority) beside the
+    // extraction; `stream` waits for ev_init before the table's first use
+    cudaStream_t side = nullptr;
+    cudaEvent_t ev_side_in = nullptr, ev_init = nullptr;
+    bool init_pending = false;
     uint32_t nw = 1, bucket_bits = 8, n_buckets = 256, bucket_shift = 56;
     int sm_count = 148;
     uint64_t slot_bytes = 16, record_bytes = 16, packed_bytes = 8;
@@ -166,6 +171,7 @@ struct kc_context {
     DevBuf bloom, table;
     DevBuf low_packed;
     DevBuf roots, chunks, chunk_pass, chunk_off, root_count;
+    DevBuf pass_bits;  // export: bit per table slot that passes min..max
     uint64_t n_chunks = 0;  // entries of `chunks` (live table regions) of the last export
     DevBuf sort_tmp, sort_hist, sort_offs, sort_sums;
     DevBuf set_tiles, tile_prefix, set_info;  // multi-set batches
@@ -235,19 +241,41 @@ cudaEvent_t next_event(kc_context* c) {
 struct Stage {
     kc_context* c;
     int id;
+    cudaStream_t st;
     cudaEvent_t a = nullptr;
-    Stage(kc_context* ctx, int s, uint64_t n_launch = 1) : c(ctx), id(s) {
+    Stage(kc_context* ctx, int s, uint64_t n_launch = 1, cudaStream_t on = nullptr)
+        : c(ctx), id(s), st(on ? on : ctx->stream) {
         c->launches[s] += n_launch;
-        if (c->profiling && (a = next_event(c))) cudaEventRecord(a, c->stream);
+        if (c->profiling && (a = next_event(c))) cudaEventRecord(a, st);
     }
     ~Stage() {
         if (!a) return;
         cudaEvent_t b = next_event(c);
         if (!b) return;
-        cudaEventRecord(b, c->stream);
+        cudaEventRecord(b, st);
         c->spans.push_back({id, {a, b}});
     }
 };
+
+// CTAs of a grid-stride kernel that are resident at once on the device (at
+// most `cap`): launching more leaves a second, partial wave.
+template <class Kernel>
+uint64_t resident_grid(const kc_context* c, Kernel k, int threads, uint64_t cap) {
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, threads, 0) != cudaSuccess || per_sm < 1) {
+        cudaGetLastError();
+        per_sm = 1;
+    }
+    return std::max<uint64_t>(1, std::min<uint64_t>(cap, (uint64_t)c->sm_count * (uint64_t)per_sm));
+}
+
+// `stream` waits for the table initialisation launched on `side`.
+int join_init(kc_context* c) {
+    if (!c->init_pending) return KC_OK;
+    c->init_pending = false;
+    CK(cudaStreamWaitEvent(c->stream, c->ev_init, 0));
+    return KC_OK;
+}
 
 int setup_shape(kc_context* c) {
     const kc_config& g = c->cfg;
@@ -409,13 +437,21 @@ int size_structures(kc_context* c, const std::vector<uint64_t>& kb, double scale
     CK(c->meta.ensure(nb * sizeof(kc::BucketMeta)));
     CKR(put(c, c->meta.p, c->h_meta.data(), nb * sizeof(kc::BucketMeta)));
     {
-        Stage st(c, KC_STAGE_INIT, 1);
-        CKR(fill_dev(c, c->bloom.p, bw * sizeof(uint64_t), 0));
-        const int ig = 148 * 8;
-        if (c->nw == 1) kc::init_slots<1><<<ig, 256, 0, c->stream>>>(c->table.p, ts);
-        else if (c->nw == 2) kc::init_slots<2><<<ig, 256, 0, c->stream>>>(c->table.p, ts);
-        else kc::init_slots<4><<<ig, 256, 0, c->stream>>>(c->table.p, ts);
+        // Filter and table initialisation on the side stream, after the work
+        // already queued on `stream` (a previous count may still read the
+        // table), one CTA per SM: it runs beside the extraction, which is
+        // bound by instruction issue, not by HBM; the count joins it.
+        CK(cudaEventRecord(c->ev_side_in, c->stream));
+        CK(cudaStreamWaitEvent(c->side, c->ev_side_in, 0));
+        Stage st(c, KC_STAGE_INIT, bw ? 2 : 1, c->side);
+        const int ig = c->sm_count;
+        if (bw) kc::fill_words<<<ig, 256, 0, c->side>>>(c->bloom.as<uint32_t>(), bw * 2, 0u);
+        if (c->nw == 1) kc::init_slots<1><<<ig, 256, 0, c->side>>>(c->table.p, ts);
+        else if (c->nw == 2) kc::init_slots<2><<<ig, 256, 0, c->side>>>(c->table.p, ts);
+        else kc::init_slots<4><<<ig, 256, 0, c->side>>>(c->table.p, ts);
         CK(cudaGetLastError());
+        CK(cudaEventRecord(c->ev_init, c->side));
+        c->init_pending = true;
     }
     CK(c->overflow.ensure(nb * sizeof(uint32_t)));
     CKR(fill_dev(c, c->overflow.p, nb * sizeof(uint32_t), 0));
@@ -427,6 +463,7 @@ int size_structures(kc_context* c, const std::vector<uint64_t>& kb, double scale
 template <int NW>
 void launch_count(kc_context* c, uint64_t n_keys, int use_filter) {
     constexpr int TILE = kc::count_tile<NW>();
+    join_init(c);
     // each CTA covers CNT_SEGS_PER_WARP segments per warp, in blockIdx order
     const uint64_t tiles = ceil_div(n_keys, (uint64_t)TILE * kc::CNT_SEGS_PER_WARP);
     if (!tiles) return;
@@ -708,7 +745,7 @@ int process_batch(kc_context* c, const uint8_t* buf, uint64_t n, int has_halo) {
     }
     {
         Stage st(c, KC_STAGE_PACK_LOW);
-        kc::pack_low<NW><<<std::min<uint64_t>(ceil_div(nsegs, 8), 148 * 16), 256, 0, c->stream>>>(
+        kc::pack_low<NW><<<std::min<uint64_t>(ceil_div(nsegs, 256), (uint64_t)c->sm_count * 8), 256, 0, c->stream>>>(
             c->routed.p, c->tile_low.as<uint32_t>(), c->tile_low_prefix.as<uint64_t>(), nsegs, c->cfg.k, low_dst,
             low_base);
     }
@@ -729,6 +766,7 @@ int run_export(kc_context* c, const std::vector<kc::ExportChunk>& ch, uint64_t n
                std::vector<uint64_t>& totals) {
     const uint64_t nch = ch.size();
     c->n_chunks = nch;
+    CKR(join_init(c));
     CK(c->chunks.ensure(std::max<uint64_t>(nch, 1) * sizeof(kc::ExportChunk)));
     CK(c->chunk_pass.ensure(std::max<uint64_t>(nch, 1) * sizeof(uint32_t)));
     CK(c->chunk_off.ensure(std::max<uint64_t>(nch, 1) * sizeof(uint64_t)));
@@ -737,11 +775,22 @@ int run_export(kc_context* c, const std::vector<kc::ExportChunk>& ch, uint64_t n
     CKR(fill_dev(c, c->root_count.p, (n_groups + 1) * sizeof(uint64_t), 0));
     unsigned long long* rcd = c->root_count.as<unsigned long long>();
     const uint64_t grid = std::min<uint64_t>(std::max<uint64_t>(nch, 1), (uint64_t)c->sm_count * 8);
+    // the counting pass leaves a bit per passing slot when every chunk is whole
+    // 32-slot words (bucket tables are powers of two of at least 64 slots at
+    // offsets that are multiples of 64), and the writing pass reads only those
+    uint32_t* bits = nullptr;
+    bool whole_words = true;
+    for (const kc::ExportChunk& e : ch) whole_words = whole_words && e.slot_begin % 32 == 0 && e.n_slots % 32 == 0;
+    if (whole_words && nch) {
+        CK(c->pass_bits.ensure(ceil_div(c->table_slots_used, 32) * sizeof(uint32_t)));
+        bits = c->pass_bits.as<uint32_t>();
+    }
     if (nch) {
         Stage st(c, KC_STAGE_EXPORT);
-        kc::export_count<NW><<<grid, kc::EXP_THREADS, 0, c->stream>>>(
+        const uint64_t cgrid = resident_grid(c, kc::export_count<NW>, kc::EXP_THREADS, nch);
+        kc::export_count<NW><<<cgrid, kc::EXP_THREADS, 0, c->stream>>>(
             c->table.p, c->chunks.as<kc::ExportChunk>(), nch, c->cfg.min_count, c->cfg.max_count,
-            c->chunk_pass.as<uint32_t>(), rcd, rcd + n_groups);
+            c->chunk_pass.as<uint32_t>(), rcd, rcd + n_groups, bits);
         CK(cudaGetLastError());
     }
     int rc;
@@ -756,9 +805,15 @@ int run_export(kc_context* c, const std::vector<kc::ExportChunk>& ch, uint64_t n
     CK(c->roots.ensure(std::max<uint64_t>(R, 1) * c->record_bytes));
     if (nch && R) {
         Stage st(c, KC_STAGE_EXPORT);
-        kc::export_write<NW><<<grid, kc::EXP_THREADS, 0, c->stream>>>(
-            c->table.p, c->chunks.as<kc::ExportChunk>(), nch, c->cfg.min_count, c->cfg.max_count,
-            c->chunk_off.as<uint64_t>(), c->roots.as<uint8_t>());
+        if (bits)
+            kc::export_write_bits<NW><<<resident_grid(c, kc::export_write_bits<NW>, kc::EXP_THREADS, nch),
+                                        kc::EXP_THREADS, 0, c->stream>>>(
+                c->table.p, bits, c->chunks.as<kc::ExportChunk>(), nch, c->chunk_off.as<uint64_t>(),
+                c->roots.as<uint8_t>());
+        else
+            kc::export_write<NW><<<grid, kc::EXP_THREADS, 0, c->stream>>>(
+                c->table.p, c->chunks.as<kc::ExportChunk>(), nch, c->cfg.min_count, c->cfg.max_count,
+                c->chunk_off.as<uint64_t>(), c->roots.as<uint8_t>());
         CK(cudaGetLastError());
     }
     return KC_OK;
@@ -1049,10 +1104,15 @@ int kc_create(const kc_config* cfg, kc_context** out) {
         delete c;
         return fail(KC_ERR_DEVICE, "stream/event creation failed: %s", cudaGetErrorString(e));
     }
+    int prio_low = 0, prio_high = 0;
+    cudaDeviceGetStreamPriorityRange(&prio_low, &prio_high);
     if ((e = cudaStreamCreateWithFlags(&c->h2d, cudaStreamNonBlocking)) != cudaSuccess ||
-        (e = cudaStreamCreateWithFlags(&c->d2h, cudaStreamNonBlocking)) != cudaSuccess) {
-        delete c;
-        return fail(KC_ERR_DEVICE, "copy stream creation failed: %s", cudaGetErrorString(e));
+        (e = cudaStreamCreateWithFlags(&c->d2h, cudaStreamNonBlocking)) != cudaSuccess ||
+        (e = cudaStreamCreateWithPriority(&c->side, cudaStreamNonBlocking, prio_high)) != cudaSuccess ||
+        (e = cudaEventCreateWithFlags(&c->ev_side_in, cudaEventDisableTiming)) != cudaSuccess ||
+        (e = cudaEventCreateWithFlags(&c->ev_init, cudaEventDisableTiming)) != cudaSuccess) {
+        kc_destroy(c);
+        return fail(KC_ERR_DEVICE, "stream creation failed: %s", cudaGetErrorString(e));
     }
     for (int i = 0; i < 2; ++i) {
         cudaEventCreateWithFlags(&c->ev_h2d[i], cudaEventDisableTiming);
@@ -1093,11 +1153,12 @@ void kc_destroy(kc_context* c) {
     if (!c) return;
     cudaSetDevice(c->device);
     if (c->stream) cudaStreamSynchronize(c->stream);
+    if (c->side) cudaStreamSynchronize(c->side);
     DevBuf* bufs[] = {&c->stage,  &c->tile_nl,   &c->tile_line, &c->bucket_count, &c->bucket_cursor, &c->region_end, &c->region_fill, &c->routed,
                       &c->tile_low, &c->tile_fail, &c->tile_low_prefix, &c->scan_sums, &c->scalars, &c->overflow,
                       &c->meta,   &c->bloom,     &c->table,     &c->low_packed,   &c->roots,         &c->chunks,
                       &c->root_count, &c->chunk_pass, &c->chunk_off, &c->sort_tmp, &c->sort_hist, &c->sort_offs, &c->sort_sums,
-                      &c->set_tiles, &c->tile_prefix, &c->set_info};
+                      &c->set_tiles, &c->tile_prefix, &c->set_info, &c->pass_bits};
     for (DevBuf* b : bufs) b->release();
     for (cudaEvent_t e : c->ev_pool) cudaEventDestroy(e);
     if (c->h2d) cudaStreamSynchronize(c->h2d);
@@ -1117,6 +1178,9 @@ void kc_destroy(kc_context* c) {
     c->stage2.release();
     if (c->h2d) cudaStreamDestroy(c->h2d);
     if (c->d2h) cudaStreamDestroy(c->d2h);
+    if (c->side) cudaStreamDestroy(c->side);
+    if (c->ev_side_in) cudaEventDestroy(c->ev_side_in);
+    if (c->ev_init) cudaEventDestroy(c->ev_init);
     if (c->ev0) cudaEventDestroy(c->ev0);
     if (c->ev1) cudaEventDestroy(c->ev1);
     if (c->stream) cudaStreamDestroy(c->stream);

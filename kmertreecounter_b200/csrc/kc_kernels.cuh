@@ -1353,50 +1353,79 @@ __global__ void init_slots(void* tab, uint64_t n) {
 // low.bin packing (src/ExportWriter.h:522-550): k/32 full words as raw
 // little-endian u64, then the top ceil(2(k%32)/8) bytes of the tail word
 // (masked to its 2(k%32) high bits), in little-endian byte order.
+// One key packed at d (P bytes; full = k/32 whole words, tail_bytes of the
+// masked tail word).
+template <int NW>
+__device__ __forceinline__ void pack_key(const typename KeyOf<NW>::T& key, uint8_t* d, uint32_t full,
+                                         uint32_t tail_bytes, uint32_t P, uint64_t tmask) {
+    // word f of the key (f < 4; words past the key's width read 0)
+    auto word = [&](uint32_t f) -> uint64_t {
+        if constexpr (NW == 1) {
+            return f == 0 ? key : 0ull;
+        } else if constexpr (NW == 2) {
+            return f == 0 ? key.w0 : (f == 1 ? key.w1 : 0ull);
+        } else {
+            return f == 0 ? key.w0 : (f == 1 ? key.w1 : (f == 2 ? key.w2 : key.w3));
+        }
+    };
+    if (P == 8) {
+        *reinterpret_cast<uint64_t*>(d) = full ? word(0) : (word(0) & tmask);
+    } else if (P == 16) {
+        reinterpret_cast<uint64_t*>(d)[0] = word(0);
+        reinterpret_cast<uint64_t*>(d)[1] = full == 2 ? word(1) : (word(1) & tmask);
+    } else {
+        // k/32 whole words little-endian, then the top tail_bytes bytes
+        // of the masked tail word (src/ExportWriter.h:522-550)
+        uint32_t q = 0;
+        for (uint32_t f = 0; f < full; ++f) {
+            const uint64_t w = word(f);
+            for (uint32_t b = 0; b < 8; ++b) d[q++] = (uint8_t)(w >> (8 * b));
+        }
+        if (tail_bytes) {
+            const uint64_t tw = (full < 4 ? word(full) : 0ull) & tmask;
+            for (uint32_t b = 8 - tail_bytes; b < 8; ++b) d[q++] = (uint8_t)(tw >> (8 * b));
+        }
+    }
+}
+
+// A warp packs 32 segments at a time: lane l loads segment l's count and
+// output index (one coalesced load each), then the warp walks the segments,
+// every lane loading all of its keys of a segment (up to SEG/32) before
+// storing any, so several loads per lane are in flight.
 template <int NW>
 __global__ void pack_low(const void* routed, const uint32_t* seg_low, const uint64_t* seg_low_prefix, uint64_t n_segs,
                          uint32_t k, uint8_t* out, uint64_t out_base) {
     using K = typename KeyOf<NW>::T;
     constexpr int SEG = count_seg<NW>();
-    const K* keys = reinterpret_cast<const K*>(routed);
+    constexpr int PER = SEG / 32;  // keys per lane per segment
+    const K* __restrict__ keys = reinterpret_cast<const K*>(routed);
     const uint32_t full = k / 32, tail_bits = 2 * (k % 32), tail_bytes = (tail_bits + 7) / 8;
     const uint32_t P = full * 8 + tail_bytes;
     const uint64_t tmask = tail_bits ? (~0ull << (64 - tail_bits)) : 0ull;
     const int lane = threadIdx.x & 31;
     const uint64_t warps = (uint64_t)gridDim.x * (blockDim.x >> 5);
-    for (uint64_t sg = (uint64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); sg < n_segs; sg += warps) {
-        const uint32_t n = seg_low[sg];
-        const uint64_t o = out_base + seg_low_prefix[sg];
-        for (uint32_t i = lane; i < n; i += 32) {
-            const K key = keys[sg * (uint64_t)SEG + i];
-            uint64_t w[4] = {0, 0, 0, 0};
-            if constexpr (NW == 1) {
-                w[0] = key;
-            } else if constexpr (NW == 2) {
-                w[0] = key.w0;
-                w[1] = key.w1;
-            } else {
-                w[0] = key.w0;
-                w[1] = key.w1;
-                w[2] = key.w2;
-                w[3] = key.w3;
+    for (uint64_t g = ((uint64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)) * 32; g < n_segs;
+         g += warps * 32) {
+        const uint64_t my = g + lane;
+        const uint32_t n_l = my < n_segs ? seg_low[my] : 0u;
+        const uint64_t o_l = my < n_segs ? seg_low_prefix[my] : 0ull;
+        uint32_t todo = __ballot_sync(0xffffffffu, n_l != 0);
+        while (todo) {
+            const int q = __ffs(todo) - 1;
+            todo &= todo - 1;
+            const uint32_t n = __shfl_sync(0xffffffffu, n_l, q);
+            const uint64_t o = out_base + __shfl_sync(0xffffffffu, o_l, q);
+            const uint64_t s0 = (g + q) * (uint64_t)SEG;
+            K v[PER];
+#pragma unroll
+            for (int j = 0; j < PER; ++j) {
+                const uint32_t i = j * 32 + lane;
+                if (i < n) v[j] = keys[s0 + i];
             }
-            uint8_t* d = out + (o + i) * P;
-            if (P == 8) {
-                *reinterpret_cast<uint64_t*>(d) = full ? w[0] : (w[0] & tmask);
-            } else if (P == 16) {
-                reinterpret_cast<uint64_t*>(d)[0] = w[0];
-                reinterpret_cast<uint64_t*>(d)[1] = full == 2 ? w[1] : (w[1] & tmask);
-            } else {
-                // k/32 whole words little-endian, then the top tail_bytes bytes
-                // of the masked tail word (src/ExportWriter.h:522-550)
-                uint32_t q = 0;
-                for (uint32_t f = 0; f < full; ++f)
-                    for (uint32_t b = 0; b < 8; ++b) d[q++] = (uint8_t)(w[f] >> (8 * b));
-                if (tail_bytes) {
-                    const uint64_t tw = w[full] & tmask;
-                    for (uint32_t b = 8 - tail_bytes; b < 8; ++b) d[q++] = (uint8_t)(tw >> (8 * b));
-                }
+#pragma unroll
+            for (int j = 0; j < PER; ++j) {
+                const uint32_t i = j * 32 + lane;
+                if (i < n) pack_key<NW>(v[j], out + (o + i) * P, full, tail_bytes, P, tmask);
             }
         }
     }
@@ -1419,15 +1448,44 @@ __device__ __forceinline__ bool slot_used(const typename SlotOf<NW>::T& s) {
 constexpr int EXP_THREADS = 256;
 constexpr int EXP_ITEMS = 4;  // slots per thread per round (strided by EXP_THREADS)
 
+// One ExportRecord<N> {key words, count, pad = 0} at index r.
+template <int NW>
+__device__ __forceinline__ void write_record(uint8_t* records, uint64_t r, const typename SlotOf<NW>::T& v) {
+    if constexpr (NW == 1) {
+        uint4 w;
+        w.x = (uint32_t)v.key;
+        w.y = (uint32_t)(v.key >> 32);
+        w.z = v.count;
+        w.w = 0;
+        reinterpret_cast<uint4*>(records)[r] = w;
+    } else if constexpr (NW == 2) {
+        uint64_t* d = reinterpret_cast<uint64_t*>(records + r * 24);
+        d[0] = v.w0;
+        d[1] = v.w1;
+        d[2] = (uint64_t)v.count;
+    } else {
+        uint64_t* d = reinterpret_cast<uint64_t*>(records + r * 40);
+        d[0] = v.w0;
+        d[1] = v.w1;
+        d[2] = v.w2;
+        d[3] = v.w3;
+        d[4] = (uint64_t)v.count;
+    }
+}
+
 // Count slots passing the filter min <= count <= max per export chunk and per
 // root id (src/NewKmerTree.h:1159-1168), and occupied slots overall.  The
 // per-chunk counts, scanned in chunk order, are the chunks' output offsets:
 // chunks are listed root by root, so each root's records are contiguous.
+// With `pass_bits` (chunks start at and span multiples of 32 slots), bit i of
+// word w is set when arena slot 32w + i passes: a warp reads 32 consecutive
+// slots, so one ballot is one word, and export_write_bits then reads only the
+// passing slots.
 template <int NW>
 __global__ void __launch_bounds__(EXP_THREADS) export_count(const void* table, const ExportChunk* chunks,
                                                             uint64_t n_chunks, uint32_t min_c, uint32_t max_c,
                                                             uint32_t* chunk_pass, unsigned long long* root_count,
-                                                            unsigned long long* occupied) {
+                                                            unsigned long long* occupied, uint32_t* pass_bits) {
     using S = typename SlotOf<NW>::T;
     __shared__ uint32_t s_pass[EXP_THREADS / 32], s_occ[EXP_THREADS / 32];
     const S* tab = reinterpret_cast<const S*>(table);
@@ -1445,9 +1503,16 @@ __global__ void __launch_bounds__(EXP_THREADS) export_count(const void* table, c
 #pragma unroll
             for (int j = 0; j < EXP_ITEMS; ++j) {
                 const uint32_t i = i0 + j * EXP_THREADS + threadIdx.x;
+                bool ok = false;
                 if (i < ch.n_slots && slot_used<NW>(v[j])) {
                     ++occ;
-                    pass += v[j].count >= min_c && v[j].count <= max_c;
+                    ok = v[j].count >= min_c && v[j].count <= max_c;
+                    pass += ok;
+                }
+                if (pass_bits) {
+                    const uint32_t word = __ballot_sync(0xffffffffu, ok);
+                    const uint32_t i_lane0 = i - (uint32_t)lane;
+                    if (lane == 0 && i_lane0 < ch.n_slots) pass_bits[(ch.slot_begin + i_lane0) >> 5] = word;
                 }
             }
         }
@@ -1521,29 +1586,70 @@ __global__ void __launch_bounds__(EXP_THREADS) export_write(const void* table, c
             __syncthreads();  // s_warp is rewritten next round
             uint64_t r = out + before + incl - mine;
 #pragma unroll
-            for (int j = 0; j < EXP_ITEMS; ++j) {
-                if (!((keep >> j) & 1u)) continue;
-                if constexpr (NW == 1) {
-                    uint4 w;
-                    w.x = (uint32_t)v[j].key;
-                    w.y = (uint32_t)(v[j].key >> 32);
-                    w.z = v[j].count;
-                    w.w = 0;
-                    reinterpret_cast<uint4*>(records)[r] = w;
-                } else if constexpr (NW == 2) {
-                    uint64_t* d = reinterpret_cast<uint64_t*>(records + r * 24);
-                    d[0] = v[j].w0;
-                    d[1] = v[j].w1;
-                    d[2] = (uint64_t)v[j].count;
-                } else {
-                    uint64_t* d = reinterpret_cast<uint64_t*>(records + r * 40);
-                    d[0] = v[j].w0;
-                    d[1] = v[j].w1;
-                    d[2] = v[j].w2;
-                    d[3] = v[j].w3;
-                    d[4] = (uint64_t)v[j].count;
+            for (int j = 0; j < EXP_ITEMS; ++j)
+                if ((keep >> j) & 1u) write_record<NW>(records, r++, v[j]);
+            out += total;
+        }
+    }
+}
+
+// export_write over the passing-slot bitmap of export_count: a thread owns
+// two words (64 consecutive slots) per round, threads in order, so records
+// keep table order (the order export_write produces); only passing slots are
+// read, up to 8 of them in flight per thread.
+template <int NW>
+__global__ void __launch_bounds__(EXP_THREADS) export_write_bits(const void* table, const uint32_t* pass_bits,
+                                                                 const ExportChunk* chunks, uint64_t n_chunks,
+                                                                 const uint64_t* chunk_off, uint8_t* records) {
+    using S = typename SlotOf<NW>::T;
+    constexpr int BATCH = 8;
+    __shared__ uint32_t s_warp[EXP_THREADS / 32];
+    const S* tab = reinterpret_cast<const S*>(table);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (uint64_t c = blockIdx.x; c < n_chunks; c += gridDim.x) {
+        const ExportChunk ch = chunks[c];
+        const uint64_t w0 = ch.slot_begin >> 5;
+        const uint32_t nw = ch.n_slots >> 5;
+        uint64_t out = chunk_off[c];
+        for (uint32_t r0 = 0; r0 < nw; r0 += 2 * EXP_THREADS) {
+            const uint32_t wi = r0 + 2 * threadIdx.x;
+            const uint64_t cell0 = (w0 + wi) << 5;
+            uint64_t m = 0;
+            if (wi < nw) m = __ldcg(pass_bits + w0 + wi);
+            if (wi + 1 < nw) m |= (uint64_t)__ldcg(pass_bits + w0 + wi + 1) << 32;
+            // block-wide exclusive scan of the per-thread record counts
+            const uint32_t mine = __popcll(m);
+            uint32_t incl = mine;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+                if (lane >= o) incl += y;
+            }
+            if (lane == 31) s_warp[warp] = incl;
+            __syncthreads();
+            uint32_t before = 0, total = 0;
+#pragma unroll
+            for (int w = 0; w < EXP_THREADS / 32; ++w) {
+                const uint32_t t = s_warp[w];
+                before += w < warp ? t : 0u;
+                total += t;
+            }
+            __syncthreads();  // s_warp is rewritten next round
+            uint64_t r = out + before + incl - mine;
+            while (m) {
+                int b[BATCH];
+#pragma unroll
+                for (int j = 0; j < BATCH; ++j) {
+                    b[j] = m ? __ffsll(m) - 1 : -1;
+                    m &= m - 1;
                 }
-                ++r;
+                S v[BATCH];
+#pragma unroll
+                for (int j = 0; j < BATCH; ++j)
+                    if (b[j] >= 0) v[j] = tab[cell0 + b[j]];
+#pragma unroll
+                for (int j = 0; j < BATCH; ++j)
+                    if (b[j] >= 0) write_record<NW>(records, r++, v[j]);
             }
             out += total;
         }

@@ -227,7 +227,7 @@ int run(const kc_config* g, const uint8_t* d_fastq, uint64_t n, uint8_t* d_low, 
     const uint64_t P = kc_packed_bytes(k);
     if (nlow * P > low_cap) return err(KC_ERR_INVALID, "low output buffer too small");
     if (nsegs)
-        kc::pack_low<NW><<<std::min<uint64_t>(cdiv(nsegs, 8), 148 * 4), 256, 0, st>>>(routed, seg_low, seg_prefix,
+        kc::pack_low<NW><<<std::min<uint64_t>(cdiv(nsegs, 256), 148 * 4), 256, 0, st>>>(routed, seg_low, seg_prefix,
                                                                                        nsegs, k, d_low, 0);
 
     // root records grouped by root id
@@ -247,7 +247,7 @@ int run(const kc_config* g, const uint8_t* d_fastq, uint64_t n, uint8_t* d_low, 
     const uint64_t egrid = std::max<uint64_t>(1, std::min<uint64_t>(nch, 148 * 4));
     if (nch)
         kc::export_count<NW><<<egrid, kc::EXP_THREADS, 0, st>>>(table, chunks, nch, g->min_count, g->max_count,
-                                                                chunk_pass, rcount, rcount + 256);
+                                                                chunk_pass, rcount, rcount + 256, nullptr);
     uint64_t h_r[257];
     uint32_t h_pass[MAX_CHUNKS];
     NK(cudaMemcpyAsync(h_r, rcount, sizeof h_r, cudaMemcpyDeviceToHost, st));

@@ -12,7 +12,7 @@ import kmertreecounter_b200 as kc
 from kmertreecounter_b200 import _native, synth
 
 HEADERS = {"kmer_count.h": _native.LIB_PATH, "kmer_synth.h": _native.SYNTH_PATH,
-           "kmer_sizing.h": _native.LIB_PATH}
+           "kmer_sizing.h": _native.LIB_PATH, "kmer_peaks.h": _native.LIB_PATH}
 
 
 def declared(header):
@@ -51,8 +51,9 @@ def test_struct_layout_matches_header(tmp_path):
     """Every ctypes mirror of a header struct has the C compiler's size and
     field offsets."""
     structs = {"kc_config": _native.KcConfig, "kc_stats": _native.KcStats,
-               "kc_set_desc": _native.KcSetDesc, "kc_set_result": _native.KcSetResult}
-    lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "kmer_count.h"', "int main(void) {"]
+               "kc_set_desc": _native.KcSetDesc, "kc_set_result": _native.KcSetResult, "kc_peaks": _native.KcPeaks}
+    lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "kmer_count.h"', '#include "kmer_peaks.h"',
+             "int main(void) {"]
     for cname, py in structs.items():
         lines.append(f'printf("{cname} size %zu\\n", sizeof({cname}));')
         for f in py._fields_:
@@ -70,6 +71,13 @@ def test_struct_layout_matches_header(tmp_path):
         assert got[(cname, "size")] == C.sizeof(py), cname
         for f in py._fields_:
             assert got[(cname, f[0])] == getattr(py, f[0]).offset, (cname, f[0])
+
+
+@pytest.mark.parametrize("footprint", [0, 128 << 20, (4 << 30) + 4096, 64 << 30])
+def test_peaks_footprint_rejected_before_device(footprint):
+    with pytest.raises(kc.KcError) as e:
+        kc.measure_peaks(0, footprint)
+    assert e.value.code == kc.KC_ERR_INVALID
 
 
 def test_min_max_order_rejected():
