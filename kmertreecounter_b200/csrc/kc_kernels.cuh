@@ -992,6 +992,33 @@ __device__ __forceinline__ bool table_add_first(Slot2* tab, uint64_t mask, uint6
     return table_add_slow(tab, mask, h, key, add, 0);
 }
 
+// Probe-round helpers of count_routed (64- and 128-bit keys): a cell's key
+// as read (16-byte reads of a 128-bit cell may be torn while it is claimed:
+// any EMPTY half counts as empty and is settled by the CAS), the claim of a
+// cell read empty (returns the cell's key after the CAS: `key` when this
+// thread claimed it), and the match test.
+__device__ __forceinline__ bool cell_empty(uint64_t v) { return v == EMPTY; }
+__device__ __forceinline__ bool cell_empty(const ulonglong2& v) { return v.x == EMPTY || v.y == EMPTY; }
+__device__ __forceinline__ bool cell_holds(uint64_t v, uint64_t key) { return v == key; }
+__device__ __forceinline__ bool cell_holds(const ulonglong2& v, const Key2& key) {
+    return v.x == key.w0 && v.y == key.w1;
+}
+__device__ __forceinline__ uint64_t read_cell(const Slot1* s) { return __ldcg(&s->key); }
+__device__ __forceinline__ ulonglong2 read_cell(const Slot2* s) {
+    return __ldcg(reinterpret_cast<const ulonglong2*>(s));
+}
+__device__ __forceinline__ uint64_t claim_cell(Slot1* s, uint64_t key) {
+    const uint64_t old = atomicCAS(reinterpret_cast<unsigned long long*>(&s->key), EMPTY, key);
+    return old == EMPTY ? key : old;
+}
+__device__ __forceinline__ ulonglong2 claim_cell(Slot2* s, const Key2& key) {
+    const unsigned __int128 e = ~(unsigned __int128)0;
+    const unsigned __int128 kv = ((unsigned __int128)key.w1 << 64) | key.w0;
+    const unsigned __int128 old = atomicCAS(reinterpret_cast<unsigned __int128*>(s), e, kv);
+    const unsigned __int128 now = old == e ? kv : old;
+    return make_ulonglong2((uint64_t)now, (uint64_t)(now >> 64));
+}
+
 __device__ __forceinline__ bool key_eq(uint64_t a, uint64_t b) { return a == b; }
 __device__ __forceinline__ bool key_eq(const Key2& a, const Key2& b) { return a.w0 == b.w0 && a.w1 == b.w1; }
 __device__ __forceinline__ bool key_eq(const Key4& a, const Key4& b) {
@@ -1243,24 +1270,67 @@ __global__ void __launch_bounds__(CNT_THREADS, 4) count_routed(CountArgs a) {
             }
         }
         uint32_t fail_bits = 0;
+        if constexpr (NW == 4) {
 #pragma unroll
-        for (int j = 0; j < ITEMS; ++j) {
-            const uint32_t reps = mult[j] - ((first_bits >> j) & 1u);
-            if (mult[j] && reps) {
-                const uint32_t b = set_bucket0 + (uint32_t)(key_hi(it[j]) >> a.bucket_shift);
-                const MetaS m = meta_of(b);
-                bool added;
-                if constexpr (NW == 4) {
+            for (int j = 0; j < ITEMS; ++j) {
+                const uint32_t reps = mult[j] - ((first_bits >> j) & 1u);
+                if (mult[j] && reps) {
+                    const uint32_t b = set_bucket0 + (uint32_t)(key_hi(it[j]) >> a.bucket_shift);
+                    const MetaS m = meta_of(b);
                     const int r = table_add4(table + m.tab_off, m.tab_mask, h[j], it[j], reps);
                     if (r < 0) atomicOr(a.error, 1u);  // a slot was never published: reported, not retried
-                    added = r != 0;
-                } else {
-                    added = table_add_first(table + m.tab_off, m.tab_mask, h[j], it[j], reps, seen[j]);
+                    if (r == 0) {
+                        fail_bits |= 1u << j;
+                        mult[j] = reps;  // keep the count that still has to be added
+                        a.bucket_overflow[b] = 1u;
+                    }
                 }
-                if (!added) {
-                    fail_bits |= 1u << j;
-                    mult[j] = reps;  // keep the count that still has to be added
-                    a.bucket_overflow[b] = 1u;
+            }
+        } else {
+            // Repeats into the table by linear probing in lockstep rounds.
+            // Round p settles every item whose probe cell p it has read
+            // (`seen`; round 0 is the cell read with the filter word): the
+            // claims of all items (CAS on a cell read EMPTY, or with an EMPTY
+            // half for 128-bit keys) are issued before any result is used,
+            // then items whose cell holds their key add their count, and items
+            // that met another key read their next cell together.  A collision
+            // in one lane costs the warp one more round for all its items,
+            // not one more dependent chain per item.
+            uint32_t todo = 0;
+#pragma unroll
+            for (int j = 0; j < ITEMS; ++j) {
+                mult[j] = mult[j] ? mult[j] - ((first_bits >> j) & 1u) : 0u;  // occurrences left to add
+                if (mult[j]) todo |= 1u << j;
+            }
+            for (uint32_t p = 0;; ++p) {
+#pragma unroll
+                for (int j = 0; j < ITEMS; ++j) {
+                    if (((todo >> j) & 1u) && cell_empty(seen[j])) {
+                        const MetaS m = meta_of(set_bucket0 + (uint32_t)(key_hi(it[j]) >> a.bucket_shift));
+                        seen[j] = claim_cell(table + m.tab_off + (((h[j] >> 17) + p) & m.tab_mask), it[j]);
+                    }
+                }
+#pragma unroll
+                for (int j = 0; j < ITEMS; ++j) {
+                    if (!((todo >> j) & 1u)) continue;
+                    const uint32_t b = set_bucket0 + (uint32_t)(key_hi(it[j]) >> a.bucket_shift);
+                    const MetaS m = meta_of(b);
+                    if (cell_holds(seen[j], it[j])) {
+                        atomicAdd(&table[m.tab_off + (((h[j] >> 17) + p) & m.tab_mask)].count, mult[j]);
+                        todo &= ~(1u << j);
+                    } else if ((uint64_t)p + 1 >= min((uint64_t)PROBE_LIMIT, (uint64_t)m.tab_mask + 1)) {
+                        fail_bits |= 1u << j;  // mult[j] keeps the count that still has to be added
+                        todo &= ~(1u << j);
+                        a.bucket_overflow[b] = 1u;
+                    }
+                }
+                if (!__any_sync(0xffffffffu, todo != 0)) break;  // warp-uniform
+#pragma unroll
+                for (int j = 0; j < ITEMS; ++j) {
+                    if ((todo >> j) & 1u) {
+                        const MetaS m = meta_of(set_bucket0 + (uint32_t)(key_hi(it[j]) >> a.bucket_shift));
+                        seen[j] = read_cell(table + m.tab_off + (((h[j] >> 17) + p + 1) & m.tab_mask));
+                    }
                 }
             }
         }
