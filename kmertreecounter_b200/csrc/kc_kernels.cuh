@@ -1245,27 +1245,39 @@ __global__ void __launch_bounds__(CNT_THREADS, 4) count_routed(CountArgs a) {
         }
         uint32_t first_bits = 0;  // bit j: item j is a first occurrence
         if (a.use_filter) {
+            // every item's filter atomic is issued before any old value is
+            // tested (old[j] is replaced by the atomic's return value; an item
+            // whose bits were all set already keeps its read value)
+            bool in_table = false;
+            if constexpr (NW == 1) in_table = a.filter_in_table != 0;
+            uint32_t issued = 0;
 #pragma unroll
             for (int j = 0; j < ITEMS; ++j) {
                 if (mult[j]) {
-                    bool in_table = false;
-                    if constexpr (NW == 1) in_table = a.filter_in_table != 0;
                     const uint64_t bits = in_table ? (uint64_t)bloom_bits32(h[j]) : bloom_bits(h[j]);
                     if ((old[j] & bits) != bits) {
                         const MetaS m = meta_of(set_bucket0 + (uint32_t)(key_hi(it[j]) >> a.bucket_shift));
-                        uint64_t o;
                         if constexpr (NW == 1) {
                             if (in_table)
-                                o = atomicOr(&(table + m.bloom_off + ((h[j] >> 17) & m.bloom_mask))->pad, (uint32_t)bits);
+                                old[j] = atomicOr(&(table + m.bloom_off + ((h[j] >> 17) & m.bloom_mask))->pad,
+                                                  (uint32_t)bits);
                             else
-                                o = atomicOr(reinterpret_cast<unsigned long long*>(a.bloom + m.bloom_off +
-                                                                                   (h[j] & m.bloom_mask)), bits);
+                                old[j] = atomicOr(reinterpret_cast<unsigned long long*>(a.bloom + m.bloom_off +
+                                                                                        (h[j] & m.bloom_mask)),
+                                                  bits);
                         } else {
-                            o = atomicOr(reinterpret_cast<unsigned long long*>(a.bloom + m.bloom_off + (h[j] & m.bloom_mask)),
-                                         bits);
+                            old[j] = atomicOr(
+                                reinterpret_cast<unsigned long long*>(a.bloom + m.bloom_off + (h[j] & m.bloom_mask)), bits);
                         }
-                        if ((o & bits) != bits) first_bits |= 1u << j;
+                        issued |= 1u << j;
                     }
+                }
+            }
+#pragma unroll
+            for (int j = 0; j < ITEMS; ++j) {
+                if ((issued >> j) & 1u) {
+                    const uint64_t bits = in_table ? (uint64_t)bloom_bits32(h[j]) : bloom_bits(h[j]);
+                    if ((old[j] & bits) != bits) first_bits |= 1u << j;
                 }
             }
         }
