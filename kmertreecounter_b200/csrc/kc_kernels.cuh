@@ -1040,9 +1040,20 @@ struct SlotOf<4> {
     using T = Slot4;
 };
 
+// Keys per lane of the count kernel and its CTAs per SM (the register budget
+// is 65536 / (256 x CTAs)).  The kernel waits on L2 round trips, so resident
+// warps hide more than items per lane: for 64-bit keys 2 items at 6 CTAs/SM
+// (40 registers) ran 42.7 ms where 4 items at 4 CTAs ran 47.4 and 6 at 3 ran
+// 58.3 (genome-scale step, same counts); for 128-bit keys 2 items at 5 CTAs
+// (48 registers) ran 13.8 ms against 14.4 at 4 CTAs and 13.9 for 1 item at 6
+// (the k=63 shape at a tenth of its size).
 template <int NW>
 __host__ __device__ constexpr int count_items() {
-    return NW == 1 ? 4 : (NW == 2 ? 2 : 1);
+    return NW == 1 ? 2 : (NW == 2 ? 2 : 1);
+}
+template <int NW>
+__host__ __device__ constexpr int count_min_ctas() {
+    return NW == 1 ? 6 : (NW == 2 ? 5 : 4);
 }
 // Keys owned by one warp of the count kernel (a contiguous segment).
 template <int NW>
@@ -1101,7 +1112,7 @@ constexpr int CNT_SEGS_PER_WARP = 4;
 // (only this warp reads it; __syncwarp orders reads before writes): first
 // occurrences at the front, keys that met a full table at the back.
 template <int NW>
-__global__ void __launch_bounds__(CNT_THREADS, 4) count_routed(CountArgs a) {
+__global__ void __launch_bounds__(CNT_THREADS, count_min_ctas<NW>()) count_routed(CountArgs a) {
     using K = typename KeyOf<NW>::T;
     using S = typename SlotOf<NW>::T;
     // first table slot read ahead of the filter result (not for 256-bit keys,
