@@ -745,7 +745,7 @@ int process_batch(kc_context* c, const uint8_t* buf, uint64_t n, int has_halo) {
     }
     {
         Stage st(c, KC_STAGE_PACK_LOW);
-        kc::pack_low<NW><<<std::min<uint64_t>(ceil_div(nsegs, 256), (uint64_t)c->sm_count * 8), 256, 0, c->stream>>>(
+        kc::pack_low<NW><<<resident_grid(c, kc::pack_low<NW>, 256, ceil_div(nsegs, 256)), 256, 0, c->stream>>>(
             c->routed.p, c->tile_low.as<uint32_t>(), c->tile_low_prefix.as<uint64_t>(), nsegs, c->cfg.k, low_dst,
             low_base);
     }

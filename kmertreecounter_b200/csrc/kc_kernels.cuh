@@ -1094,7 +1094,7 @@ struct MetaS {
     uint32_t bloom_mask, tab_mask;
 };
 constexpr int META_SMEM_BUCKETS = 256;
-constexpr int CNT_SEGS_PER_WARP = 4;
+constexpr int CNT_SEGS_PER_WARP = 8;
 
 // For each routed key: the first-occurrence filter decides low.bin (first)
 // or the repeat table (seen before), as the reference's classifier does with
@@ -1482,15 +1482,17 @@ __device__ __forceinline__ void pack_key(const typename KeyOf<NW>::T& key, uint8
 }
 
 // A warp packs 32 segments at a time: lane l loads segment l's count and
-// output index (one coalesced load each), then the warp walks the segments,
-// every lane loading all of its keys of a segment (up to SEG/32) before
-// storing any, so several loads per lane are in flight.
+// output index (one coalesced load each), then the warp walks the segments
+// that have first occurrences, B at a time, every lane loading all of its
+// keys of those segments before storing any, so that 4 loads per lane are in
+// flight.
 template <int NW>
 __global__ void pack_low(const void* routed, const uint32_t* seg_low, const uint64_t* seg_low_prefix, uint64_t n_segs,
                          uint32_t k, uint8_t* out, uint64_t out_base) {
     using K = typename KeyOf<NW>::T;
     constexpr int SEG = count_seg<NW>();
-    constexpr int PER = SEG / 32;  // keys per lane per segment
+    constexpr int PER = SEG / 32;                  // keys per lane per segment
+    constexpr int B = PER >= 4 ? 1 : 4 / PER;      // segments per round: 4 keys per lane in flight
     const K* __restrict__ keys = reinterpret_cast<const K*>(routed);
     const uint32_t full = k / 32, tail_bits = 2 * (k % 32), tail_bytes = (tail_bits + 7) / 8;
     const uint32_t P = full * 8 + tail_bytes;
@@ -1504,22 +1506,35 @@ __global__ void pack_low(const void* routed, const uint32_t* seg_low, const uint
         const uint64_t o_l = my < n_segs ? seg_low_prefix[my] : 0ull;
         uint32_t todo = __ballot_sync(0xffffffffu, n_l != 0);
         while (todo) {
-            const int q = __ffs(todo) - 1;
-            todo &= todo - 1;
-            const uint32_t n = __shfl_sync(0xffffffffu, n_l, q);
-            const uint64_t o = out_base + __shfl_sync(0xffffffffu, o_l, q);
-            const uint64_t s0 = (g + q) * (uint64_t)SEG;
-            K v[PER];
+            // B segments per round (warp-uniform picks from `todo`)
+            uint32_t n[B];
+            uint64_t o[B], s0[B];
 #pragma unroll
-            for (int j = 0; j < PER; ++j) {
-                const uint32_t i = j * 32 + lane;
-                if (i < n) v[j] = keys[s0 + i];
+            for (int b = 0; b < B; ++b) {
+                const int q = todo ? __ffs(todo) - 1 : -1;
+                todo &= todo - 1;
+                const int src = q >= 0 ? q : 0;
+                const uint32_t nq = __shfl_sync(0xffffffffu, n_l, src);
+                const uint64_t oq = __shfl_sync(0xffffffffu, o_l, src);
+                n[b] = q >= 0 ? nq : 0u;
+                o[b] = out_base + oq;
+                s0[b] = (g + (uint64_t)src) * (uint64_t)SEG;
             }
+            K v[B][PER];
 #pragma unroll
-            for (int j = 0; j < PER; ++j) {
-                const uint32_t i = j * 32 + lane;
-                if (i < n) pack_key<NW>(v[j], out + (o + i) * P, full, tail_bytes, P, tmask);
-            }
+            for (int b = 0; b < B; ++b)
+#pragma unroll
+                for (int j = 0; j < PER; ++j) {
+                    const uint32_t i = j * 32 + lane;
+                    if (i < n[b]) v[b][j] = keys[s0[b] + i];
+                }
+#pragma unroll
+            for (int b = 0; b < B; ++b)
+#pragma unroll
+                for (int j = 0; j < PER; ++j) {
+                    const uint32_t i = j * 32 + lane;
+                    if (i < n[b]) pack_key<NW>(v[b][j], out + (o[b] + i) * P, full, tail_bytes, P, tmask);
+                }
         }
     }
 }
