@@ -388,8 +388,9 @@ int device_scan(kc_context* c, const TI* in, uint64_t n, TO* out, uint64_t base,
     return KC_OK;
 }
 
-// Allocate filter and tables from per-bucket k-mer totals of the first batch.
-int size_structures(kc_context* c, const std::vector<uint64_t>& kb, double scale) {
+// Allocate filter and tables from per-bucket k-mer totals of the first batch
+// (batch_bytes of FASTQ; 0 when no extraction follows).
+int size_structures(kc_context* c, const std::vector<uint64_t>& kb, double scale, uint64_t batch_bytes) {
     const kc_config& g = c->cfg;
     const uint32_t nb = c->n_buckets;
     c->h_meta.assign(nb, kc::BucketMeta{});
@@ -437,21 +438,34 @@ int size_structures(kc_context* c, const std::vector<uint64_t>& kb, double scale
     CK(c->meta.ensure(nb * sizeof(kc::BucketMeta)));
     CKR(put(c, c->meta.p, c->h_meta.data(), nb * sizeof(kc::BucketMeta)));
     {
-        // Filter and table initialisation on the side stream, after the work
-        // already queued on `stream` (a previous count may still read the
-        // table), one CTA per SM: it runs beside the extraction, which is
-        // bound by instruction issue, not by HBM; the count joins it.
-        CK(cudaEventRecord(c->ev_side_in, c->stream));
-        CK(cudaStreamWaitEvent(c->side, c->ev_side_in, 0));
-        Stage st(c, KC_STAGE_INIT, bw ? 2 : 1, c->side);
-        const int ig = c->sm_count;
-        if (bw) kc::fill_words<<<ig, 256, 0, c->side>>>(c->bloom.as<uint32_t>(), bw * 2, 0u);
-        if (c->nw == 1) kc::init_slots<1><<<ig, 256, 0, c->side>>>(c->table.p, ts);
-        else if (c->nw == 2) kc::init_slots<2><<<ig, 256, 0, c->side>>>(c->table.p, ts);
-        else kc::init_slots<4><<<ig, 256, 0, c->side>>>(c->table.p, ts);
+        // Filter and table initialisation.  When it is small against the
+        // first batch (under 4 bytes per FASTQ byte; the extraction moves
+        // ~0.33 GB of FASTQ per ms, the initialisation 2-5 GB per ms) it runs
+        // on the side stream, two CTAs per SM, after the work already queued
+        // on `stream` (a previous count may still read the table), beside
+        // the extraction, which is bound by instruction issue, not by HBM;
+        // the count joins it.  Otherwise it runs first at full width: 48 GB
+        // of 128-bit tables behind a 2 GiB batch slowed that batch's
+        // extraction and still held up the count.
+        const uint64_t init_bytes = bw * sizeof(uint64_t) + ts * c->slot_bytes;
+        const bool beside = init_bytes < 4 * batch_bytes;
+        cudaStream_t is = c->stream;
+        if (beside) {
+            CK(cudaEventRecord(c->ev_side_in, c->stream));
+            CK(cudaStreamWaitEvent(c->side, c->ev_side_in, 0));
+            is = c->side;
+        }
+        Stage st(c, KC_STAGE_INIT, bw ? 2 : 1, is);
+        const int ig = c->sm_count * (beside ? 2 : 8);
+        if (bw) kc::zero16<<<ig, 256, 0, is>>>(c->bloom.as<uint4>(), bw / 2);  // bw: a sum of powers of two >= 256
+        if (c->nw == 1) kc::init_slots<1><<<ig, 256, 0, is>>>(c->table.p, ts);
+        else if (c->nw == 2) kc::init_slots<2><<<ig, 256, 0, is>>>(c->table.p, ts);
+        else kc::init_slots<4><<<ig, 256, 0, is>>>(c->table.p, ts);
         CK(cudaGetLastError());
-        CK(cudaEventRecord(c->ev_init, c->side));
-        c->init_pending = true;
+        if (beside) {
+            CK(cudaEventRecord(c->ev_init, c->side));
+            c->init_pending = true;
+        }
     }
     CK(c->overflow.ensure(nb * sizeof(uint32_t)));
     CKR(fill_dev(c, c->overflow.p, nb * sizeof(uint32_t), 0));
@@ -651,7 +665,7 @@ int process_batch(kc_context* c, const uint8_t* buf, uint64_t n, int has_halo) {
         if (!c->sized) {
             double scale = 1.0;
             if (c->expected_total_bytes > n && n > 0) scale = (double)c->expected_total_bytes / (double)n;
-            if ((rc = size_structures(c, kest, scale))) return rc;
+            if ((rc = size_structures(c, kest, scale, n))) return rc;
         }
         if (!total_cap) return KC_OK;  // no k-mers in this batch
 
@@ -889,7 +903,7 @@ int finish_run(kc_context* c) {
     if (!c->sized) {
         // empty input: allocate minimal structures so the export is uniform
         std::vector<uint64_t> zero(c->n_buckets, 0);
-        if ((rc = size_structures(c, zero, 1.0))) return rc;
+        if ((rc = size_structures(c, zero, 1.0, 0))) return rc;
     }
     rc = c->nw == 1 ? export_tables<1>(c) : (c->nw == 2 ? export_tables<2>(c) : export_tables<4>(c));
     if (rc) return rc;

@@ -294,6 +294,12 @@ static __global__ void fill_words(uint32_t* __restrict__ dst, uint64_t n, uint32
         dst[i] = v;
 }
 
+// Zero n 16-byte units (16-byte aligned).
+static __global__ void zero16(uint4* __restrict__ dst, uint64_t n) {
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+        dst[i] = make_uint4(0u, 0u, 0u, 0u);
+}
+
 // ------------------------------------------------------- FASTQ line split
 
 // '\n' count per 8 KiB tile of the batch buf[0..n) (16-byte vector reads,
@@ -1044,16 +1050,16 @@ struct SlotOf<4> {
 // is 65536 / (256 x CTAs)).  The kernel waits on L2 round trips, so resident
 // warps hide more than items per lane: for 64-bit keys 2 items at 6 CTAs/SM
 // (40 registers) ran 42.7 ms where 4 items at 4 CTAs ran 47.4 and 6 at 3 ran
-// 58.3 (genome-scale step, same counts); for 128-bit keys 2 items at 5 CTAs
-// (48 registers) ran 13.8 ms against 14.4 at 4 CTAs and 13.9 for 1 item at 6
-// (the k=63 shape at a tenth of its size).
+// 58.3 (genome-scale step, same counts); for 128-bit keys 2 items at 4 CTAs
+// ran 233 ms where 5 CTAs (48 registers) ran 246 (the full k=63 shape, ten
+// passes over 48 GB of tables; at a tenth of that size 5 CTAs were ahead).
 template <int NW>
 __host__ __device__ constexpr int count_items() {
     return NW == 1 ? 2 : (NW == 2 ? 2 : 1);
 }
 template <int NW>
 __host__ __device__ constexpr int count_min_ctas() {
-    return NW == 1 ? 6 : (NW == 2 ? 5 : 4);
+    return NW == 1 ? 6 : (NW == 2 ? 4 : 4);
 }
 // Keys owned by one warp of the count kernel (a contiguous segment).
 template <int NW>
