@@ -153,6 +153,30 @@ int kc_count_host_stream(kc_context* ctx, const uint8_t* fastq, uint64_t n, kc_s
 /* Same, with the FASTQ already in device memory (a device pointer). */
 int kc_count_device(kc_context* ctx, const uint8_t* d_fastq, uint64_t n, kc_stats* stats);
 
+/* ---- one input over several GPUs (bucket owners) ------------------------
+ * The reference partitions its Bloom filters and trees by root prefix
+ * (key word 0 >> 56; src/FastqClassifier.h:211-240, src/main.cpp:38-86).
+ * Sharded, every GPU extracts and routes its slice of the FASTQ records, the
+ * slices' keys are exchanged so that each GPU receives the keys of a
+ * contiguous range of root prefixes (one all-to-all), and each GPU counts
+ * them: its root files are the root files of its prefixes, and the low.bin
+ * bytes of all GPUs concatenated are the input's low.bin.
+ *
+ * kc_route_device: extract and route whole 4-line records (the slice must
+ * start at a record) in device memory; the keys stay in the context, in
+ * root-prefix order, counts[256] receiving the keys per prefix (so prefix p's
+ * keys are at index sum(counts[0..p)) ).  stats: not touched.
+ * kc_copy_routed: copy those keys (8N bytes each) to dst (device or host),
+ * dst_bytes >= 8N x sum(counts).
+ * kc_count_keys_device: count n_keys canonical keys in device memory (8N
+ * bytes each, as routed, any order) as one input; counts[256] are the keys
+ * per root prefix (they size the filter and tables, and must sum to
+ * n_keys).  Results as after kc_count_device. */
+int kc_route_device(kc_context* ctx, const uint8_t* d_fastq, uint64_t n, uint64_t* counts);
+int kc_copy_routed(kc_context* ctx, void* dst, uint64_t dst_bytes);
+int kc_count_keys_device(kc_context* ctx, const void* d_keys, uint64_t n_keys, const uint64_t* counts,
+                         kc_stats* stats);
+
 /* ---- many read sets in one pass ----------------------------------------
  * Benchmark pattern "batched uneven samples": independent read sets of uneven
  * size and read length counted together -- every pipeline stage is one launch

@@ -29,7 +29,7 @@ ABI_SYMBOLS = (
     "kc_create", "kc_destroy", "kc_count_host", "kc_count_device", "kc_result_sizes", "kc_copy_low",
     "kc_copy_roots", "kc_write_outputs", "kc_device_results", "kc_host_alloc", "kc_host_free", "kc_stream",
     "kc_set_profiling", "kc_stage_times", "kc_stage_name", "kc_count_device_noalloc", "kc_count_host_stream",
-    "kc_histogram", "kc_count_sets",
+    "kc_histogram", "kc_count_sets", "kc_route_device", "kc_copy_routed", "kc_count_keys_device",
 )
 KC_SINK_LOW = 0
 KC_SINK_ROOT = 1
@@ -119,6 +119,9 @@ def _load():
         "kc_count_host_stream": (i32, [vp, vp, u64, SINK_FN, vp, stp]),
         "kc_histogram": (i32, [vp, u32, u32, C.POINTER(u64), C.POINTER(u64)]),
         "kc_count_sets": (i32, [vp, vp, C.POINTER(KcSetDesc), u32, C.POINTER(KcSetResult), stp]),
+        "kc_route_device": (i32, [vp, vp, u64, C.POINTER(u64)]),
+        "kc_copy_routed": (i32, [vp, vp, u64]),
+        "kc_count_keys_device": (i32, [vp, vp, u64, C.POINTER(u64), stp]),
         "kc_measure_peaks": (i32, [i32, u64, C.POINTER(KcPeaks)]),
     }
     for name, (res, args) in sig.items():
@@ -220,6 +223,25 @@ class Counter:
     def count_device(self, dptr, n):
         """Count FASTQ bytes already in device memory (an integer device pointer)."""
         check(lib.kc_count_device(self._ctx, C.c_void_p(dptr), n, C.byref(self.stats)))
+        return self.stats
+
+    # -- one input over several GPUs (include/kmer_count.h, bucket owners)
+    def route_device(self, dptr, n):
+        """Extract and route whole FASTQ records in device memory; returns the
+        keys per root prefix (uint64[256]); the keys stay in the context."""
+        counts = np.zeros(256, np.uint64)
+        check(lib.kc_route_device(self._ctx, C.c_void_p(dptr), n, counts.ctypes.data_as(C.POINTER(C.c_uint64))))
+        return counts
+
+    def copy_routed(self, addr, cap):
+        """Copy the routed keys (prefix order) to addr (device or host)."""
+        check(lib.kc_copy_routed(self._ctx, C.c_void_p(addr), cap))
+
+    def count_keys_device(self, dptr, n_keys, counts):
+        """Count n_keys routed canonical keys in device memory as one input."""
+        counts = np.ascontiguousarray(counts, np.uint64)
+        check(lib.kc_count_keys_device(self._ctx, C.c_void_p(dptr), n_keys,
+                                       counts.ctypes.data_as(C.POINTER(C.c_uint64)), C.byref(self.stats)))
         return self.stats
 
     def sizes(self):

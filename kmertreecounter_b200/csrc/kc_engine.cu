@@ -173,6 +173,10 @@ struct kc_context {
     DevBuf roots, chunks, chunk_pass, chunk_off, root_count;
     DevBuf pass_bits;  // export: bit per table slot that passes min..max
     uint64_t n_chunks = 0;  // entries of `chunks` (live table regions) of the last export
+    // kc_route_device: keys held in `routed` (bucket order) and per routing bucket
+    uint64_t routed_keys = 0;
+    std::vector<uint64_t> route_counts;
+    bool have_route = false;
     DevBuf sort_tmp, sort_hist, sort_offs, sort_sums;
     DevBuf set_tiles, tile_prefix, set_info;  // multi-set batches
 
@@ -590,9 +594,15 @@ int launch_extract(kc_context* c, const uint8_t* buf, uint64_t n, int has_halo, 
     return KC_OK;
 }
 
-// Count one batch of FASTQ bytes already in device memory.
 template <int NW>
-int process_batch(kc_context* c, const uint8_t* buf, uint64_t n, int has_halo) {
+int count_and_pack(kc_context* c, uint64_t n_keys, uint32_t ext_err);
+
+// Count one batch of FASTQ bytes already in device memory.  route_only:
+// route it exactly (every tile's histogram, no estimated regions) into
+// `routed`, bucket-contiguous in bucket order, and stop there (filter and
+// tables untouched; kc_route_device).
+template <int NW>
+int process_batch(kc_context* c, const uint8_t* buf, uint64_t n, int has_halo, bool route_only = false) {
     if (reinterpret_cast<uintptr_t>(buf) % 16)
         return fail(KC_ERR_INVALID, "device FASTQ batch must be 16-byte aligned");
     const uint32_t nb = c->n_buckets;
@@ -633,7 +643,7 @@ int process_batch(kc_context* c, const uint8_t* buf, uint64_t n, int has_halo) {
     constexpr int CT = kc::count_tile<NW>();
     constexpr int SEG = kc::count_seg<NW>();
     const uint32_t rb = std::min<uint32_t>(nb, 256), per = nb / rb;
-    bool est = tiles >= kc::EST_MIN_TILES;
+    bool est = tiles >= kc::EST_MIN_TILES && !route_only;
     std::vector<uint64_t> start(rb), end(rb), cursor(rb);
     uint64_t n_keys = 0, kb = 0;
     for (int attempt = 0;; ++attempt) {
@@ -651,9 +661,11 @@ int process_batch(kc_context* c, const uint8_t* buf, uint64_t n, int has_halo) {
         uint64_t total_cap = 0;
         const double f = est ? (double)tiles / (double)ceil_div(tiles, stride) : 1.0;
         for (uint32_t b = 0; b < nb; ++b) kest[b] = (uint64_t)((double)c->h_bucket_count[b] * f);
+        if (route_only) c->route_counts.assign(rb, 0);
         for (uint32_t r = 0; r < rb; ++r) {
             uint64_t exact = 0;
             for (uint32_t q = 0; q < per; ++q) exact += c->h_bucket_count[r * per + q];
+            if (route_only) c->route_counts[r] = exact;
             const double e = (double)exact * f;
             const uint64_t cap = est ? (uint64_t)(e * 1.02 + 4.0 * std::sqrt(e) + 256.0) : exact;
             start[r] = total_cap;
@@ -662,12 +674,15 @@ int process_batch(kc_context* c, const uint8_t* buf, uint64_t n, int has_halo) {
         }
         // at least 65536 keys: one CTA's run of a bucket (<= 8192 keys) always fits
         const uint64_t ovf_cap = est ? std::max<uint64_t>(1ull << 16, total_cap / 32) : 0;
-        if (!c->sized) {
+        if (!c->sized && !route_only) {
             double scale = 1.0;
             if (c->expected_total_bytes > n && n > 0) scale = (double)c->expected_total_bytes / (double)n;
             if ((rc = size_structures(c, kest, scale, n))) return rc;
         }
-        if (!total_cap) return KC_OK;  // no k-mers in this batch
+        if (!total_cap) {  // no k-mers in this batch
+            if (route_only) c->routed_keys = 0;
+            return KC_OK;
+        }
 
         const uint64_t cap_keys = total_cap + ovf_cap;
         const uint64_t ctiles = ceil_div(cap_keys, CT);
@@ -715,7 +730,23 @@ int process_batch(kc_context* c, const uint8_t* buf, uint64_t n, int has_halo) {
     if (c->after_scatter) CK(cudaEventRecord(c->after_scatter, c->stream));
     uint32_t ext_err = 0;
     CKR(get(c, &ext_err, c->scalars.as<uint32_t>() + 12, sizeof(uint32_t)));
+    if (route_only) {
+        CKR(sync_stream(c));
+        if (ext_err) return fail(KC_ERR_DEVICE, "internal error: routing bucket disagreed with its reservation");
+        c->routed_keys = n_keys;
+        return KC_OK;
+    }
+    return count_and_pack<NW>(c, n_keys, ext_err);
+}
 
+// Filter, tables and low.bin packing of the n_keys keys in `routed`
+// (EMPTY keys are skipped); ext_err is the extraction's error word, read back
+// with the count's.
+template <int NW>
+int count_and_pack(kc_context* c, uint64_t n_keys, uint32_t ext_err) {
+    constexpr int SEG = kc::count_seg<NW>();
+    uint64_t* d_scal = c->scalars.as<uint64_t>();
+    int rc;
     const uint64_t nsegs = ceil_div(n_keys, SEG);
     launch_count<NW>(c, n_keys, 1);
     CK(cudaGetLastError());
@@ -1060,6 +1091,36 @@ int run_batch(kc_context* c, const uint8_t* buf, uint64_t n, int has_halo) {
     return process_batch<4>(c, buf, n, has_halo);
 }
 
+// Count n_keys canonical keys already extracted and routed elsewhere (the
+// owner side of a sharded count): size from the per-routing-bucket totals,
+// copy the keys into `routed`, then filter, tables and packing as for a
+// batch of FASTQ.
+template <int NW>
+int count_keys(kc_context* c, const void* d_keys, uint64_t n_keys, const uint64_t* counts) {
+    constexpr int CT = kc::count_tile<NW>();
+    constexpr int SEG = kc::count_seg<NW>();
+    const uint32_t nb = c->n_buckets;
+    const uint32_t per = nb / 256;  // table buckets per routing bucket (1 or 16)
+    std::vector<uint64_t> kest(nb);
+    for (uint32_t b = 0; b < nb; ++b) {
+        const uint64_t r = counts[b / per];
+        kest[b] = r / per + ((b % per) < (r % per) ? 1 : 0);
+    }
+    int rc;
+    if ((rc = size_structures(c, kest, 1.0, 0))) return rc;
+    const uint64_t ctiles = ceil_div(n_keys, CT);
+    CK(c->routed.ensure(ctiles * CT * (uint64_t)(8 * NW)));
+    CK(c->tile_low.ensure(ctiles * (CT / SEG) * sizeof(uint32_t)));
+    CK(c->tile_fail.ensure(ctiles * (CT / SEG) * sizeof(uint32_t)));
+    CK(c->tile_low_prefix.ensure(ctiles * (CT / SEG) * sizeof(uint64_t)));
+    CK(c->scalars.ensure(64));
+    CKR(fill_dev(c, c->scalars.as<uint32_t>() + 12, 2 * sizeof(uint32_t), 0));
+    CK(cudaMemcpyAsync(c->routed.p, d_keys, n_keys * (uint64_t)(8 * NW), cudaMemcpyDefault, c->stream));
+    c->K += n_keys;
+    c->batches++;
+    return count_and_pack<NW>(c, n_keys, 0);
+}
+
 }  // namespace
 
 // ------------------------------------------------------------------ C ABI
@@ -1314,6 +1375,67 @@ int host_pipeline(kc_context* c, const uint8_t* fastq, uint64_t n) {
         if (rc) return rc;
         if (c->stream_low && (rc = stream_out_low(c))) return rc;
     }
+    return KC_OK;
+}
+
+int kc_route_device(kc_context* c, const uint8_t* d_fastq, uint64_t n, uint64_t* counts) {
+    if (!c || (!d_fastq && n) || !counts) return fail(KC_ERR_INVALID, "null argument");
+    int rc = begin_run(c, n);
+    if (rc) return rc;
+    c->have_route = false;
+    c->routed_keys = 0;
+    c->route_counts.assign(256, 0);
+    if (n) {
+        c->batches = 1;
+        c->input_bytes = n;
+        rc = c->nw == 1 ? process_batch<1>(c, d_fastq, n, 0, true)
+                        : (c->nw == 2 ? process_batch<2>(c, d_fastq, n, 0, true) : process_batch<4>(c, d_fastq, n, 0, true));
+        if (rc) return rc;
+    }
+    CKR(sync_stream(c));
+    collect_stage_times(c);
+    for (int r = 0; r < 256; ++r) counts[r] = r < (int)c->route_counts.size() ? c->route_counts[r] : 0;
+    c->have_route = true;
+    return KC_OK;
+}
+
+int kc_copy_routed(kc_context* c, void* dst, uint64_t cap) {
+    if (!c) return fail(KC_ERR_INVALID, "null context");
+    if (!c->have_route) return fail(KC_ERR_STATE, "no routed keys: call kc_route_device first");
+    const uint64_t bytes = c->routed_keys * 8ull * c->nw;
+    if (!bytes) return KC_OK;
+    if (!dst || cap < bytes) return fail(KC_ERR_INVALID, "destination holds %llu bytes, %llu needed",
+                                         (unsigned long long)cap, (unsigned long long)bytes);
+    CK(cudaMemcpyAsync(dst, c->routed.p, bytes, cudaMemcpyDefault, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    return KC_OK;
+}
+
+int kc_count_keys_device(kc_context* c, const void* d_keys, uint64_t n_keys, const uint64_t* counts,
+                         kc_stats* stats) {
+    if (!c || (!d_keys && n_keys) || !counts) return fail(KC_ERR_INVALID, "null argument");
+    uint64_t total = 0;
+    for (int r = 0; r < 256; ++r) total += counts[r];
+    if (total != n_keys) return fail(KC_ERR_INVALID, "bucket counts sum to %llu, not n_keys = %llu",
+                                     (unsigned long long)total, (unsigned long long)n_keys);
+    const auto t0 = std::chrono::steady_clock::now();
+    int rc = begin_run(c, 0);
+    if (rc) return rc;
+    c->have_route = false;  // `routed` is overwritten
+    CK(cudaEventRecord(c->ev0, c->stream));
+    if (n_keys) {
+        rc = c->nw == 1 ? count_keys<1>(c, d_keys, n_keys, counts)
+                        : (c->nw == 2 ? count_keys<2>(c, d_keys, n_keys, counts) : count_keys<4>(c, d_keys, n_keys, counts));
+        if (rc) return rc;
+    }
+    if ((rc = finish_run(c))) return rc;
+    CK(cudaEventRecord(c->ev1, c->stream));
+    CK(cudaEventSynchronize(c->ev1));
+    collect_stage_times(c);
+    float ms = 0;
+    cudaEventElapsedTime(&ms, c->ev0, c->ev1);
+    const double wall = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    fill_stats(c, stats, ms, wall);
     return KC_OK;
 }
 
