@@ -976,28 +976,6 @@ __device__ __forceinline__ bool table_add(Slot4* tab, uint64_t mask, uint64_t h,
     return table_add4(tab, mask, h, key, add) > 0;
 }
 
-// First probe already read (`seen`): settle the common cases inline -- the
-// slot holds the key (add), or is empty (claim, add) -- else walk on.
-__device__ __forceinline__ bool table_add_first(Slot1* tab, uint64_t mask, uint64_t h, uint64_t key, uint32_t add,
-                                                uint64_t seen) {
-    Slot1* s = tab + ((h >> 17) & mask);
-    if (seen == EMPTY) seen = atomicCAS(reinterpret_cast<unsigned long long*>(&s->key), EMPTY, key), seen = seen == EMPTY ? key : seen;
-    if (seen == key) {
-        atomicAdd(&s->count, add);
-        return true;
-    }
-    return table_add_slow(tab, mask, h, key, add, 1);
-}
-__device__ __forceinline__ bool table_add_first(Slot2* tab, uint64_t mask, uint64_t h, const Key2& key, uint32_t add,
-                                                ulonglong2 seen) {
-    Slot2* s = tab + ((h >> 17) & mask);
-    if (seen.x == key.w0 && seen.y == key.w1) {
-        atomicAdd(&s->count, add);
-        return true;
-    }
-    return table_add_slow(tab, mask, h, key, add, 0);
-}
-
 // Probe-round helpers of count_routed (64- and 128-bit keys): a cell's key
 // as read (16-byte reads of a 128-bit cell may be torn while it is claimed:
 // any EMPTY half counts as empty and is settled by the CAS), the claim of a
@@ -1023,12 +1001,6 @@ __device__ __forceinline__ ulonglong2 claim_cell(Slot2* s, const Key2& key) {
     const unsigned __int128 old = atomicCAS(reinterpret_cast<unsigned __int128*>(s), e, kv);
     const unsigned __int128 now = old == e ? kv : old;
     return make_ulonglong2((uint64_t)now, (uint64_t)(now >> 64));
-}
-
-__device__ __forceinline__ bool key_eq(uint64_t a, uint64_t b) { return a == b; }
-__device__ __forceinline__ bool key_eq(const Key2& a, const Key2& b) { return a.w0 == b.w0 && a.w1 == b.w1; }
-__device__ __forceinline__ bool key_eq(const Key4& a, const Key4& b) {
-    return a.w0 == b.w0 && a.w1 == b.w1 && a.w2 == b.w2 && a.w3 == b.w3;
 }
 
 template <int NW>
