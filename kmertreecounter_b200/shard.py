@@ -18,9 +18,10 @@ so no k-mer spans two slices and every rank reads its slice as a file of its
 own.
 
 Collectives, in this order on every rank (also when a rank failed, so that no
-rank waits for good): all_gather_object (routing errors), all_reduce (prefix
-counts), all_to_all_single (split sizes), all_to_all_single (keys),
-all_gather_object (counting errors), barrier (before the merge).
+rank waits for good): broadcast_object_list (the slice cuts, found by rank
+0), all_gather_object (routing errors), all_reduce (prefix counts),
+all_to_all_single (split sizes), all_to_all_single (keys), all_gather_object
+(counting errors), barrier (before the merge).
 
     python -m torch.distributed.run --nproc-per-node 8 --master-addr 127.0.0.1 \\
         -m kmertreecounter_b200.shard --k 31 --out out/ reads.fq
@@ -195,7 +196,9 @@ def main():
     dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
     try:
         data = np.memmap(a.file, np.uint8, mode="r")
-        cuts = record_starts(data, world)
+        cuts = [record_starts(data, world) if rank == 0 else None]  # one scan of the file, not one per rank
+        dist.broadcast_object_list(cuts, src=0)
+        cuts = cuts[0]
         t0 = time.perf_counter()
         with Counter(k=a.k, min_count=a.min_count, max_count=a.max_count, device=local) as c:
             route, count, nw = gpu_stages(c, data[cuts[rank]:cuts[rank + 1]], torch.device("cuda", local))
