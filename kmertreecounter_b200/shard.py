@@ -196,9 +196,16 @@ def main():
     dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
     try:
         data = np.memmap(a.file, np.uint8, mode="r")
-        cuts = [record_starts(data, world) if rank == 0 else None]  # one scan of the file, not one per rank
-        dist.broadcast_object_list(cuts, src=0)
-        cuts = cuts[0]
+        msg = [None]  # one scan of the file (rank 0), not one per rank; its failure reaches every rank
+        if rank == 0:
+            try:
+                msg[0] = ("ok", record_starts(data, world))
+            except Exception as e:
+                msg[0] = ("err", f"rank 0: slicing {a.file}: {e}")
+        dist.broadcast_object_list(msg, src=0)
+        if msg[0][0] != "ok":
+            raise RuntimeError(msg[0][1])
+        cuts = msg[0][1]
         t0 = time.perf_counter()
         with Counter(k=a.k, min_count=a.min_count, max_count=a.max_count, device=local) as c:
             route, count, nw = gpu_stages(c, data[cuts[rank]:cuts[rank + 1]], torch.device("cuda", local))
