@@ -211,6 +211,7 @@ def main():
             route, count, nw = gpu_stages(c, data[cuts[rank]:cuts[rank + 1]], torch.device("cuda", local))
             st, ranges, _ = exchange_and_count(route, count, nw, torch.device("cuda", local), dist)
             part = os.path.join(a.out, f".rank{rank}")
+            os.makedirs(part, exist_ok=True)
             c.write_outputs(part)
         dist.barrier()
         wall = time.perf_counter() - t0

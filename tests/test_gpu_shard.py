@@ -105,3 +105,31 @@ def test_two_owners_on_one_gpu_match_the_oracle(k, tmp_path):
     wk, wc, K = oracle.count(data, k)
     assert int(glob.sum()) == K
     assert np.array_equal(mk, wk) and np.array_equal(mc, wc.astype(np.uint64))
+
+
+def test_shard_command_line_one_rank(tmp_path):
+    """The command line end to end under torch.distributed.run with one rank
+    (NCCL collectives over one GPU, no peer): merged output == oracle."""
+    import os
+    import socket
+    import subprocess
+    import sys
+    data = synth.fastq(synth.plain_small(seed=44, scale=0.05))
+    path = tmp_path / "reads.fq"
+    data.tofile(path)
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    out = tmp_path / "out"
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", "--nproc-per-node", "1", "--master-addr",
+           "127.0.0.1", "--master-port", str(port), "-m", "kmertreecounter_b200.shard", "--k", "31", "--out", str(out),
+           str(path)]
+    p = subprocess.run(cmd, cwd=root, capture_output=True, text=True, timeout=300,
+                       env=dict(os.environ, PYTHONPATH=root + os.pathsep + os.environ.get("PYTHONPATH", "")))
+    assert p.returncode == 0, p.stderr[-2000:]
+    low, roots, _ = oracle.read_outputs(str(out), 31)
+    mk, mc = oracle.merged_counts(low, roots["key"].reshape(-1, 1), roots["count"], nw=1)
+    wk, wc, K = oracle.count(data, 31)
+    assert np.array_equal(mk, wk) and np.array_equal(mc, wc.astype(np.uint64))
+    assert '"total_kmers": %d' % K in p.stdout
