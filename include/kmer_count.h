@@ -165,7 +165,9 @@ int kc_count_device(kc_context* ctx, const uint8_t* d_fastq, uint64_t n, kc_stat
  * kc_route_device: extract and route whole 4-line records (the slice must
  * start at a record) in device memory; the keys stay in the context, in
  * root-prefix order, counts[256] receiving the keys per prefix (so prefix p's
- * keys are at index sum(counts[0..p)) ).  stats: not touched.
+ * keys are at index sum(counts[0..p)) ).  The slice is routed in one pass
+ * (device_batch_bytes does not split it): its keys take 8N bytes per k-mer,
+ * about 2.5N times the slice's FASTQ bytes for 150 bp reads.
  * kc_copy_routed: copy those keys (8N bytes each) to dst (device or host),
  * dst_bytes >= 8N x sum(counts).
  * kc_count_keys_device: count n_keys canonical keys in device memory (8N
