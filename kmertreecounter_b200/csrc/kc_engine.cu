@@ -172,6 +172,7 @@ struct kc_context {
     DevBuf low_packed;
     DevBuf roots, chunks, chunk_pass, chunk_off, root_count;
     DevBuf pass_bits;  // export: bit per table slot that passes min..max
+    DevBuf loads;      // kc_bucket_loads: per-model-bucket totals (kept: no cudaMalloc/cudaFree per call)
     uint64_t n_chunks = 0;  // entries of `chunks` (live table regions) of the last export
     // kc_route_device: keys held in `routed` (bucket order) and per routing bucket
     uint64_t routed_keys = 0;
@@ -1233,7 +1234,7 @@ void kc_destroy(kc_context* c) {
                       &c->tile_low, &c->tile_fail, &c->tile_low_prefix, &c->scan_sums, &c->scalars, &c->overflow,
                       &c->meta,   &c->bloom,     &c->table,     &c->low_packed,   &c->roots,         &c->chunks,
                       &c->root_count, &c->chunk_pass, &c->chunk_off, &c->sort_tmp, &c->sort_hist, &c->sort_offs, &c->sort_sums,
-                      &c->set_tiles, &c->tile_prefix, &c->set_info, &c->pass_bits};
+                      &c->set_tiles, &c->tile_prefix, &c->set_info, &c->pass_bits, &c->loads};
     for (DevBuf* b : bufs) b->release();
     for (cudaEvent_t e : c->ev_pool) cudaEventDestroy(e);
     if (c->h2d) cudaStreamSynchronize(c->h2d);
@@ -1674,9 +1675,8 @@ extern "C" int kc_bucket_loads(kc_context* c, uint64_t* distinct, uint64_t* tabl
     if (!c->have_result) return fail(KC_ERR_STATE, "no result: run a count first");
     if (c->batch_result) return fail(KC_ERR_STATE, "not available for a multi-set result");
     if (c->stream_low) return fail(KC_ERR_STATE, "streamed results are not kept on the device");
-    DevBuf d;
-    CK(d.ensure(3 * KC_MODEL_BUCKETS * sizeof(unsigned long long)));
-    unsigned long long* dd = d.as<unsigned long long>();
+    CK(c->loads.ensure(3 * KC_MODEL_BUCKETS * sizeof(unsigned long long)));
+    unsigned long long* dd = c->loads.as<unsigned long long>();
     CK(cudaMemsetAsync(dd, 0, 3 * KC_MODEL_BUCKETS * sizeof(unsigned long long), c->stream));
     if (c->nw == 1) loads_kernels<1>(c, dd);
     else if (c->nw == 2) loads_kernels<2>(c, dd);
@@ -1685,7 +1685,6 @@ extern "C" int kc_bucket_loads(kc_context* c, uint64_t* distinct, uint64_t* tabl
     std::vector<unsigned long long> h(3 * KC_MODEL_BUCKETS);
     CK(cudaMemcpyAsync(h.data(), dd, h.size() * sizeof(unsigned long long), cudaMemcpyDeviceToHost, c->stream));
     CK(cudaStreamSynchronize(c->stream));
-    d.release();
     for (int i = 0; i < KC_MODEL_BUCKETS; ++i) {
         if (distinct) distinct[i] = h[i];
         if (table_keys) table_keys[i] = h[KC_MODEL_BUCKETS + i];
