@@ -1679,16 +1679,33 @@ __global__ void __launch_bounds__(EXP_THREADS) export_write(const void* table, c
     }
 }
 
-// export_write over the passing-slot bitmap of export_count: a thread owns
-// two words (64 consecutive slots) per round, threads in order, so records
-// keep table order (the order export_write produces); only passing slots are
-// read, up to 8 of them in flight per thread.
+// Position of the r-th (0-based) set bit of x, by halving with popcounts;
+// always 0..31.
+__device__ __forceinline__ uint32_t nth_set_bit(uint32_t x, uint32_t r) {
+    uint32_t pos = 0, c;
+    c = __popc(x & 0xFFFFu);
+    if (r >= c) { r -= c; pos += 16; x >>= 16; }
+    c = __popc(x & 0xFFu);
+    if (r >= c) { r -= c; pos += 8; x >>= 8; }
+    c = __popc(x & 0xFu);
+    if (r >= c) { r -= c; pos += 4; x >>= 4; }
+    c = __popc(x & 0x3u);
+    if (r >= c) { r -= c; pos += 2; x >>= 2; }
+    if (r >= (x & 1u)) pos += 1;
+    return pos;
+}
+
+// export_write over the passing-slot bitmap of export_count.  Per round a
+// warp covers 32 bitmap words (1024 slots) and lane l of each pass takes the
+// warp's l-th passing slot: the owning word by a binary search over the
+// lanes' running popcounts, the bit by nth_set_bit.  Every lane reads one slot per
+// pass and consecutive lanes write consecutive records, in table order (the
+// order export_write produces).
 template <int NW>
 __global__ void __launch_bounds__(EXP_THREADS) export_write_bits(const void* table, const uint32_t* pass_bits,
                                                                  const ExportChunk* chunks, uint64_t n_chunks,
                                                                  const uint64_t* chunk_off, uint8_t* records) {
     using S = typename SlotOf<NW>::T;
-    constexpr int BATCH = 8;
     __shared__ uint32_t s_warp[EXP_THREADS / 32];
     const S* tab = reinterpret_cast<const S*>(table);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -1697,21 +1714,17 @@ __global__ void __launch_bounds__(EXP_THREADS) export_write_bits(const void* tab
         const uint64_t w0 = ch.slot_begin >> 5;
         const uint32_t nw = ch.n_slots >> 5;
         uint64_t out = chunk_off[c];
-        for (uint32_t r0 = 0; r0 < nw; r0 += 2 * EXP_THREADS) {
-            const uint32_t wi = r0 + 2 * threadIdx.x;
-            const uint64_t cell0 = (w0 + wi) << 5;
-            uint64_t m = 0;
-            if (wi < nw) m = __ldcg(pass_bits + w0 + wi);
-            if (wi + 1 < nw) m |= (uint64_t)__ldcg(pass_bits + w0 + wi + 1) << 32;
-            // block-wide exclusive scan of the per-thread record counts
-            const uint32_t mine = __popcll(m);
-            uint32_t incl = mine;
+        for (uint32_t r0 = 0; r0 < nw; r0 += EXP_THREADS) {
+            const uint32_t wi = r0 + threadIdx.x;
+            const uint32_t m = wi < nw ? __ldcg(pass_bits + w0 + wi) : 0u;
+            uint32_t incl = __popc(m);  // warp-inclusive running count
 #pragma unroll
             for (int o = 1; o < 32; o <<= 1) {
                 const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
                 if (lane >= o) incl += y;
             }
-            if (lane == 31) s_warp[warp] = incl;
+            const uint32_t wtot = __shfl_sync(0xffffffffu, incl, 31);
+            if (lane == 31) s_warp[warp] = wtot;
             __syncthreads();
             uint32_t before = 0, total = 0;
 #pragma unroll
@@ -1721,21 +1734,27 @@ __global__ void __launch_bounds__(EXP_THREADS) export_write_bits(const void* tab
                 total += t;
             }
             __syncthreads();  // s_warp is rewritten next round
-            uint64_t r = out + before + incl - mine;
-            while (m) {
-                int b[BATCH];
+            const uint64_t base = out + before;
+            const uint64_t cell_w = (w0 + r0 + (uint32_t)warp * 32) << 5;  // first slot of lane 0's word
+            for (uint32_t n0 = 0; n0 < wtot; n0 += 32) {
+                const uint32_t n = n0 + lane;
+                // owner lane q: the first lane whose running count exceeds n
+                uint32_t lo = 0, hi = 31;
 #pragma unroll
-                for (int j = 0; j < BATCH; ++j) {
-                    b[j] = m ? __ffsll(m) - 1 : -1;
-                    m &= m - 1;
+                for (int step = 0; step < 5; ++step) {
+                    const uint32_t mid = (lo + hi) >> 1;
+                    const uint32_t v = __shfl_sync(0xffffffffu, incl, mid);
+                    if (v > n) hi = mid;
+                    else lo = mid + 1;
                 }
-                S v[BATCH];
-#pragma unroll
-                for (int j = 0; j < BATCH; ++j)
-                    if (b[j] >= 0) v[j] = tab[cell0 + b[j]];
-#pragma unroll
-                for (int j = 0; j < BATCH; ++j)
-                    if (b[j] >= 0) write_record<NW>(records, r++, v[j]);
+                const uint32_t q = lo;
+                const uint32_t mq = __shfl_sync(0xffffffffu, m, q);
+                const uint32_t eq = __shfl_sync(0xffffffffu, incl, q) - __popc(mq);  // passing slots before word q
+                if (n < wtot) {
+                    const uint32_t bit = nth_set_bit(mq, n - eq);
+                    const S v = tab[cell_w + ((uint64_t)q << 5) + bit];
+                    write_record<NW>(records, base + n, v);
+                }
             }
             out += total;
         }
