@@ -47,6 +47,29 @@ KC_HD uint64_t brev64(uint64_t x) {
     return ((uint64_t)brev32((uint32_t)x) << 32) | brev32((uint32_t)(x >> 32));
 #endif
 }
+KC_HD uint32_t popc32(uint32_t x) {
+#ifdef __CUDA_ARCH__
+    return (uint32_t)__popc(x);
+#else
+    return (uint32_t)__builtin_popcount(x);
+#endif
+}
+
+// Position of the r-th (0-based) set bit of x, by halving with popcounts;
+// always 0..31 (the export's bitmap walk).
+KC_HD uint32_t nth_set_bit(uint32_t x, uint32_t r) {
+    uint32_t pos = 0, c;
+    c = popc32(x & 0xFFFFu);
+    if (r >= c) { r -= c; pos += 16; x >>= 16; }
+    c = popc32(x & 0xFFu);
+    if (r >= c) { r -= c; pos += 8; x >>= 8; }
+    c = popc32(x & 0xFu);
+    if (r >= c) { r -= c; pos += 4; x >>= 4; }
+    c = popc32(x & 0x3u);
+    if (r >= c) { r -= c; pos += 2; x >>= 2; }
+    if (r >= (x & 1u)) pos += 1;
+    return pos;
+}
 
 constexpr int EXT_THREADS = 256;                     // extraction CTA
 constexpr int EXT_BPT = 32;                          // bytes per thread
@@ -1677,22 +1700,6 @@ __global__ void __launch_bounds__(EXP_THREADS) export_write(const void* table, c
             out += total;
         }
     }
-}
-
-// Position of the r-th (0-based) set bit of x, by halving with popcounts;
-// always 0..31.
-__device__ __forceinline__ uint32_t nth_set_bit(uint32_t x, uint32_t r) {
-    uint32_t pos = 0, c;
-    c = __popc(x & 0xFFFFu);
-    if (r >= c) { r -= c; pos += 16; x >>= 16; }
-    c = __popc(x & 0xFFu);
-    if (r >= c) { r -= c; pos += 8; x >>= 8; }
-    c = __popc(x & 0xFu);
-    if (r >= c) { r -= c; pos += 4; x >>= 4; }
-    c = __popc(x & 0x3u);
-    if (r >= c) { r -= c; pos += 2; x >>= 2; }
-    if (r >= (x & 1u)) pos += 1;
-    return pos;
 }
 
 // export_write over the passing-slot bitmap of export_count.  Per round a

@@ -8,7 +8,8 @@
 //     C = complemented bases in read order, both left-aligned,
 //   * bucket_of_window() equals the top bits of that canonical key (k <= 64),
 //   * for k = 65..128: window_at4() and canonical4() the same way, and
-//     runs_at_least5() marks exactly the bytes that end k consecutive bases.
+//     runs_at_least5() marks exactly the bytes that end k consecutive bases,
+//   * nth_set_bit() finds every set bit of random words in order.
 #include <cstdio>
 #include <cstdint>
 #include <cstdlib>
@@ -106,9 +107,31 @@ static long check_long_keys(std::mt19937_64& rng) {
     return checks;
 }
 
+// nth_set_bit (the export's bitmap walk) against a plain enumeration.
+static long check_nth_set_bit(std::mt19937_64& rng) {
+    long checks = 0;
+    for (int t = 0; t < 100000; ++t) {
+        uint32_t x = (uint32_t)rng();
+        if (t % 3 == 0) x &= (uint32_t)rng();
+        if (t % 7 == 0) x = t % 14 ? 0xFFFFFFFFu : 0u;
+        uint32_t r = 0;
+        for (uint32_t b = 0; b < 32; ++b) {
+            if (!((x >> b) & 1u)) continue;
+            if (nth_set_bit(x, r) != b) {
+                std::printf("nth_set_bit mismatch x=%08x r=%u\n", x, r);
+                std::exit(1);
+            }
+            ++r;
+            ++checks;
+        }
+    }
+    return checks;
+}
+
 int main() {
     std::mt19937_64 rng(12345);
     long checks = 0;
+    checks += check_nth_set_bit(rng);
     for (int iter = 0; iter < 20000; ++iter) {
         // three 32-byte segments of codes, byte 0 of each in bits 63..62
         std::vector<int> bases(96);
