@@ -11,10 +11,13 @@
 //                       on the routed array, bucket by bucket:     filter and
 //                       the working set of in-flight CTAs stays    tables stay
 //                       within one or two buckets, i.e. in L2      L2-resident)
-//   retry_failed        re-insert keys whose table overflowed, after the host
-//                       grew that bucket's table (rehash)
+//   rehash_bucket,      after the host grew an overflowed bucket's table:
+//   count_routed        move its keys, then re-insert the keys that met the
+//     (table only)      full table
 //   pack_low            first occurrences -> packed low.bin bytes
-//   export_{count,write} table slots -> ExportRecord<N> grouped by root id
+//   export_count,       table slots -> ExportRecord<N> grouped by root id
+//   export_write_bits   (per-chunk counts and a bitmap of passing slots, then
+//                       one read of only those slots)
 //
 // Reference semantics are restated in the comments of each kernel with the
 // file:line of ScorchShana/KmerTreeCounter they follow.
