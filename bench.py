@@ -58,11 +58,17 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-peaks", action="store_true", help="skip the atomic/link microbenchmark")
-    ap.add_argument("--sample-scale", type=float, default=0.05, help="CPU sample size, fraction of the workload")
+    ap.add_argument("--sample-scale", type=float, default=0.1, help="CPU sample size, fraction of the workload")
     ap.add_argument("--batch-scale", type=float, default=0.05,
                     help="read-set batch comparison: shrink genomes and read counts of the 512 sets")
     ap.add_argument("--no-batched", action="store_true")
     ap.add_argument("--no-sizing", action="store_true", help="skip the learned-vs-sampled sizing comparison")
+    ap.add_argument("--no-large-long", action="store_true",
+                    help="skip the long-key record (200 Mbp, 50x, k=63, 4096 buckets) of the default run")
+    ap.add_argument("--ll-steps", type=int, default=3, help="timed steps of the long-key record")
+    ap.add_argument("--no-file-to-file", action="store_true",
+                    help="skip the command-line leg (bin/Tree vs the reference's Tree on the same file)")
+    ap.add_argument("--write-sample", metavar="PATH", help=argparse.SUPPRESS)
     return ap.parse_args()
 
 
@@ -138,6 +144,13 @@ class ClockSampler:
 
 # --------------------------------------------------------------- workload
 
+DESCRIBE = {
+    "genome_scale": "genome_scale: 100 Mbp genome 45% GC 20% repeats, 30x 150 bp (20M reads), k=31",
+    "large_long": "large_long: 200 Mbp genome 40% GC 30% repeats, 50x 150 bp (66.7M reads), k=63, 4096 buckets",
+    "plain_small": "plain_small: 5 Mbp genome, 100k x 150 bp, k=31",
+}
+
+
 def make_workload(name, scale):
     from kmertreecounter_b200 import synth
     preset, k, buckets = WORKLOADS[name]
@@ -146,15 +159,63 @@ def make_workload(name, scale):
     return p, k, buckets, bases
 
 
-def cpu_sample(name, sample_scale, workdir):
-    """Write a bounded sample of the workload (same shape, shrunken) to disk."""
+def workload_config(args, world, fastq_bytes, bases, reads):
+    """The `config` object of both arms' lines (the reference arm reports our
+    arm's config: its steps are bounded samples of this workload)."""
+    k, buckets = WORKLOADS[args.workload][1:]
+    name = DESCRIBE[args.workload] if args.scale == 1.0 else f"{args.workload} scale={args.scale}"
+    return {"workload": name, "k": k, "n_buckets": buckets, "fastq_bytes": int(fastq_bytes), "bases": int(bases),
+            "reads": int(reads), "l2": "inputs larger than L2 (FASTQ %.1f GB)" % (fastq_bytes / 1e9),
+            "parallelism": f"replica x{world}"}
+
+
+def write_sample(name, scale, path):
+    """Child-process mode (`bench.py --write-sample`): write a bounded sample
+    of the workload (same shape, genome and reads shrunk together) to `path`
+    and print the sample's and the full workload's sizes as JSON.  Run in a
+    short-lived child so that the process timing the reference maps none of
+    the counter's libraries."""
     from kmertreecounter_b200 import synth
     preset, k, _ = WORKLOADS[name]
-    p = getattr(synth, preset)(scale=sample_scale)
+    p = getattr(synth, preset)(scale=scale)
     data = synth.fastq(p)
-    path = os.path.join(workdir, "sample.fastq")
     data.tofile(path)
-    return path, data, k, int(p.n_reads) * int(p.read_len_min), p
+    full = getattr(synth, preset)(scale=1.0)
+    print(json.dumps({"path": path, "k": k, "bytes": int(data.size), "bases": int(p.n_reads) * int(p.read_len_min),
+                      "reads": int(p.n_reads), "genome_len": int(p.genome_len),
+                      "full": {"fastq_bytes": synth.fastq_bytes(full),
+                               "bases": int(full.n_reads) * int(full.read_len_min), "reads": int(full.n_reads)}}))
+
+
+def cpu_sample(name, sample_scale, workdir):
+    """Bounded sample of the workload on disk, written by a child process:
+    (path, the sample bytes, k, sample bases, description dict)."""
+    path = os.path.join(workdir, "sample.fastq")
+    out = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--write-sample", path,
+                          "--workload", name, "--sample-scale", str(sample_scale)],
+                         capture_output=True, text=True, check=True)
+    info = json.loads(out.stdout.strip().splitlines()[-1])
+    data = np.fromfile(path, dtype=np.uint8)
+    return path, data, info["k"], info["bases"], info
+
+
+def host_facts():
+    """Host cores, memory and CPU model, for the CPU lines."""
+    model = None
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    model = line.split(":", 1)[1].strip()
+                    break
+    except OSError:
+        pass
+    try:
+        ram = os.sysconf("SC_PAGE_SIZE") * os.sysconf("SC_PHYS_PAGES")
+    except (ValueError, OSError):
+        ram = None
+    return {"cores": len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count(),
+            "cpu_model": model, "ram_gb": round(ram / 2**30, 1) if ram else None}
 
 
 def time_reference(path, data, k, bases, runs, workdir):
@@ -162,8 +223,8 @@ def time_reference(path, data, k, bases, runs, workdir):
     (Gbases/s, seconds), kind, cores."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle
-    cores = os.cpu_count() or 1
-    K_expected = oracle.extract(data, k).shape[0]
+    cores = host_facts()["cores"] or 1
+    K_expected = oracle.total_kmers(data, k)
     out = []
     if os.path.exists(oracle.REF_TREE):
         kind = "reference"
@@ -190,19 +251,34 @@ def time_reference(path, data, k, bases, runs, workdir):
     return out, kind, cores
 
 
+# DRAM traffic (dram__bytes_read.sum + dram__bytes_write.sum) of the count
+# kernel per step of the genome-scale workload, from one ncu capture of the
+# kernel sources whose sha256 is given (the capture and its command are
+# summarised in profiles/count_routed_genome_scale.md).  Reported only while
+# the kernel sources are unchanged since that capture.
+PROFILED_TRAFFIC = {
+    "genome_scale": {"sources_sha256": None, "bytes_per_step": None},
+}
+KERNEL_SOURCES = ("kmertreecounter_b200/csrc/kc_kernels.cuh", "kmertreecounter_b200/csrc/kc_engine.cu")
+
+
+def kernel_sources_sha256():
+    import hashlib
+    h = hashlib.sha256()
+    for rel in KERNEL_SOURCES:
+        with open(os.path.join(ROOT, rel), "rb") as f:
+            h.update(f.read())
+    return h.hexdigest()
+
+
 def profile_traffic(args):
-    """DRAM bytes (read + write) of count_routed per step from the committed
-    ncu summary of this workload (profiles/count_routed_genome_scale.md)."""
-    if args.workload != "genome_scale" or args.scale != 1.0:
-        return None
-    try:
-        with open(os.path.join(ROOT, "profiles", "count_routed_genome_scale.md")) as f:
-            for line in f:
-                if line.startswith("traffic_bytes_per_step:"):
-                    return int(line.split(":")[1])
-    except OSError:
-        pass
-    return None
+    """(traffic bytes per step or None, note)."""
+    e = PROFILED_TRAFFIC.get(args.workload)
+    if not e or args.scale != 1.0 or not e["bytes_per_step"]:
+        return None, "no capture of this workload"
+    if e["sources_sha256"] != kernel_sources_sha256():
+        return None, "kernel sources changed since the last capture"
+    return e["bytes_per_step"], "ncu capture of these kernel sources"
 
 
 def pipeline_roofline(dev_peaks, pk, F, K, L, R, P, rec, ms_step, count_ms):
@@ -306,7 +382,7 @@ def compare_batched(args, kc, torch):
             "speedup": plain_ms / batched_ms, "kmers": int(sum(r.total_kmers for r in res))}
 
 
-def compare_sizing(args, kc, torch, dev, n, k, buckets):
+def compare_sizing(args, kc, torch, dev, n, k, buckets, device_batch=None, steps=None):
     """Learned vs sampled sizing on the same resident FASTQ, each timed end to
     end per step by wall clock on its own context (every count call returns
     synchronised).  A learned step counts the first 1% of the reads (plain
@@ -323,7 +399,9 @@ def compare_sizing(args, kc, torch, dev, n, k, buckets):
     for rule in ("sampled", "learned"):
         mode = kc.KC_SIZING_LEARNED if rule == "learned" else kc.KC_SIZING_SAMPLED
         cfg = kc.default_config(k=k, n_buckets=buckets, sizing=mode)
-        if args.workload in DEVICE_BATCH:
+        if device_batch:
+            cfg.device_batch_bytes = device_batch
+        elif args.workload in DEVICE_BATCH:
             cfg.device_batch_bytes = DEVICE_BATCH[args.workload]
         with kc.Counter(cfg) as c:
             def step():
@@ -332,7 +410,7 @@ def compare_sizing(args, kc, torch, dev, n, k, buckets):
                 return c.count_device(dev.data_ptr(), n)
             step()
             times = []
-            for _ in range(max(args.steps, 1)):
+            for _ in range(max(steps or args.steps, 1)):
                 torch.cuda.synchronize()
                 t = time.perf_counter()
                 st = step()
@@ -343,6 +421,97 @@ def compare_sizing(args, kc, torch, dev, n, k, buckets):
     out["identical_counts"] = bool(np.array_equal(hist["sampled"][0], hist["learned"][0])
                                    and hist["sampled"][1] == hist["learned"][1])
     out["margin"] = model.margin
+    return out
+
+
+def large_long_record(args, kc, torch, dev_peaks, pk):
+    """The long-key shape at full size (seeded 200 Mbp genome, 40% GC, 30%
+    repeat families, 50x of 150 bp = 66.7M reads, 10 Gbases, 21 GB FASTQ,
+    1% substitution; canonical k=63, 128-bit keys, 4096 buckets), FASTQ
+    resident in HBM and counted in 2 GiB device passes: Gbases/s over
+    --ll-steps steps timed with CUDA events on the library's stream, stage
+    times, the count kernel's roofline in the same units as the main line,
+    and learned vs sampled sizing on the same input."""
+    from kmertreecounter_b200 import synth
+    torch.cuda.empty_cache()
+    p = synth.large_long()
+    bases = int(p.n_reads) * int(p.read_len_min)
+    data = synth.fastq(p)
+    n = int(data.size)
+    dev = torch.from_numpy(data).cuda()
+    del data
+    torch.cuda.synchronize()
+    k, buckets = 63, 4096
+    cfg = kc.default_config(k=k, n_buckets=buckets, device_batch_bytes=DEVICE_BATCH["large_long"])
+    steps = max(1, args.ll_steps)
+    stage_ms = {}
+    with kc.Counter(cfg) as c:
+        stream = torch.cuda.ExternalStream(c.stream)
+        c.count_device(dev.data_ptr(), n)  # warm-up, sizes every buffer
+        c.set_profiling(True)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            st = c.count_device(dev.data_ptr(), n)
+            for name, (ms, _) in c.stage_times().items():
+                stage_ms[name] = stage_ms.get(name, 0.0) + ms
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms_step = e0.elapsed_time(e1) / steps
+        _, distinct = c.histogram(1, 2)
+        stats = st.as_dict()
+        stats.pop("root_counts", None)
+    K, L = stats["total_kmers"], stats["low_records"]
+    alg = 64 * K + 64 * (K - L)
+    count_ms = stage_ms.get("count", 0.0) / steps
+    roof = pipeline_roofline(dev_peaks, pk, n, K, L, stats["root_records"], kc.packed_bytes(k), kc.record_bytes(k),
+                             ms_step, count_ms)
+    out = {"config": {"workload": DESCRIBE["large_long"], "k": k, "n_buckets": buckets, "fastq_bytes": n,
+                      "bases": bases, "reads": int(p.n_reads), "device_pass_bytes": DEVICE_BATCH["large_long"]},
+           "value": bases / (ms_step / 1e3) / 1e9, "unit": "Gbases/s", "ms_per_step": ms_step, "steps": steps,
+           "distinct_kmers": distinct, "distinct_kmers_per_s": distinct / (ms_step / 1e3), "stats": stats,
+           "stages_ms_per_step": {s_: v / steps for s_, v in stage_ms.items()},
+           "roofline": {"bound": "hbm", "kernel": "count_routed", "alg_bytes_per_step": alg,
+                        "achieved": alg / (count_ms / 1e3) / 1e9 if count_ms else None, "peak": pk["hbm_gbs"],
+                        "frac": alg / (count_ms / 1e3) / 1e9 / pk["hbm_gbs"] if count_ms else None},
+           "pipeline_roofline": roof.get("pipeline")}
+    if not args.no_sizing:
+        out["sizing"] = compare_sizing(args, kc, torch, dev, n, k, buckets, DEVICE_BATCH["large_long"], steps)
+    del dev
+    torch.cuda.empty_cache()
+    return out
+
+
+def file_to_file(args, sample_path, sample_bases, k, ref_sample_gbs, full_path, full_bases):
+    """This build's drop-in command line (`bin/Tree <fastq> <k> <n_thread>
+    <mem_gb>`) timed like the reference's `Tree`: wall clock of the whole
+    process, from reading the FASTQ file to low.bin and root_0..255.bin
+    written under ./tmp/, device set-up included.  On the reference's own
+    sample file (beside the reference's time on it) and on the full workload's
+    file."""
+    tree = os.path.join(ROOT, "kmertreecounter_b200", "bin", "Tree")
+    threads = str(max(6, host_facts()["cores"] or 6))
+
+    def run(path, bases, runs):
+        best = None
+        for _ in range(runs):
+            with tempfile.TemporaryDirectory(dir=os.path.dirname(path)) as wd:
+                t = time.perf_counter()
+                r = subprocess.run([tree, path, str(k), threads, "16"], cwd=wd, capture_output=True, text=True)
+                dt = time.perf_counter() - t
+                if r.returncode:
+                    return {"error": f"exit {r.returncode}: {r.stderr.strip()[-200:]}"}
+                if best is None or dt < best:
+                    best = dt
+        return {"seconds": best, "gbases_s": bases / best / 1e9, "runs": runs}
+
+    out = {"method": "wall clock of the process, outputs written to ./tmp/ on local disk, best of the runs"}
+    ours = run(sample_path, sample_bases, 2)
+    out["sample"] = {"ours": ours, "reference_gbases_s": ref_sample_gbs,
+                     "ratio": ours["gbases_s"] / ref_sample_gbs if "gbases_s" in ours and ref_sample_gbs else None}
+    if full_path:
+        out["full"] = {"ours": run(full_path, full_bases, 2)}
     return out
 
 
@@ -473,6 +642,7 @@ def run_ours(args):
     dominant = max(stage_ms, key=lambda s: stage_ms[s]) if stage_ms else None
     roof = pipeline_roofline(dev_peaks, pk, n, K, L, stats["root_records"], kc.packed_bytes(k), kc.record_bytes(k),
                              ms_step, count_ms)
+    traffic, traffic_note = profile_traffic(args)
 
     line = {
         "metric": "FASTQ Gbases/s to exact k-mer counts on 1 B200",
@@ -487,10 +657,7 @@ def run_ours(args):
         "vs_baseline": None,
         "dtype": "u64",
         "data": "synthetic (seeded generator, reference benchmark shape)",
-        "config": {"workload": f"{args.workload}: 100 Mbp genome 45% GC 20% repeats, 30x 150 bp (20M reads), k=31"
-                   if args.workload == "genome_scale" and args.scale == 1.0 else f"{args.workload} scale={args.scale}",
-                   "k": k, "n_buckets": buckets, "fastq_bytes": n, "bases": bases, "reads": int(p.n_reads),
-                   "l2": "inputs larger than L2 (FASTQ %.1f GB)" % (n / 1e9), "parallelism": f"replica x{world}"},
+        "config": workload_config(args, world, n, bases, p.n_reads),
         "distinct_kmers": distinct,
         "distinct_kmers_per_s": distinct * world / (ms_step / 1e3),
         "stats": stats,
@@ -502,7 +669,8 @@ def run_ours(args):
         "roofline": {"bound": "hbm", "kernel": "count_routed", "achieved": achieved, "peak": pk["hbm_gbs"],
                      "unit": "GB/s", "frac": (achieved / pk["hbm_gbs"]) if achieved else None,
                      "peak_source": pk["source"], "alg_bytes_per_launch": alg_bytes,
-                     "traffic": profile_traffic(args), "per": "step (all count_routed launches of one count)",
+                     "traffic": traffic, "traffic_source": traffic_note,
+                     "per": "step (all count_routed launches of one count)",
                      "dominant_stage": dominant, "atomic": roof.get("count_routed_atomic")},
         "pipeline_roofline": roof.get("pipeline"),
         "clocks": clk,
@@ -515,18 +683,36 @@ def run_ours(args):
         except kc.KcError as e:
             line["sizing"] = {"error": str(e)}
     del dev
+    ftf_dir, full_path = None, None
+    if rank == 0 and not args.no_file_to_file and not args.no_cpu_baseline:
+        import shutil
+        ftf_dir = tempfile.TemporaryDirectory()
+        if shutil.disk_usage(ftf_dir.name).free > 3 * n:  # the FASTQ plus the outputs of one run
+            full_path = os.path.join(ftf_dir.name, "full.fastq")
+            host.tofile(full_path)
     kc.host_free(host_ptr)
 
+    if rank == 0 and not args.no_large_long and args.workload == "genome_scale" and args.scale == 1.0:
+        try:
+            line["large_long"] = large_long_record(args, kc, torch, dev_peaks, pk)
+        except kc.KcError as e:
+            line["large_long"] = {"error": str(e)}
     if rank == 0 and not args.no_batched and args.workload == "genome_scale":
         line["batched_sets"] = compare_batched(args, kc, torch)
     if rank == 0 and not args.no_cpu_baseline:
         with tempfile.TemporaryDirectory() as wd:
-            path, data, kk, sbases, sp = cpu_sample(args.workload, args.sample_scale, wd)
+            path, data, kk, sbases, info = cpu_sample(args.workload, args.sample_scale, wd)
             res, kind, cores = time_reference(path, data, kk, sbases, 2, wd)
             best = max(r[0] for r in res)
             line["cpu_baseline"] = {"value": best, "unit": "Gbases/s", "cores": cores, "kind": kind,
-                                    "sample": f"{args.workload} at scale {args.sample_scale}: {int(sp.n_reads)} reads, "
-                                              f"{data.size} FASTQ bytes, best of {len(res)} runs"}
+                                    "sample": f"{args.workload} at scale {args.sample_scale}: {info['reads']} reads, "
+                                              f"{data.size} FASTQ bytes, best of {len(res)} runs",
+                                    "host": host_facts()}
+            if not args.no_file_to_file:
+                line["file_to_file"] = file_to_file(args, path, sbases, kk, best if kind == "reference" else None,
+                                                    full_path, bases)
+    if ftf_dir is not None:
+        ftf_dir.cleanup()
     if world > 1:
         import torch.distributed as dist
         dist.barrier()
@@ -542,7 +728,7 @@ def run_reference(args):
     if rank != 0:
         return
     with tempfile.TemporaryDirectory() as wd:
-        path, data, k, bases, sp = cpu_sample(args.workload, args.sample_scale, wd)
+        path, data, k, bases, info = cpu_sample(args.workload, args.sample_scale, wd)
         res, kind, cores = time_reference(path, data, k, bases, max(args.warmup, 0) + args.steps, wd)
         timed = res[max(args.warmup, 0):] or res
         secs = sum(r[1] for r in timed)
@@ -561,10 +747,15 @@ def run_reference(args):
             "vs_baseline": None,
             "dtype": "u64",
             "data": "synthetic (seeded generator, reference benchmark shape)",
-            "config": {"workload": f"{args.workload} sample at scale {args.sample_scale}", "k": k,
-                       "fastq_bytes": int(data.size), "bases": bases},
+            "config": workload_config(args, world, info["full"]["fastq_bytes"], info["full"]["bases"],
+                                      info["full"]["reads"]),
             "cpu_baseline": {"value": value, "unit": "Gbases/s", "cores": cores, "kind": kind,
-                             "sample": f"{args.workload} at scale {args.sample_scale}: {int(sp.n_reads)} reads per step"},
+                             "sample": f"each step one run of the reference's Tree ({cores} threads) on a bounded "
+                                       f"sample of this workload: the same generator at scale {args.sample_scale} "
+                                       f"(genome {info['genome_len']} bp, {info['reads']} reads, {data.size} FASTQ "
+                                       f"bytes, same coverage and error model); runs whose k-mer total differs "
+                                       f"from the oracle's are rejected and repeated",
+                             "host": host_facts()},
             "e2e": {"value": value, "unit": "Gbases/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         }
         print(json.dumps(line), flush=True)
@@ -572,6 +763,9 @@ def run_reference(args):
 
 def main():
     args = parse()
+    if args.write_sample:
+        write_sample(args.workload, args.sample_scale, args.write_sample)
+        return
     if args.impl == "reference":
         run_reference(args)
     else:

@@ -54,7 +54,13 @@ extern "C" {
  * (src/main.cpp:314-374); n_thread, mem_gb and map_capacity have no meaning on
  * the device and are accepted and ignored by the CLI. */
 typedef struct kc_config {
-    uint32_t k;            /* 1..128; key words N = 1 for k<=32, 2 for k<=64, 4 for k<=128 */
+    uint32_t k;            /* 1..128; key words N = 1 for k<=32, 2 for k<=64, 4 for k<=128.
+                            * k = 96 differs from the reference on purpose: the
+                            * reference leaves bases older than the window in key
+                            * word 3 of F-oriented keys (its forward register is
+                            * masked only in the last word, src/GetKmer.h:58-82),
+                            * so one k-mer can get several root records; here word
+                            * 3 is 0 and every k-mer has one key. */
     uint32_t canonical;    /* must be 1: the reference always counts canonical */
     uint32_t min_count;    /* root-record filter, inclusive (src/NewKmerTree.h:1159-1168) */
     uint32_t max_count;
@@ -212,11 +218,11 @@ int kc_count_sets(kc_context* ctx, const uint8_t* d_fastq, const kc_set_desc* se
  * and per-root record counts (256 entries, may be NULL). */
 int kc_result_sizes(kc_context* ctx, uint64_t* low_bytes, uint64_t* n_root_records, uint64_t* root_counts);
 
-/* Copy the packed low.bin bytes into dst (cap bytes). */
+/* Copy the packed low.bin bytes into dst (cap bytes; host or device memory). */
 int kc_copy_low(kc_context* ctx, uint8_t* dst, uint64_t cap);
 
 /* Copy all root records (ExportRecord<N>, grouped by root id 0..255 in
- * order) into dst (cap bytes). */
+ * order) into dst (cap bytes; host or device memory). */
 int kc_copy_roots(kc_context* ctx, uint8_t* dst, uint64_t cap);
 
 /* Merged count histogram of the last device-held result (kc_count_host or
@@ -273,15 +279,21 @@ const char* kc_stage_name(int stage);
  * afford cudaMalloc/cudaFree (cudaFree synchronises the device).
  *
  * Counts a FASTQ already in device memory (16-byte aligned, at most
- * KC_NOALLOC_MAX_FASTQ_BYTES, 256 buckets) on `stream` (a cudaStream_t, NULL
- * = default stream) and writes the packed low.bin bytes to d_low and the
- * root records, grouped by root id, to d_roots (device buffers with the
- * given byte capacities); stats receives the counters.  All scratch comes
- * from one static device array of KC_NOALLOC_SCRATCH_BYTES that every GPU
- * loading this library holds until exit.  The first call on a device looks up
- * that array's address (make it before any stream capture).  Calls share the
- * array: overlapping calls on the GPU race and must be serialised by the
- * caller.  Larger inputs are rejected with KC_ERR_INVALID. */
+ * KC_NOALLOC_MAX_FASTQ_BYTES, 256 buckets, k 1..64, canonical only) on
+ * `stream` (a cudaStream_t, NULL = default stream) and writes the packed
+ * low.bin bytes to d_low and the root records, grouped by root id, to d_roots
+ * (device buffers with the given byte capacities); stats receives the
+ * counters.  All scratch comes from one static device array of
+ * KC_NOALLOC_SCRATCH_BYTES per GPU, held until exit.  With CUDA's lazy module
+ * loading (the default since CUDA 12.2) that array is reserved when the first
+ * call on a device looks up its address, not when the library is loaded: make
+ * that first call before the caller's allocator claims the device budget (or
+ * run with CUDA_MODULE_LOADING=EAGER), and before any stream capture.  Calls
+ * share the array: overlapping calls on the GPU race and must be serialised
+ * by the caller.  Larger inputs, other k or bucket counts, an unaligned input
+ * and output buffers too small for the result are rejected with
+ * KC_ERR_INVALID; a table that outgrows the array ends the call with
+ * KC_ERR_OVERFLOW. */
 #define KC_NOALLOC_SCRATCH_BYTES (64ull << 20)
 #define KC_NOALLOC_MAX_FASTQ_BYTES (1ull << 20)
 

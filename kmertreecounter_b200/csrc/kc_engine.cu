@@ -1609,7 +1609,7 @@ int kc_copy_low(kc_context* c, uint8_t* dst, uint64_t cap) {
     if (cap < bytes) return fail(KC_ERR_INVALID, "destination too small: %llu < %llu", (unsigned long long)cap,
                                  (unsigned long long)bytes);
     if (bytes) {
-        CK(cudaMemcpyAsync(dst, c->low_packed.p, bytes, cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaMemcpyAsync(dst, c->low_packed.p, bytes, cudaMemcpyDefault, c->stream));
         CK(cudaStreamSynchronize(c->stream));
     }
     return KC_OK;
@@ -1622,7 +1622,7 @@ int kc_copy_roots(kc_context* c, uint8_t* dst, uint64_t cap) {
     if (cap < bytes) return fail(KC_ERR_INVALID, "destination too small: %llu < %llu", (unsigned long long)cap,
                                  (unsigned long long)bytes);
     if (bytes) {
-        CK(cudaMemcpyAsync(dst, c->roots.p, bytes, cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaMemcpyAsync(dst, c->roots.p, bytes, cudaMemcpyDefault, c->stream));
         CK(cudaStreamSynchronize(c->stream));
     }
     return KC_OK;

@@ -13,11 +13,15 @@
 // Limits and sharing rules:
 //   * scratch = KC_NOALLOC_SCRATCH_BYTES (64 MiB) per device, held by every
 //     GPU that loads this library until the process exits;
-//   * input at most KC_NOALLOC_MAX_FASTQ_BYTES (1 MiB) and 256 buckets;
-//     larger requests are rejected with KC_ERR_INVALID before any work;
+//   * input at most KC_NOALLOC_MAX_FASTQ_BYTES (1 MiB), 256 buckets, k 1..64,
+//     canonical only; other requests are rejected with KC_ERR_INVALID before
+//     any work;
 //   * the first call on a device resolves the array's device address
-//     (cudaGetSymbolAddress) with that device current; make that first call
-//     before any stream capture;
+//     (cudaGetSymbolAddress) with that device current.  Under CUDA's lazy
+//     module loading (the default since CUDA 12.2) this is also when the
+//     64 MiB are reserved, so make that first call before the caller's
+//     allocator claims the device budget (or set CUDA_MODULE_LOADING=EAGER),
+//     and before any stream capture;
 //   * every call reuses the same array and clears what must start at zero;
 //     calls that overlap on the GPU (two streams, two host threads) race on
 //     it and must be serialised by the caller.
@@ -48,6 +52,18 @@ int err(int code, const char* msg) { return kc_internal_set_error(code, msg); }
     do {                                                                      \
         cudaError_t e_ = (x);                                                 \
         if (e_ != cudaSuccess) return err(KC_ERR_DEVICE, cudaGetErrorString(e_)); \
+    } while (0)
+
+// Inside a count: on a CUDA error, wait for the work already queued on the
+// caller's stream first, so that no kernel of this call still reads the
+// shared array or writes the caller's buffers after the call returned.
+#define NKS(x)                                                                \
+    do {                                                                      \
+        cudaError_t e_ = (x);                                                 \
+        if (e_ != cudaSuccess) {                                              \
+            cudaStreamSynchronize(st);                                        \
+            return err(KC_ERR_DEVICE, cudaGetErrorString(e_));                \
+        }                                                                     \
     } while (0)
 
 // Bump allocator over the static array (host-side offsets only).
@@ -99,12 +115,12 @@ int run(const kc_config* g, const uint8_t* d_fastq, uint64_t n, uint8_t* d_low, 
     uint32_t* chunk_pass = cv.take<uint32_t>(MAX_CHUNKS);
     uint64_t* chunk_off = cv.take<uint64_t>(MAX_CHUNKS);
     if (!cv.ok) return err(KC_ERR_OVERFLOW, "no-alloc scratch exhausted (fixed part)");
-    NK(cudaMemsetAsync(scal, 0, 16 * sizeof(uint64_t), st));
+    NKS(cudaMemsetAsync(scal, 0, 16 * sizeof(uint64_t), st));
 
     // line index per tile, then per-bucket k-mer totals
     if (tiles) kc::lines_per_tile<<<tiles, kc::EXT_THREADS, 0, st>>>(d_fastq, n, tile_nl);
     scan<uint32_t, uint64_t>(tile_nl, tiles, tile_line, 0, sums, scal + 0, st);
-    NK(cudaMemsetAsync(bcount, 0, NB * sizeof(uint64_t), st));
+    NKS(cudaMemsetAsync(bcount, 0, NB * sizeof(uint64_t), st));
     kc::ExtractArgs ea{};
     ea.buf = d_fastq;
     ea.n = n;
@@ -117,10 +133,10 @@ int run(const kc_config* g, const uint8_t* d_fastq, uint64_t n, uint8_t* d_low, 
     ea.bucket_cursor = bcursor;
     ea.error = reinterpret_cast<uint32_t*>(scal + 8);
     if (tiles) kc::extract_kernel<NW, kc::HIST><<<tiles, kc::EXT_THREADS, kc::extract_smem_bytes<NW, kc::HIST>(NB), st>>>(ea);
-    NK(cudaGetLastError());
+    NKS(cudaGetLastError());
     uint64_t h_count[NB];
-    NK(cudaMemcpyAsync(h_count, bcount, sizeof h_count, cudaMemcpyDeviceToHost, st));
-    NK(cudaStreamSynchronize(st));
+    NKS(cudaMemcpyAsync(h_count, bcount, sizeof h_count, cudaMemcpyDeviceToHost, st));
+    NKS(cudaStreamSynchronize(st));
     uint64_t start[NB], K = 0;
     for (int b = 0; b < NB; ++b) {
         start[b] = K;
@@ -155,15 +171,15 @@ int run(const kc_config* g, const uint8_t* d_fastq, uint64_t n, uint8_t* d_low, 
     SlotT* table = reinterpret_cast<SlotT*>(scratch + tab_off);
     if (ts > tab_cap) return err(KC_ERR_OVERFLOW, "no-alloc scratch exhausted: tables do not fit");
 
-    NK(cudaMemcpyAsync(meta, h_meta, sizeof h_meta, cudaMemcpyHostToDevice, st));
-    NK(cudaMemsetAsync(bloom, 0, bw * sizeof(uint64_t), st));
-    NK(cudaMemsetAsync(overflow, 0, NB * sizeof(uint32_t), st));
+    NKS(cudaMemcpyAsync(meta, h_meta, sizeof h_meta, cudaMemcpyHostToDevice, st));
+    NKS(cudaMemsetAsync(bloom, 0, bw * sizeof(uint64_t), st));
+    NKS(cudaMemsetAsync(overflow, 0, NB * sizeof(uint32_t), st));
     kc::init_slots<NW><<<256, 256, 0, st>>>(table, ts);
-    NK(cudaMemcpyAsync(bcursor, start, sizeof start, cudaMemcpyHostToDevice, st));
+    NKS(cudaMemcpyAsync(bcursor, start, sizeof start, cudaMemcpyHostToDevice, st));
     ea.routed = routed;
     // the scatter's staging area needs more than the default 48 KiB
     const size_t smem_sc = kc::extract_smem_bytes<NW, kc::SCATTER>(NB);
-    NK(cudaFuncSetAttribute(kc::extract_kernel<NW, kc::SCATTER>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_sc));
+    NKS(cudaFuncSetAttribute(kc::extract_kernel<NW, kc::SCATTER>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_sc));
     if (tiles) kc::extract_kernel<NW, kc::SCATTER><<<tiles, kc::EXT_THREADS, smem_sc, st>>>(ea);
 
     kc::CountArgs ca{};
@@ -180,57 +196,65 @@ int run(const kc_config* g, const uint8_t* d_fastq, uint64_t n, uint8_t* d_low, 
     ca.use_filter = 1;
     const uint64_t cgrid = cdiv(K, (uint64_t)CT * kc::CNT_SEGS_PER_WARP);
     if (cgrid) kc::count_routed<NW><<<cgrid, kc::CNT_THREADS, 0, st>>>(ca);
-    NK(cudaGetLastError());
+    NKS(cudaGetLastError());
 
     // overflow: grow the bucket's table inside the arena, move, retry
     uint64_t rehashes = 0;
     for (int round = 0;; ++round) {
         uint32_t h_over[NB];
-        NK(cudaMemcpyAsync(h_over, overflow, sizeof h_over, cudaMemcpyDeviceToHost, st));
-        NK(cudaStreamSynchronize(st));
+        NKS(cudaMemcpyAsync(h_over, overflow, sizeof h_over, cudaMemcpyDeviceToHost, st));
+        NKS(cudaStreamSynchronize(st));
         bool any = false;
         for (int b = 0; b < NB; ++b) any |= h_over[b] != 0;
         if (!any) break;
         if (round > 16) return err(KC_ERR_OVERFLOW, "no-alloc tables kept overflowing");
-        NK(cudaMemsetAsync(overflow, 0, NB * sizeof(uint32_t), st));
+        NKS(cudaMemsetAsync(overflow, 0, NB * sizeof(uint32_t), st));
         for (int b = 0; b < NB; ++b) {
             if (!h_over[b]) continue;
-            const uint64_t old_slots = h_meta[b].tab_mask + 1, new_slots = old_slots * 4;
-            if (ts + new_slots > tab_cap) return err(KC_ERR_OVERFLOW, "no-alloc scratch exhausted while growing a table");
-            kc::init_slots<NW><<<64, 256, 0, st>>>(table + ts, new_slots);
-            uint32_t* failed = reinterpret_cast<uint32_t*>(scal + 9);
-            NK(cudaMemsetAsync(failed, 0, sizeof(uint32_t), st));
-            kc::rehash_bucket<NW><<<64, 256, 0, st>>>(table + h_meta[b].tab_off, old_slots, table + ts, new_slots - 1, failed);
-            uint32_t h_failed = 0;
-            NK(cudaMemcpyAsync(&h_failed, failed, sizeof h_failed, cudaMemcpyDeviceToHost, st));
-            NK(cudaStreamSynchronize(st));
-            if (h_failed) return err(KC_ERR_OVERFLOW, "no-alloc table growth failed");
-            h_meta[b].tab_off = ts;
-            h_meta[b].tab_mask = new_slots - 1;
-            ts += new_slots;
+            // grow x4 into the free end of the arena; a growth whose rehash
+            // still meets a full probe window (pathological clustering) is
+            // dropped and the table grown x4 again, as the engine does
+            const uint64_t old_slots = h_meta[b].tab_mask + 1;
+            for (uint64_t new_slots = old_slots * 4;; new_slots *= 4) {
+                if (ts + new_slots > tab_cap)
+                    return err(KC_ERR_OVERFLOW, "no-alloc scratch exhausted while growing a table");
+                kc::init_slots<NW><<<64, 256, 0, st>>>(table + ts, new_slots);
+                uint32_t* failed = reinterpret_cast<uint32_t*>(scal + 9);
+                NKS(cudaMemsetAsync(failed, 0, sizeof(uint32_t), st));
+                kc::rehash_bucket<NW><<<64, 256, 0, st>>>(table + h_meta[b].tab_off, old_slots, table + ts,
+                                                          new_slots - 1, failed);
+                uint32_t h_failed = 0;
+                NKS(cudaMemcpyAsync(&h_failed, failed, sizeof h_failed, cudaMemcpyDeviceToHost, st));
+                NKS(cudaStreamSynchronize(st));
+                if (!h_failed) {
+                    h_meta[b].tab_off = ts;
+                    h_meta[b].tab_mask = new_slots - 1;
+                    ts += new_slots;
+                    break;
+                }
+            }
             ++rehashes;
         }
-        NK(cudaMemcpyAsync(meta, h_meta, sizeof h_meta, cudaMemcpyHostToDevice, st));
+        NKS(cudaMemcpyAsync(meta, h_meta, sizeof h_meta, cudaMemcpyHostToDevice, st));
         ca.use_filter = 0;
         kc::count_routed<NW><<<cgrid, kc::CNT_THREADS, 0, st>>>(ca);
-        NK(cudaGetLastError());
+        NKS(cudaGetLastError());
     }
 
     // first occurrences -> packed low.bin bytes in the caller's buffer
     scan<uint32_t, uint64_t>(seg_low, nsegs, seg_prefix, 0, sums, scal + 1, st);
     uint64_t nlow = 0;
     uint32_t ext_err = 0;
-    NK(cudaMemcpyAsync(&nlow, scal + 1, sizeof nlow, cudaMemcpyDeviceToHost, st));
-    NK(cudaMemcpyAsync(&ext_err, scal + 8, sizeof ext_err, cudaMemcpyDeviceToHost, st));
-    NK(cudaStreamSynchronize(st));
+    NKS(cudaMemcpyAsync(&nlow, scal + 1, sizeof nlow, cudaMemcpyDeviceToHost, st));
+    NKS(cudaMemcpyAsync(&ext_err, scal + 8, sizeof ext_err, cudaMemcpyDeviceToHost, st));
+    NKS(cudaStreamSynchronize(st));
     if (ext_err) return err(KC_ERR_DEVICE, "internal error: routing bucket disagreed with its reservation");
     const uint64_t P = kc_packed_bytes(k);
     if (nlow * P > low_cap) return err(KC_ERR_INVALID, "low output buffer too small");
-    if (nsegs)
-        kc::pack_low<NW><<<std::min<uint64_t>(cdiv(nsegs, 256), 148 * 4), 256, 0, st>>>(routed, seg_low, seg_prefix,
-                                                                                       nsegs, k, d_low, 0);
 
-    // root records grouped by root id
+    // export chunk list (root records grouped by root id): checked for room
+    // before anything else is launched, so every error return below finds
+    // the stream idle
     kc::ExportChunk h_chunks[MAX_CHUNKS];
     uint64_t nch = 0;
     const uint64_t CH = std::max<uint64_t>(16384, cdiv(ts, 700));
@@ -242,17 +266,22 @@ int run(const kc_config* g, const uint8_t* d_fastq, uint64_t n, uint8_t* d_low, 
     kc::ExportChunk* chunks = reinterpret_cast<kc::ExportChunk*>(table + ts);
     if ((ts * sizeof(SlotT) + nch * sizeof(kc::ExportChunk) + 256) > tab_cap * sizeof(SlotT))
         return err(KC_ERR_OVERFLOW, "no-alloc scratch exhausted at export");
-    NK(cudaMemcpyAsync(chunks, h_chunks, nch * sizeof(kc::ExportChunk), cudaMemcpyHostToDevice, st));
-    NK(cudaMemsetAsync(rcount, 0, 257 * sizeof(uint64_t), st));
+    if (nsegs)
+        kc::pack_low<NW><<<std::min<uint64_t>(cdiv(nsegs, 256), 148 * 4), 256, 0, st>>>(routed, seg_low, seg_prefix,
+                                                                                       nsegs, k, d_low, 0);
+
+    // root records grouped by root id
+    NKS(cudaMemcpyAsync(chunks, h_chunks, nch * sizeof(kc::ExportChunk), cudaMemcpyHostToDevice, st));
+    NKS(cudaMemsetAsync(rcount, 0, 257 * sizeof(uint64_t), st));
     const uint64_t egrid = std::max<uint64_t>(1, std::min<uint64_t>(nch, 148 * 4));
     if (nch)
         kc::export_count<NW><<<egrid, kc::EXP_THREADS, 0, st>>>(table, chunks, nch, g->min_count, g->max_count,
                                                                 chunk_pass, rcount, rcount + 256, nullptr);
     uint64_t h_r[257];
     uint32_t h_pass[MAX_CHUNKS];
-    NK(cudaMemcpyAsync(h_r, rcount, sizeof h_r, cudaMemcpyDeviceToHost, st));
-    if (nch) NK(cudaMemcpyAsync(h_pass, chunk_pass, nch * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
-    NK(cudaStreamSynchronize(st));
+    NKS(cudaMemcpyAsync(h_r, rcount, sizeof h_r, cudaMemcpyDeviceToHost, st));
+    if (nch) NKS(cudaMemcpyAsync(h_pass, chunk_pass, nch * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+    NKS(cudaStreamSynchronize(st));
     uint64_t R = 0;
     for (int r = 0; r < 256; ++r) R += h_r[r];
     uint64_t h_off[MAX_CHUNKS];
@@ -262,12 +291,12 @@ int run(const kc_config* g, const uint8_t* d_fastq, uint64_t n, uint8_t* d_low, 
     }
     const uint64_t rec = kc_record_bytes(k);
     if (R * rec > roots_cap) return err(KC_ERR_INVALID, "root output buffer too small");
-    if (nch) NK(cudaMemcpyAsync(chunk_off, h_off, nch * sizeof(uint64_t), cudaMemcpyHostToDevice, st));
+    if (nch) NKS(cudaMemcpyAsync(chunk_off, h_off, nch * sizeof(uint64_t), cudaMemcpyHostToDevice, st));
     if (nch && R)
         kc::export_write<NW><<<egrid, kc::EXP_THREADS, 0, st>>>(table, chunks, nch, g->min_count, g->max_count,
                                                                 chunk_off, d_roots);
-    NK(cudaGetLastError());
-    NK(cudaStreamSynchronize(st));
+    NKS(cudaGetLastError());
+    NKS(cudaStreamSynchronize(st));
     if (stats) {
         std::memset(stats, 0, sizeof *stats);
         stats->input_bytes = n;

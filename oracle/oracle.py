@@ -24,6 +24,9 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB = os.path.join(HERE, "_build", "libkmer_oracle.so")
 REF_TREE = os.path.join(HERE, "_ref", "Tree")
 REF_HIST = os.path.join(HERE, "_ref", "histogram_tool")
+# where build() looks for the reference's sources (absent on machines that
+# only carry the prebuilt oracle/_ref binaries)
+REF_SRC = os.environ.get("KC_REFERENCE_SRC", "/root/reference")
 
 _lib = None
 
@@ -35,7 +38,7 @@ def build():
     if not os.path.exists(LIB) or os.path.getmtime(LIB) < os.path.getmtime(src):
         subprocess.check_call(["make", "-s", "-C", HERE, "oracle"])
     if not os.path.exists(REF_TREE):
-        subprocess.call(["make", "-s", "-C", HERE, "ref"])
+        subprocess.call(["make", "-s", "-C", HERE, "ref", f"REF={REF_SRC}"])
 
 
 def _load():
@@ -79,6 +82,13 @@ def extract(data, k):
     out = np.empty((K, words(k)), dtype=np.uint64)
     lib.kor_extract(buf.ctypes.data, buf.size, k, out.ctypes.data, K)
     return out
+
+
+def total_kmers(data, k):
+    """K (valid windows) without materialising the keys."""
+    lib = _load()
+    buf = _as_u8(data)
+    return int(lib.kor_extract(buf.ctypes.data, buf.size, k, None, 0))
 
 
 def count(data, k):
@@ -145,7 +155,10 @@ def _sort_unique(keys, counts):
     """Sort (n, N) keys lexicographically and sum counts of equal keys."""
     if keys.shape[0] == 0:
         return keys.reshape(0, keys.shape[1] if keys.ndim == 2 else 1), counts.astype(np.uint64)
-    order = np.lexsort(tuple(keys[:, i] for i in range(keys.shape[1] - 1, -1, -1)))
+    if keys.shape[1] == 1:
+        order = np.argsort(keys[:, 0], kind="stable")
+    else:
+        order = np.lexsort(tuple(keys[:, i] for i in range(keys.shape[1] - 1, -1, -1)))
     ks, cs = keys[order], counts[order].astype(np.uint64)
     new = np.ones(ks.shape[0], dtype=bool)
     new[1:] = np.any(ks[1:] != ks[:-1], axis=1)

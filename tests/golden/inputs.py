@@ -18,6 +18,18 @@ def plain_small(seed=1, scale=1.0):
     return synth.fastq(synth.plain_small(seed=seed, scale=scale)).tobytes()
 
 
+# The benchmark shapes (seeded generator): genome-scale (100 Mbp, 45% GC, 20%
+# repeat families, 30x, 3' error ramp, k=31) and large long keys (200 Mbp, 40%
+# GC, 30% repeats, 50x, k=63), `scale` shrinking genome and reads together.
+# These return numpy arrays (the full genome-scale input is 6.3 GB).
+def genome_scale(seed=2, scale=1.0):
+    return synth.fastq(synth.genome_scale(seed=seed, scale=scale))
+
+
+def large_long(seed=5, scale=1.0):
+    return synth.fastq(synth.large_long(seed=seed, scale=scale))
+
+
 def _seq(rng, n, alphabet=b"ACGT"):
     a = np.frombuffer(alphabet, dtype=np.uint8)
     return a[rng.integers(0, a.size, n)].tobytes()

@@ -1,6 +1,6 @@
 """Generate tests/golden/golden.json from the REFERENCE implementation.
 
-Run in a checkout where the reference sources exist and `make -C oracle ref`
+Run in a checkout where the reference sources exist and `make -C oracle ref REF=<reference tree>`
 has built oracle/_ref/Tree (the reference's own main.cpp compiled from its
 source files).  For every case this script:
   1. builds the FASTQ bytes (tests/golden/inputs.py, deterministic),
@@ -13,7 +13,11 @@ source files).  For every case this script:
 The oracle itself is NOT used to produce the recorded values; the tests
 compare the oracle (CPU) and the GPU path against them.
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py [--only name,name,...]
+
+With --only, the named cases are (re)generated and merged into the existing
+golden.json; the others are kept as they are.  The full genome-scale case
+needs ~40 GB of host memory and ~20 GB of disk for the reference's outputs.
 """
 import hashlib
 import json
@@ -21,6 +25,7 @@ import os
 import subprocess
 import sys
 import tempfile
+import time
 
 import numpy as np
 
@@ -37,20 +42,25 @@ CASES = [
     ("plain_small", "plain_small", {"seed": 1}, [31]),
     ("plain_small_s7", "plain_small", {"seed": 7, "scale": 0.3}, [21, 32, 33, 63, 65, 101, 127, 128]),
     ("adversarial", "adversarial", {"seed": 11}, [17, 31, 32, 33, 64, 65, 100, 128]),
+    # the benchmark shapes: genome-scale at 5% (1M reads, 313 MB) and in full
+    # (20M reads, 3 Gbases, 6.3 GB), large long keys at 2% (1.3M reads, 418 MB)
+    ("genome_scale_s05", "genome_scale", {"seed": 2, "scale": 0.05}, [31]),
+    ("large_long_s02", "large_long", {"seed": 5, "scale": 0.02}, [63]),
+    ("genome_scale_full", "genome_scale", {"seed": 2, "scale": 1.0}, [31]),
 ]
+# host resources for the reference runs of each case (threads, memory_limit_gb)
+RESOURCES = {"genome_scale_full": (8, 40)}
 
 
-def reference_case(data, k, workdir, tries=4):
-    fq = os.path.join(workdir, "in.fastq")
-    with open(fq, "wb") as f:
-        f.write(data)
-    K_oracle = int(oracle.extract(np.frombuffer(data, np.uint8), k).shape[0])
+def reference_case(fq, K_oracle, k, workdir, tries=4, threads=8, mem_gb=4):
     for attempt in range(tries):
         tmp = os.path.join(workdir, "tmp")
         if os.path.isdir(tmp):
             for f in os.listdir(tmp):
                 os.remove(os.path.join(tmp, f))
-        out, rc = oracle.run_reference(fq, k, workdir, threads=8, mem_gb=4)
+        t0 = time.time()
+        out, rc = oracle.run_reference(fq, k, workdir, threads=threads, mem_gb=mem_gb)
+        wall = time.time() - t0
         K_ref = oracle.reference_total(out)
         total = None
         if rc == 0 and K_ref == K_oracle:
@@ -67,8 +77,8 @@ def reference_case(data, k, workdir, tries=4):
     else:
         raise RuntimeError("reference never produced a complete run")
     hist_file = os.path.join(workdir, "hist.tsv")
-    subprocess.run([oracle.REF_HIST, "precise", tmp, str(k), "4", "4", hist_file, "1", "64"], check=True,
-                   capture_output=True)
+    subprocess.run([oracle.REF_HIST, "precise", tmp, str(k), str(threads), str(mem_gb), hist_file, "1", "64"],
+                   check=True, capture_output=True)
     with open(hist_file) as f:
         tool_hist = [int(line.split("\t")[1]) for line in f if line.strip()]
     return {
@@ -80,22 +90,38 @@ def reference_case(data, k, workdir, tries=4):
         "digest": oracle.digest(keys, counts),
         "hist_1_64": [int(x) for x in oracle.histogram(counts, 1, 64)],
         "histogram_tool_precise_1_64": tool_hist,
+        "reference_wall_s": round(wall, 2),
+        "reference_threads": threads,
     }
 
 
 def main():
     oracle.build()
+    only = None
+    if "--only" in sys.argv:
+        only = set(sys.argv[sys.argv.index("--only") + 1].split(","))
+    path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden.json")
     golden = {}
-    with tempfile.TemporaryDirectory() as wd:
+    if only and os.path.exists(path):
+        with open(path) as f:
+            golden = json.load(f)
+    with tempfile.TemporaryDirectory(dir=os.environ.get("KC_GOLDEN_TMP")) as wd:
         for name, builder, kw, ks in CASES:
+            if only and name not in only:
+                continue
             data = getattr(inputs, builder)(**kw)
             entry = {"builder": builder, "kwargs": kw, "fastq_bytes": len(data),
                      "fastq_sha256": hashlib.sha256(data).hexdigest(), "k": {}}
+            threads, mem_gb = RESOURCES.get(name, (8, 4))
+            fq = os.path.join(wd, "in.fastq")
+            with open(fq, "wb") as f:
+                f.write(data)
+            K_oracle = {k: oracle.total_kmers(np.frombuffer(data, np.uint8), k) for k in ks}
+            del data  # the full genome-scale input is 6.3 GB; the reference needs the memory
             for k in ks:
                 print(f"{name} k={k}", flush=True)
-                entry["k"][str(k)] = reference_case(data, k, wd)
+                entry["k"][str(k)] = reference_case(fq, K_oracle[k], k, wd, threads=threads, mem_gb=mem_gb)
             golden[name] = entry
-    path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden.json")
     with open(path, "w") as f:
         json.dump(golden, f, indent=1, sort_keys=True)
     print("wrote", path)

@@ -87,3 +87,55 @@ def check_filtered(counter, data, k, min_count, max_count):
     got[rid] = True
     assert np.array_equal(got, expect)
     assert np.array_equal(roots["count"].astype(np.int64), table[rid])
+
+
+def merged_on_device(low_raw, roots_raw, k):
+    """Merged exact (key, count) table of low.bin bytes and root records held
+    in CUDA uint8 tensors, computed on the GPU with torch (for outputs of
+    hundreds of millions of keys, where numpy sorting takes minutes): returns
+    (keys (D, N) uint64, counts (D,) uint64) as numpy arrays in the oracle's
+    lexicographic order, ready for oracle.digest.  Needs packed low.bin
+    records of whole words (packed bytes == 8N: k = 31, 32, 63, 64)."""
+    import torch
+    nw = oracle.words(k)
+    if oracle.packed_bytes(k) != 8 * nw:
+        raise ValueError("merged_on_device needs whole-word low.bin records")
+    rec_words = nw + 1
+    lk = low_raw.view(torch.int64).view(-1, nw)
+    rr = roots_raw.view(torch.int64).view(-1, rec_words)
+    keys = torch.cat([lk, rr[:, :nw]])
+    cnt = torch.cat([torch.ones(lk.shape[0], dtype=torch.int64, device=lk.device), rr[:, nw] & 0xFFFFFFFF])
+    del lk, rr
+    # unsigned lexicographic order: flip the sign bit, stable sorts from the
+    # last word to the first
+    order = None
+    for w in range(nw - 1, -1, -1):
+        col = keys[:, w] if order is None else keys[order, w]
+        _, idx = torch.sort(col ^ (-(2 ** 63)), stable=True)
+        order = idx if order is None else order[idx]
+        del col, idx
+    keys, cnt = keys[order], cnt[order]
+    del order
+    new = torch.ones(keys.shape[0], dtype=torch.bool, device=keys.device)
+    if keys.shape[0] > 1:
+        new[1:] = (keys[1:] != keys[:-1]).any(dim=1)
+    seg = torch.cumsum(new.to(torch.int64), 0) - 1
+    D = int(seg[-1].item()) + 1 if seg.numel() else 0
+    out_c = torch.zeros(D, dtype=torch.int64, device=keys.device).index_add_(0, seg, cnt)
+    out_k = keys[new]
+    return (out_k.cpu().numpy().view(np.uint64).reshape(-1, nw), out_c.cpu().numpy().view(np.uint64))
+
+
+def device_outputs(counter, k):
+    """The counter's last result copied into CUDA uint8 tensors (low bytes,
+    root record bytes) and the per-root record counts."""
+    import torch
+    lb, nr, per_root = counter.sizes()
+    rec = 8 * oracle.words(k) + 8
+    low = torch.empty(max(lb, 8), dtype=torch.uint8, device="cuda")[:lb]
+    roots = torch.empty(max(nr * rec, 8), dtype=torch.uint8, device="cuda")[:nr * rec]
+    if lb:
+        counter.copy_low_into(low.data_ptr(), lb)
+    if nr:
+        counter.copy_roots_into(roots.data_ptr(), nr * rec)
+    return low, roots, per_root

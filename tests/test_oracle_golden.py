@@ -15,7 +15,11 @@ import inputs
 import oracle
 
 CASES = [(name, k) for name, ks in [("plain_small", [31]), ("plain_small_s7", [21, 32, 33, 63, 65, 101, 127, 128]),
-                                    ("adversarial", [17, 31, 32, 33, 64, 65, 100, 128])] for k in ks]
+                                    ("adversarial", [17, 31, 32, 33, 64, 65, 100, 128]),
+                                    # the benchmark shapes, scaled (313 MB and 418 MB of FASTQ;
+                                    # ~30 s and ~40 s of oracle each); the full genome-scale
+                                    # fixture (6.3 GB) is checked on the GPU only
+                                    ("genome_scale_s05", [31]), ("large_long_s02", [63])] for k in ks]
 
 _cache = {}
 
