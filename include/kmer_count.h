@@ -248,6 +248,70 @@ void kc_host_free(void* p);
 /* CUDA stream of the context (as void*), for callers that time it. */
 void* kc_stream(kc_context* ctx);
 
+/* ---- post-processing (tool/PostProcess.h) -------------------------------
+ * The reference's PostProcess::merge_all (tool/PostProcess.h:63-139) turns a
+ * count's low.bin and root files into
+ *   final_root.bin  all root records, root files 0..255 in order, unchanged
+ *   final_low.bin   the low.bin keys that are no root file's key, sorted
+ *                   (lexicographic over the key words) and unique, each as
+ *                   its N raw little-endian 64-bit words (kmer<N>)
+ *   freq_hist.txt   "count\tnum_kmers" then "c\tn" lines in ascending c:
+ *                   each root record counts at its count + 1, each
+ *                   final_low.bin key at 1; not written when both are empty.
+ * The reference reads low.bin as raw kmer<N> records, which matches its
+ * packed layout only when that is 8N bytes (k = 29..32, 61..64, 93..96,
+ * 125..128); here low.bin is unpacked with k, so every k is handled. */
+typedef struct kc_post_stats {
+    uint64_t root_records;  /* records in final_root.bin */
+    uint64_t low_in;        /* keys read from low.bin */
+    uint64_t low_in_roots;  /* of those, keys that are also root keys (left out) */
+    uint64_t final_low;     /* keys in final_low.bin */
+    uint64_t hist_lines;    /* count lines in freq_hist.txt (0: not written) */
+} kc_post_stats;
+
+/* From the last single-input result held on the device (after kc_count_host,
+ * kc_count_device or kc_count_keys_device); files go to out_dir (created if
+ * missing).  The sorting and filtering run on the context's device. */
+int kc_post_process(kc_context* ctx, const char* out_dir, kc_post_stats* stats);
+
+/* From low.bin and root_0..255.bin in temp_dir (as Tree writes them; missing
+ * root files count as empty), counted with cfg->k, on cfg->device. */
+int kc_post_process_dir(const kc_config* cfg, const char* temp_dir, const char* out_dir, kc_post_stats* stats);
+
+/* ---- Stage-0 figures of the reference -----------------------------------
+ * Before counting, the reference samples at most 256 MB of the FASTQ (three
+ * thirds of that from the start, middle and end of a plain file; the head of
+ * a gzip file; src/FastqPreReader.h:110-330), counts the sample's canonical
+ * k-mers per root prefix (key word 0 >> 56), raises counts below 1000 to
+ * 1000, assigns prefixes to its classifier threads by the longest-processing-
+ * time rule (src/main.cpp:38-86) and sizes one Bloom filter per prefix
+ * (src/main.cpp:88-108).  This build sizes from exact per-bucket totals or a
+ * learned model; these entry points compute the reference's figures for
+ * side-by-side diagnostics (bin/Tree prints them as the reference does). */
+typedef struct kc_stage0 {
+    uint64_t estimated_file_size;        /* raw FASTQ bytes assumed: file size, 4x for gzip */
+    uint64_t sample_bytes;               /* FASTQ bytes the sampler parsed */
+    uint64_t sampled_kmers;              /* canonical k-mers in the sample (before raising) */
+    uint64_t average_prefix_count;       /* "Average prefix count" */
+    uint64_t max_bloom_filter_capacity;  /* "Max Bloom Filter capacity", 64-bit words */
+    uint32_t classifier_num;             /* classifier threads for n_thread (src/main.cpp:114-117) */
+    uint32_t reserved;
+    uint64_t prefix_count[256];          /* sampled k-mers per root prefix, raised to >= 1000 */
+    uint64_t bloom_filter_capacity[256]; /* filter words per root prefix */
+    uint32_t prefix_owner[256];          /* classifier of each root prefix */
+    uint32_t load_order[256];            /* classifiers in the order the reference prints their loads */
+    uint64_t classifier_load[256];       /* total prefix count per classifier */
+} kc_stage0;
+
+/* The rules alone, from per-prefix sampled counts (256 entries), the raw
+ * FASTQ size and the thread count (6 or more, as the reference requires).
+ * Needs no device. */
+int kc_stage0_rule(const uint64_t* prefix_counts, uint64_t estimated_file_size, uint32_t n_thread, kc_stage0* out);
+
+/* Sample the FASTQ at fastq_path as the reference does, count the sample's
+ * k-mers (cfg->k) per root prefix on cfg->device, and apply the rules. */
+int kc_stage0_file(const kc_config* cfg, const char* fastq_path, uint32_t n_thread, kc_stage0* out);
+
 /* ---- diagnostics ----------------------------------------------------------
  * The reference prints per-stage timers and, with TEST_MODE, cycle counters
  * (src/main.cpp:270-309, src/definition.h:4).  Here: with profiling on, every
@@ -262,7 +326,8 @@ void* kc_stream(kc_context* ctx);
 #define KC_STAGE_EXPORT 7
 #define KC_STAGE_SORT 8
 #define KC_STAGE_INIT 9
-#define KC_STAGE_COUNT 10
+#define KC_STAGE_SUBROUTE 10 /* 64-bit keys: grouping a batch's keys by table window */
+#define KC_STAGE_COUNT 11
 
 int kc_set_profiling(kc_context* ctx, int enable);
 

@@ -8,5 +8,6 @@ include/kmer_count.h); this package is its Python binding.
 from ._native import (  # noqa: F401
     ABI_SYMBOLS, KC_ERR_DEVICE, KC_ERR_INVALID, KC_ERR_IO, KC_ERR_NOMEM, KC_ERR_OVERFLOW, KC_ERR_STATE, KC_OK,
     KC_SINK_LOW, KC_SINK_ROOT, KC_SIZING_LEARNED, KC_SIZING_SAMPLED, Counter, KcConfig, KcError, KcStats, count_fastq, default_config,
-    host_alloc, host_free, last_error, lib, measure_peaks, packed_bytes, record_bytes, record_dtype,
+    host_alloc, host_free, last_error, lib, measure_peaks, packed_bytes, record_bytes, record_dtype, stage0_file,
+    stage0_rule, post_process_dir,
 )

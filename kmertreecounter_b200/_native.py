@@ -30,13 +30,14 @@ ABI_SYMBOLS = (
     "kc_copy_roots", "kc_write_outputs", "kc_device_results", "kc_host_alloc", "kc_host_free", "kc_stream",
     "kc_set_profiling", "kc_stage_times", "kc_stage_name", "kc_count_device_noalloc", "kc_count_host_stream",
     "kc_histogram", "kc_count_sets", "kc_route_device", "kc_copy_routed", "kc_count_keys_device",
+    "kc_stage0_rule", "kc_stage0_file", "kc_post_process", "kc_post_process_dir",
 )
 KC_SINK_LOW = 0
 KC_SINK_ROOT = 1
 SINK_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_int, C.c_uint32, C.c_void_p, C.c_uint64)
 NOALLOC_SCRATCH_BYTES = 64 << 20
 NOALLOC_MAX_FASTQ_BYTES = 1 << 20
-STAGE_COUNT = 10
+STAGE_COUNT = 11
 
 
 class KcConfig(C.Structure):
@@ -81,6 +82,25 @@ class KcPeaks(C.Structure):
                 ("l2_footprint_bytes", C.c_uint64)]
 
 
+class KcStage0(C.Structure):
+    _fields_ = [("estimated_file_size", C.c_uint64), ("sample_bytes", C.c_uint64), ("sampled_kmers", C.c_uint64),
+                ("average_prefix_count", C.c_uint64), ("max_bloom_filter_capacity", C.c_uint64),
+                ("classifier_num", C.c_uint32), ("reserved", C.c_uint32), ("prefix_count", C.c_uint64 * 256),
+                ("bloom_filter_capacity", C.c_uint64 * 256), ("prefix_owner", C.c_uint32 * 256),
+                ("load_order", C.c_uint32 * 256), ("classifier_load", C.c_uint64 * 256)]
+
+    def loads_in_print_order(self):
+        """(classifier, load) in the order the reference prints its
+        "Classifier i total prefix count: c" lines."""
+        return [(int(self.load_order[i]), int(self.classifier_load[self.load_order[i]]))
+                for i in range(self.classifier_num)]
+
+
+class KcPostStats(C.Structure):
+    _fields_ = [("root_records", C.c_uint64), ("low_in", C.c_uint64), ("low_in_roots", C.c_uint64),
+                ("final_low", C.c_uint64), ("hist_lines", C.c_uint64)]
+
+
 class KcError(RuntimeError):
     def __init__(self, code, msg):
         super().__init__(f"kc error {code}: {msg}")
@@ -123,6 +143,10 @@ def _load():
         "kc_copy_routed": (i32, [vp, vp, u64]),
         "kc_count_keys_device": (i32, [vp, vp, u64, C.POINTER(u64), stp]),
         "kc_measure_peaks": (i32, [i32, u64, C.POINTER(KcPeaks)]),
+        "kc_stage0_rule": (i32, [C.POINTER(u64), u64, u32, C.POINTER(KcStage0)]),
+        "kc_stage0_file": (i32, [cfgp, C.c_char_p, u32, C.POINTER(KcStage0)]),
+        "kc_post_process": (i32, [vp, C.c_char_p, C.POINTER(KcPostStats)]),
+        "kc_post_process_dir": (i32, [cfgp, C.c_char_p, C.c_char_p, C.POINTER(KcPostStats)]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -299,6 +323,13 @@ class Counter:
     def write_outputs(self, out_dir):
         check(lib.kc_write_outputs(self._ctx, str(out_dir).encode()))
 
+    def post_process(self, out_dir):
+        """final_root.bin, final_low.bin and freq_hist.txt of the last result
+        (tool/PostProcess.h merge_all) into out_dir; returns KcPostStats."""
+        st = KcPostStats()
+        check(lib.kc_post_process(self._ctx, str(out_dir).encode(), C.byref(st)))
+        return st
+
     def device_results(self):
         dl, lb, dr, nr = C.c_void_p(), C.c_uint64(), C.c_void_p(), C.c_uint64()
         check(lib.kc_device_results(self._ctx, C.byref(dl), C.byref(lb), C.byref(dr), C.byref(nr)))
@@ -311,6 +342,33 @@ def count_fastq(path, out_dir, **kw):
     st = KcStats()
     check(lib.kc_count_fastq(C.byref(cfg), str(path).encode(), str(out_dir).encode(), C.byref(st)))
     return st
+
+
+def post_process_dir(temp_dir, out_dir, k, device=0):
+    """tool/PostProcess.h merge_all on the low.bin and root files in temp_dir."""
+    cfg = default_config(k=k, device=device)
+    st = KcPostStats()
+    check(lib.kc_post_process_dir(C.byref(cfg), str(temp_dir).encode(), str(out_dir).encode(), C.byref(st)))
+    return st
+
+
+def stage0_rule(prefix_counts, estimated_file_size, n_thread=8):
+    """The reference's Stage-0 rules on per-prefix sampled counts (KcStage0)."""
+    counts = np.ascontiguousarray(prefix_counts, np.uint64)
+    assert counts.size == 256
+    out = KcStage0()
+    check(lib.kc_stage0_rule(counts.ctypes.data_as(C.POINTER(C.c_uint64)), estimated_file_size, n_thread,
+                             C.byref(out)))
+    return out
+
+
+def stage0_file(path, k=31, n_thread=8, device=0):
+    """The reference's Stage-0 sample of the FASTQ at `path`, its per-prefix
+    k-mer counts (counted on `device`) and rules (KcStage0)."""
+    cfg = default_config(k=k, device=device)
+    out = KcStage0()
+    check(lib.kc_stage0_file(C.byref(cfg), str(path).encode(), n_thread, C.byref(out)))
+    return out
 
 
 def measure_peaks(device=0, footprint_bytes=4 << 30):

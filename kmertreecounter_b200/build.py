@@ -4,6 +4,7 @@ Produces, in-tree:
   kmertreecounter_b200/libkmertree_b200.so   sm_100a kernels + C ABI (include/kmer_count.h)
   kmertreecounter_b200/libkc_synth.so        seeded workload generator (include/kmer_synth.h)
   kmertreecounter_b200/bin/Tree              reference-compatible command line
+  kmertreecounter_b200/bin/PostProcess       tool/PostProcess.h's merge on the device
 nvcc cross-compiles sm_100a without a GPU.
 """
 import os
@@ -20,6 +21,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 LIB = os.path.join(HERE, "libkmertree_b200.so")
 SYNTH = os.path.join(HERE, "libkc_synth.so")
 TREE = os.path.join(HERE, "bin", "Tree")
+POST = os.path.join(HERE, "bin", "PostProcess")
 
 
 def _run(cmd):
@@ -42,8 +44,9 @@ def _deps(*names):
 
 def build(force=False, verbose_ptxas=False):
     os.makedirs(os.path.join(HERE, "bin"), exist_ok=True)
-    srcs = ["kc_engine.cu", "kc_sort.cu", "kc_io.cpp", "kc_noalloc.cu", "kc_mlp.cu", "kc_peaks.cu"]
-    hdrs = ["kc_kernels.cuh", "kc_scan.cuh", "kc_internal.h"]
+    srcs = ["kc_engine.cu", "kc_sort.cu", "kc_post.cu", "kc_io.cpp", "kc_stage0.cpp", "kc_noalloc.cu", "kc_mlp.cu",
+            "kc_peaks.cu"]
+    hdrs = ["kc_kernels.cuh", "kc_scan.cuh", "kc_window.cuh", "kc_internal.h"]
     if force or _stale(LIB, _deps(*srcs, *hdrs)):
         cmd = [NVCC, *ARCH, "-lineinfo", "-O3", "-std=c++20", "-Xcompiler", "-fPIC", "-shared",
                "--expt-relaxed-constexpr", "-o", LIB]
@@ -56,6 +59,9 @@ def build(force=False, verbose_ptxas=False):
               "-lpthread"])
     if force or _stale(TREE, _deps("tree_main.cpp") + [LIB]):
         _run(["g++", "-O2", "-std=c++20", "-o", TREE, os.path.join(CSRC, "tree_main.cpp"), "-L" + HERE,
+              "-lkmertree_b200", "-Wl,-rpath,$ORIGIN/.."])
+    if force or _stale(POST, _deps("post_main.cpp") + [LIB]):
+        _run(["g++", "-O2", "-std=c++20", "-o", POST, os.path.join(CSRC, "post_main.cpp"), "-L" + HERE,
               "-lkmertree_b200", "-Wl,-rpath,$ORIGIN/.."])
     return LIB
 

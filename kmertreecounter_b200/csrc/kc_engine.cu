@@ -18,8 +18,11 @@
 #include <chrono>
 #include <cmath>
 #include <cstdarg>
+#include <cstdlib>
 #include <cstdio>
 #include <cstring>
+#include <cerrno>
+#include <unistd.h>
 #include <condition_variable>
 #include <deque>
 #include <mutex>
@@ -34,6 +37,7 @@
 #include "kc_internal.h"
 #include "kc_kernels.cuh"
 #include "kc_scan.cuh"
+#include "kc_window.cuh"
 
 namespace {
 
@@ -141,8 +145,16 @@ struct kc_context {
     void* sink_user = nullptr;
     int sink_rc = 0;        // first non-zero sink return (guarded by pin_mu)
     bool deliver_err = false;  // a piece's copy failed (guarded by pin_mu)
-    static constexpr uint64_t PIN_BYTES = 512ull << 20;
+    static constexpr uint64_t PIN_BYTES = 128ull << 20;
     static constexpr int PIN_SLOTS = 4;
+    // input read from a file descriptor (kc_count_fastq): pieces are read
+    // into a small pinned ring by parallel preads, then copied to the device
+    int src_fd = -1;
+    static constexpr uint64_t RING_BYTES = 64ull << 20;
+    static constexpr int RING_SLOTS = 4;
+    uint8_t* ring[RING_SLOTS] = {};
+    cudaEvent_t ev_ring[RING_SLOTS] = {};
+    uint64_t ring_next = 0;
     uint8_t* pin[PIN_SLOTS] = {};
     cudaEvent_t ev_pin[PIN_SLOTS] = {};
     struct Piece {
@@ -180,6 +192,15 @@ struct kc_context {
     bool have_route = false;
     DevBuf sort_tmp, sort_hist, sort_offs, sort_sums;
     DevBuf set_tiles, tile_prefix, set_info;  // multi-set batches
+    // windowed count of 64-bit keys (kc_window.cuh): window-grouped keys,
+    // per-bucket window ids and per-window counts and key ranges
+    bool window_count = true;    // KC_WINDOW_COUNT=0 in the environment: count_routed only
+    bool win_ready = false;      // windows built for the current table layout
+    uint64_t n_wins = 0;
+    std::vector<kc::BucketWin> h_bucket_win;
+    std::vector<kc::WinInfo> h_win_info;
+    DevBuf routed2, bucket_win, win_info, win_count, win_padded, win_start, win_cursor, win_end;
+    uint64_t window_spill = 0;   // keys counted from the spill area (all batches of the run)
 
     // host mirrors
     std::vector<kc::BucketMeta> h_meta;
@@ -230,7 +251,7 @@ struct kc_context {
 namespace {
 
 const char* const kStageNames[KC_STAGE_COUNT] = {"lines", "scan", "extract_hist", "extract_scatter", "count",
-                                                  "rehash", "pack_low", "export", "sort", "init"};
+                                                  "rehash", "pack_low", "export", "sort", "init", "subroute"};
 
 cudaEvent_t next_event(kc_context* c) {
     if (c->ev_used == c->ev_pool.size()) {
@@ -438,6 +459,7 @@ int size_structures(kc_context* c, const std::vector<uint64_t>& kb, double scale
     }
     c->bloom_words = c->nw == 1 ? ts / 2 : bw;  // in 64-bit words (cells hold 32 filter bits each)
     c->table_slots_used = ts;
+    c->win_ready = false;
     CK(c->bloom.ensure(bw * sizeof(uint64_t)));
     CK(c->table.ensure(ts * c->slot_bytes + ts * c->slot_bytes / 4));  // room for a few in-place growths
     CK(c->meta.ensure(nb * sizeof(kc::BucketMeta)));
@@ -549,9 +571,179 @@ int rehash_loop(kc_context* c, uint64_t n_keys) {
             ++c->rehashes;
         }
         CKR(put(c, c->meta.p, c->h_meta.data(), nb * sizeof(kc::BucketMeta)));
+        c->win_ready = false;  // grown buckets leave the windowed count (their filter and table part)
         launch_count<NW>(c, n_keys, 0);
         CK(cudaGetLastError());
     }
+}
+
+// Windows of the current table layout, or false when some bucket's filter and
+// table have parted (a table that grew after an overflow keeps its old cells
+// as the filter): the windowed count needs the filter word in the first probe
+// cell of the key's own table.
+bool build_windows(kc_context* c) {
+    const uint32_t nb = c->n_buckets;
+    c->h_bucket_win.assign(nb, kc::BucketWin{});
+    c->h_win_info.clear();
+    for (uint32_t b = 0; b < nb; ++b) {
+        const kc::BucketMeta& m = c->h_meta[b];
+        if (m.bloom_off != m.tab_off || m.bloom_mask != m.tab_mask) return false;
+        const uint64_t cells = m.tab_mask + 1;
+        const uint32_t n = cells <= (uint64_t)kc::WIN_Z ? 1u : (uint32_t)(cells >> kc::WIN_ZSHIFT);
+        c->h_bucket_win[b] = kc::BucketWin{(uint32_t)c->h_win_info.size(), n == 1 ? kc::WIN_SINGLE : kc::WIN_ZSHIFT};
+        for (uint32_t q = 0; q < n; ++q) c->h_win_info.push_back(kc::WinInfo{b, q});
+    }
+    c->n_wins = c->h_win_info.size();
+    return true;
+}
+
+// Count the keys [off, off + n) of `routed` (off a multiple of the count
+// segment) with count_routed: the spill area of the windowed count.
+template <int NW>
+void launch_count_range(kc_context* c, uint64_t off, uint64_t n, int use_filter) {
+    constexpr int TILE = kc::count_tile<NW>();
+    constexpr int SEG = kc::count_seg<NW>();
+    join_init(c);
+    const uint64_t tiles = ceil_div(n, (uint64_t)TILE * kc::CNT_SEGS_PER_WARP);
+    if (!tiles) return;
+    kc::CountArgs a{};
+    a.routed = c->routed.as<uint8_t>() + off * (uint64_t)(8 * NW);
+    a.n_keys = n;
+    a.meta = c->meta.as<kc::BucketMeta>();
+    a.bloom = c->bloom.as<uint64_t>();
+    a.table = c->table.p;
+    a.seg_low = c->tile_low.as<uint32_t>() + off / SEG;
+    a.seg_fail = c->tile_fail.as<uint32_t>() + off / SEG;
+    a.bucket_overflow = c->overflow.as<uint32_t>();
+    a.error = c->scalars.as<uint32_t>() + 13;
+    a.bucket_shift = c->bucket_shift;
+    a.n_buckets = c->n_buckets;
+    a.use_filter = use_filter;
+    a.filter_in_table = c->nw == 1;
+    Stage st(c, KC_STAGE_COUNT_ROUTED);
+    kc::count_routed<NW><<<tiles, kc::CNT_THREADS, 0, c->stream>>>(a);
+}
+
+// Windowed count of one batch of 64-bit keys in `routed` (kc_window.cuh):
+// group the keys by window (ranges estimated from every 16th chunk, the
+// overflow of a window to a spill area; exact ranges for small batches or
+// when the spill area overflows), count every window in shared memory, even
+// windows first, then the spilled keys with count_routed.  `routed` then
+// holds the window-grouped keys with per-segment first occurrences and
+// overflowed keys as count_routed leaves them, and n_keys becomes its length.
+int window_count(kc_context* c, uint64_t& n_keys) {
+    const uint64_t nw = c->n_wins;
+    if (!c->win_ready) {
+        CK(c->bucket_win.ensure(c->n_buckets * sizeof(kc::BucketWin)));
+        CK(c->win_info.ensure(nw * sizeof(kc::WinInfo)));
+        CK(cudaMemcpyAsync(c->bucket_win.p, c->h_bucket_win.data(), c->n_buckets * sizeof(kc::BucketWin),
+                           cudaMemcpyHostToDevice, c->stream));
+        CK(cudaMemcpyAsync(c->win_info.p, c->h_win_info.data(), nw * sizeof(kc::WinInfo), cudaMemcpyHostToDevice,
+                           c->stream));
+        CK(c->win_count.ensure(nw * sizeof(uint32_t)));
+        CK(c->win_padded.ensure(nw * sizeof(uint32_t)));  // capacities
+        CK(c->win_start.ensure(nw * sizeof(uint64_t)));
+        CK(c->win_cursor.ensure(nw * sizeof(uint64_t)));
+        CK(c->win_end.ensure(nw * sizeof(uint64_t)));
+        c->win_ready = true;
+    }
+    uint64_t* d_scal = c->scalars.as<uint64_t>();
+    uint32_t* d_spill_full = c->scalars.as<uint32_t>() + 14;
+    const auto* meta = c->meta.as<kc::BucketMeta>();
+    const auto* bwin = c->bucket_win.as<kc::BucketWin>();
+    const uint64_t cchunks = ceil_div(n_keys, kc::SUB_CHUNK);
+    const uint64_t small_grid = std::min<uint64_t>(ceil_div(nw, 256), (uint64_t)c->sm_count * 8);
+    // sampled ranges need enough sampled chunks per window to be worth it
+    uint32_t stride = cchunks >= 64ull * 16 ? 16u : 1u;
+    uint64_t total = 0, spill_start = 0, spill_used = 0;
+    for (;;) {
+        CKR(fill_dev(c, c->win_count.p, nw * sizeof(uint32_t), 0));
+        {
+            Stage st(c, KC_STAGE_SUBROUTE, 2);
+            const uint64_t g = ceil_div(cchunks, stride);
+            if (g)
+                kc::subroute_count<<<g, kc::SUB_THREADS, 0, c->stream>>>(
+                    c->routed.as<uint64_t>(), n_keys, meta, bwin, c->bucket_shift, stride, c->win_count.as<uint32_t>());
+            kc::window_caps<<<small_grid, 256, 0, c->stream>>>(c->win_count.as<uint32_t>(), nw, stride,
+                                                                c->win_padded.as<uint32_t>());
+            CK(cudaGetLastError());
+        }
+        int rc;
+        if ((rc = device_scan<uint32_t, uint64_t>(c, c->win_padded.as<uint32_t>(), nw, c->win_start.as<uint64_t>(), 0,
+                                                  d_scal + 3)))
+            return rc;
+        CKR(get(c, &total, d_scal + 3, sizeof(uint64_t)));
+        CKR(sync_stream(c));
+        spill_start = total;
+        const uint64_t spill_cap = stride > 1 ? std::max<uint64_t>(1ull << 16, (total / 16 + 63) & ~63ull) : 0;
+        const uint64_t arr = total + spill_cap;
+        CK(c->routed2.ensure(std::max<uint64_t>(arr, 1) * sizeof(uint64_t)));
+        CK(c->tile_low.ensure(std::max<uint64_t>(arr / kc::WIN_SEG, 1) * sizeof(uint32_t)));
+        CK(c->tile_fail.ensure(std::max<uint64_t>(arr / kc::WIN_SEG, 1) * sizeof(uint32_t)));
+        CK(c->tile_low_prefix.ensure(std::max<uint64_t>(arr / kc::WIN_SEG, 1) * sizeof(uint64_t)));
+        CKR(put(c, d_scal + 5, &spill_start, sizeof(uint64_t)));
+        CKR(fill_dev(c, d_spill_full, sizeof(uint32_t), 0));
+        {
+            Stage st(c, KC_STAGE_SUBROUTE, n_keys ? 2 : 1);
+            kc::window_bounds<<<small_grid, 256, 0, c->stream>>>(c->win_start.as<uint64_t>(), c->win_padded.as<uint32_t>(),
+                                                                 nw, c->win_cursor.as<uint64_t>(), c->win_end.as<uint64_t>());
+            kc::ScatterArgs sa{};
+            sa.keys = c->routed.as<uint64_t>();
+            sa.n = n_keys;
+            sa.meta = meta;
+            sa.bw = bwin;
+            sa.bucket_shift = c->bucket_shift;
+            sa.win_cursor = c->win_cursor.as<unsigned long long>();
+            sa.win_end = c->win_end.as<uint64_t>();
+            sa.spill_cursor = reinterpret_cast<unsigned long long*>(d_scal + 5);
+            sa.spill_end = arr;
+            sa.spill_full = d_spill_full;
+            sa.out = c->routed2.as<uint64_t>();
+            if (n_keys)
+                kc::subroute_scatter<<<ceil_div(n_keys, kc::SCAT_CHUNK), kc::SCAT_THREADS, kc::scatter_smem_bytes(),
+                                       c->stream>>>(sa);
+            CK(cudaGetLastError());
+        }
+        uint32_t full = 0;
+        uint64_t spill_end = 0;
+        CKR(get(c, &spill_end, d_scal + 5, sizeof(uint64_t)));
+        CKR(get(c, &full, d_spill_full, sizeof(uint32_t)));
+        CKR(sync_stream(c));
+        if (full && stride > 1) {  // the estimate missed by more than the spill area: exact ranges
+            stride = 1;
+            continue;
+        }
+        if (full) return fail(KC_ERR_DEVICE, "internal error: exact window ranges overflowed");
+        spill_used = spill_end - spill_start;
+        break;
+    }
+    std::swap(c->routed, c->routed2);
+    n_keys = spill_start + spill_used;
+    CKR(join_init(c));
+    kc::WindowArgs a{};
+    a.keys = c->routed.as<uint64_t>();
+    a.win_start = c->win_start.as<uint64_t>();
+    a.win_fill = c->win_cursor.as<unsigned long long>();
+    a.win_cap = c->win_padded.as<uint32_t>();
+    a.wins = c->win_info.as<kc::WinInfo>();
+    a.bw = bwin;
+    a.meta = meta;
+    a.table = c->table.as<kc::Slot1>();
+    a.seg_low = c->tile_low.as<uint32_t>();
+    a.seg_fail = c->tile_fail.as<uint32_t>();
+    a.bucket_overflow = c->overflow.as<uint32_t>();
+    {
+        Stage st(c, KC_STAGE_COUNT_ROUTED, 2);
+        for (uint32_t ph = 0; ph < 2; ++ph) {
+            a.phase = ph;
+            kc::count_window<<<nw, kc::WIN_THREADS, kc::window_smem_bytes(), c->stream>>>(a);
+        }
+        CK(cudaGetLastError());
+    }
+    if (spill_used) launch_count_range<1>(c, spill_start, spill_used, 1);
+    c->window_spill += spill_used;
+    CK(cudaGetLastError());
+    return KC_OK;
 }
 
 // mode HIST: totals of `bins` buckets (the top log2(bins) key bits) over
@@ -748,8 +940,20 @@ int count_and_pack(kc_context* c, uint64_t n_keys, uint32_t ext_err) {
     constexpr int SEG = kc::count_seg<NW>();
     uint64_t* d_scal = c->scalars.as<uint64_t>();
     int rc;
+    bool windowed = false;
+    if constexpr (NW == 1) {
+        // 64-bit keys count in shared-memory windows while every bucket's
+        // filter sits in its table's cells (no table has grown yet)
+        // (windows pay a read and a write of every table cell per batch:
+        // worth it from 2 keys per cell, e.g. a whole input in one pass,
+        // not for the host path's batches against the whole input's tables)
+        if (c->window_count && n_keys >= 2 * c->table_slots_used && (c->win_ready || build_windows(c))) {
+            if ((rc = window_count(c, n_keys))) return rc;
+            windowed = true;
+        }
+    }
+    if (!windowed) launch_count<NW>(c, n_keys, 1);
     const uint64_t nsegs = ceil_div(n_keys, SEG);
-    launch_count<NW>(c, n_keys, 1);
     CK(cudaGetLastError());
     if ((rc = rehash_loop<NW>(c, n_keys))) return rc;
 
@@ -907,6 +1111,7 @@ int begin_run(kc_context* c, uint64_t total_bytes) {
     c->rehashes = 0;
     c->overflow_keys = 0;
     c->reroutes = 0;
+    c->window_spill = 0;
     c->batches = 0;
     c->input_bytes = 0;
     c->sized = false;
@@ -1217,10 +1422,14 @@ int kc_create(const kc_config* cfg, kc_context** out) {
                          (int)kc::extract_smem_bytes<4, kc::HIST>(4096));
     cudaFuncSetAttribute(kc::extract_kernel<4, kc::SCATTER>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)kc::extract_smem_bytes<4, kc::SCATTER>(4096));
+    cudaFuncSetAttribute(kc::count_window, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kc::window_smem_bytes());
+    cudaFuncSetAttribute(kc::subroute_scatter, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)kc::scatter_smem_bytes());
     if ((e = cudaGetLastError()) != cudaSuccess) {
         delete c;
         return fail(KC_ERR_DEVICE, "kernel attribute setup failed: %s", cudaGetErrorString(e));
     }
+    if (const char* w = std::getenv("KC_WINDOW_COUNT")) c->window_count = std::strcmp(w, "0") != 0;
     *out = c;
     return KC_OK;
 }
@@ -1234,7 +1443,9 @@ void kc_destroy(kc_context* c) {
                       &c->tile_low, &c->tile_fail, &c->tile_low_prefix, &c->scan_sums, &c->scalars, &c->overflow,
                       &c->meta,   &c->bloom,     &c->table,     &c->low_packed,   &c->roots,         &c->chunks,
                       &c->root_count, &c->chunk_pass, &c->chunk_off, &c->sort_tmp, &c->sort_hist, &c->sort_offs, &c->sort_sums,
-                      &c->set_tiles, &c->tile_prefix, &c->set_info, &c->pass_bits, &c->loads};
+                      &c->set_tiles, &c->tile_prefix, &c->set_info, &c->pass_bits, &c->loads, &c->routed2,
+                      &c->bucket_win, &c->win_info, &c->win_count, &c->win_padded, &c->win_start, &c->win_cursor,
+                      &c->win_end};
     for (DevBuf* b : bufs) b->release();
     for (cudaEvent_t e : c->ev_pool) cudaEventDestroy(e);
     if (c->h2d) cudaStreamSynchronize(c->h2d);
@@ -1247,6 +1458,10 @@ void kc_destroy(kc_context* c) {
     for (int i = 0; i < kc_context::PIN_SLOTS; ++i) {
         if (c->ev_pin[i]) cudaEventDestroy(c->ev_pin[i]);
         if (c->pin[i]) cudaFreeHost(c->pin[i]);
+    }
+    for (int i = 0; i < kc_context::RING_SLOTS; ++i) {
+        if (c->ev_ring[i]) cudaEventDestroy(c->ev_ring[i]);
+        if (c->ring[i]) cudaFreeHost(c->ring[i]);
     }
     if (c->ev_pack) cudaEventDestroy(c->ev_pack);
     if (c->ev_mbox) cudaEventDestroy(c->ev_mbox);
@@ -1333,6 +1548,32 @@ std::vector<uint64_t> plan_batches(uint64_t n, uint64_t B) {
     return v;
 }
 
+// pread of [off, off + n) into dst by up to 8 threads (page-cache copies run
+// at memory speed per thread, so a few threads read several times faster).
+static bool read_parallel(int fd, uint8_t* dst, uint64_t off, uint64_t n) {
+    const uint64_t parts = std::max<uint64_t>(1, std::min<uint64_t>(8, n >> 23));  // >= 8 MiB each
+    const uint64_t each = (n + parts - 1) / parts;
+    std::vector<std::thread> th;
+    std::vector<char> ok(parts, 0);
+    auto work = [&](uint64_t p) {
+        const uint64_t a = p * each, b = std::min<uint64_t>(n, a + each);
+        uint64_t got = a;
+        while (got < b) {
+            const ssize_t r = ::pread(fd, dst + got, b - got, (off_t)(off + got));
+            if (r < 0 && errno == EINTR) continue;
+            if (r <= 0) return;
+            got += (uint64_t)r;
+        }
+        ok[p] = 1;
+    };
+    for (uint64_t p = 1; p < parts; ++p) th.emplace_back(work, p);
+    work(0);
+    for (auto& t : th) t.join();
+    for (char v : ok)
+        if (!v) return false;
+    return true;
+}
+
 // Host input, double-buffered: batch i+1 is copied host->device on its own
 // stream (chunk_bytes pieces) while batch i is counted.  Staging buffers are
 // [HALO | batch | pad]; the HALO bytes before a batch are copied from the
@@ -1352,22 +1593,43 @@ int host_pipeline(kc_context* c, const uint8_t* fastq, uint64_t n) {
     if (nbatch > 1) CK(c->stage2.ensure(kc::HALO + cap + kc::EXT_TILE));
     uint8_t* slots[2] = {c->stage.as<uint8_t>(), c->stage2.as<uint8_t>()};
     const uint64_t chunk = std::max<uint64_t>(c->cfg.chunk_bytes, 1 << 20);
+    const bool from_file = c->src_fd >= 0;
     auto enqueue_copy = [&](uint64_t i) -> int {
         const int slot = (int)(i & 1);
         const uint64_t off = offs[i], len = plan[i];
         uint8_t* dst = slots[slot];
         if (i >= 2) CK(cudaStreamWaitEvent(c->h2d, c->ev_free[slot], 0));
-        if (off >= (uint64_t)kc::HALO) CK(cudaMemcpyAsync(dst, fastq + off - kc::HALO, kc::HALO, cudaMemcpyHostToDevice, c->h2d));
-        for (uint64_t q = 0; q < len; q += chunk)
-            CK(cudaMemcpyAsync(dst + kc::HALO + q, fastq + off + q, std::min<uint64_t>(chunk, len - q),
-                               cudaMemcpyHostToDevice, c->h2d));
+        if (from_file) {
+            // [HALO before the batch | batch] from the file, through the ring
+            const uint64_t start = off >= (uint64_t)kc::HALO ? off - kc::HALO : off;
+            uint8_t* d = off >= (uint64_t)kc::HALO ? dst : dst + kc::HALO;
+            const uint64_t total = off + len - start;
+            for (uint64_t q = 0; q < total; q += kc_context::RING_BYTES) {
+                const uint64_t m = std::min<uint64_t>(kc_context::RING_BYTES, total - q);
+                const int s = (int)(c->ring_next++ % kc_context::RING_SLOTS);
+                CK(cudaEventSynchronize(c->ev_ring[s]));  // its previous copy has left
+                if (!read_parallel(c->src_fd, c->ring[s], start + q, m))
+                    return fail(KC_ERR_IO, "Failed to read fastq data at byte %llu", (unsigned long long)(start + q));
+                CK(cudaMemcpyAsync(d + q, c->ring[s], m, cudaMemcpyHostToDevice, c->h2d));
+                CK(cudaEventRecord(c->ev_ring[s], c->h2d));
+            }
+        } else {
+            if (off >= (uint64_t)kc::HALO)
+                CK(cudaMemcpyAsync(dst, fastq + off - kc::HALO, kc::HALO, cudaMemcpyHostToDevice, c->h2d));
+            for (uint64_t q = 0; q < len; q += chunk)
+                CK(cudaMemcpyAsync(dst + kc::HALO + q, fastq + off + q, std::min<uint64_t>(chunk, len - q),
+                                   cudaMemcpyHostToDevice, c->h2d));
+        }
         CK(cudaEventRecord(c->ev_h2d[slot], c->h2d));
         return KC_OK;
     };
     int rc;
     if (nbatch && (rc = enqueue_copy(0))) return rc;
     for (uint64_t i = 0; i < nbatch; ++i) {
-        if (i + 1 < nbatch && (rc = enqueue_copy(i + 1))) return rc;
+        // host memory: the next batch's copy is queued before this batch's
+        // work; from a file, its read follows this batch's launches, so that
+        // the device counts while the host reads
+        if (!from_file && i + 1 < nbatch && (rc = enqueue_copy(i + 1))) return rc;
         const int slot = (int)(i & 1);
         CK(cudaStreamWaitEvent(c->stream, c->ev_h2d[slot], 0));
         c->after_scatter = c->ev_free[slot];
@@ -1375,6 +1637,7 @@ int host_pipeline(kc_context* c, const uint8_t* fastq, uint64_t n) {
         c->after_scatter = nullptr;
         if (rc) return rc;
         if (c->stream_low && (rc = stream_out_low(c))) return rc;
+        if (from_file && i + 1 < nbatch && (rc = enqueue_copy(i + 1))) return rc;
     }
     return KC_OK;
 }
@@ -1459,9 +1722,14 @@ int kc_count_host(kc_context* c, const uint8_t* fastq, uint64_t n, kc_stats* sta
     return KC_OK;
 }
 
-int kc_count_host_stream(kc_context* c, const uint8_t* fastq, uint64_t n, kc_sink_fn sink, void* user,
-                         kc_stats* stats) {
-    if (!c || (!fastq && n) || !sink) return fail(KC_ERR_INVALID, "null argument");
+}  // extern "C"
+
+namespace {
+
+// The streamed count of n input bytes from host memory (fastq) or from a file
+// descriptor (fd >= 0, read in pieces through the pinned ring).
+int count_stream_impl(kc_context* c, const uint8_t* fastq, int fd, uint64_t n, kc_sink_fn sink, void* user,
+                      kc_stats* stats) {
     const auto t0 = std::chrono::steady_clock::now();
     int rc = begin_run(c, n);
     if (rc) return rc;
@@ -1510,6 +1778,22 @@ int kc_count_host_stream(kc_context* c, const uint8_t* fastq, uint64_t n, kc_sin
             c->stream_low = false;
         }
     } stop{c};
+    if (fd >= 0) {
+        for (int i = 0; i < kc_context::RING_SLOTS; ++i) {
+            if (!c->ring[i] && cudaHostAlloc(reinterpret_cast<void**>(&c->ring[i]), kc_context::RING_BYTES,
+                                             cudaHostAllocDefault) != cudaSuccess) {
+                cudaGetLastError();
+                c->ring[i] = nullptr;
+                return fail(KC_ERR_NOMEM, "pinned read ring allocation failed");
+            }
+            if (!c->ev_ring[i]) CK(cudaEventCreateWithFlags(&c->ev_ring[i], cudaEventDisableTiming));
+        }
+    }
+    struct SourceGuard {
+        kc_context* c;
+        ~SourceGuard() { c->src_fd = -1; }
+    } src{c};
+    c->src_fd = fd;
     CK(cudaEventRecord(c->ev0, c->stream));
     rc = host_pipeline(c, fastq, n);
     if (!rc) rc = finish_run(c);
@@ -1527,7 +1811,23 @@ int kc_count_host_stream(kc_context* c, const uint8_t* fastq, uint64_t n, kc_sin
     return KC_OK;
 }
 
+}  // namespace
+
+extern "C" {
+
+int kc_count_host_stream(kc_context* c, const uint8_t* fastq, uint64_t n, kc_sink_fn sink, void* user,
+                         kc_stats* stats) {
+    if (!c || (!fastq && n) || !sink) return fail(KC_ERR_INVALID, "null argument");
+    return count_stream_impl(c, fastq, -1, n, sink, user, stats);
+}
+
 }  // extern "C"
+
+// The streamed count of a plain FASTQ file's n bytes read from fd (kc_count_fastq).
+int kc_internal_count_fd_stream(kc_context* c, int fd, uint64_t n, kc_sink_fn sink, void* user, kc_stats* stats) {
+    if (!c || fd < 0 || !sink) return fail(KC_ERR_INVALID, "null argument");
+    return count_stream_impl(c, nullptr, fd, n, sink, user, stats);
+}
 
 namespace {
 
@@ -1695,7 +1995,45 @@ extern "C" int kc_bucket_loads(kc_context* c, uint64_t* distinct, uint64_t* tabl
 
 int kc_internal_set_error(int code, const char* msg) { return fail(code, "%s", msg); }
 
+namespace {
+template <int NW>
+int prefix_counts_impl(kc_context* c, const uint8_t* host, uint64_t n, uint64_t* counts) {
+    const uint64_t tiles = ceil_div(n, kc::EXT_TILE);
+    CK(c->stage.ensure(kc::HALO + n + kc::EXT_TILE));
+    uint8_t* buf = c->stage.as<uint8_t>() + kc::HALO;
+    CK(cudaMemcpyAsync(buf, host, n, cudaMemcpyHostToDevice, c->stream));
+    CK(c->tile_nl.ensure(std::max<uint64_t>(tiles, 1) * sizeof(uint32_t)));
+    CK(c->tile_line.ensure(std::max<uint64_t>(tiles, 1) * sizeof(uint64_t)));
+    CK(c->scalars.ensure(64));
+    CK(c->bucket_count.ensure(256 * sizeof(uint64_t)));
+    CKR(fill_dev(c, c->scalars.as<uint32_t>() + 12, sizeof(uint32_t), 0));
+    CKR(fill_dev(c, c->bucket_count.p, 256 * sizeof(uint64_t), 0));
+    if (tiles) {
+        kc::lines_per_tile<<<tiles, kc::EXT_THREADS, 0, c->stream>>>(buf, n, c->tile_nl.as<uint32_t>());
+        CK(cudaGetLastError());
+        int rc = device_scan<uint32_t, uint64_t>(c, c->tile_nl.as<uint32_t>(), tiles, c->tile_line.as<uint64_t>(), 0,
+                                                 c->scalars.as<uint64_t>());
+        if (rc) return rc;
+        if ((rc = launch_extract<NW>(c, buf, n, 0, kc::HIST, 256, 1))) return rc;
+    }
+    CKR(get(c, counts, c->bucket_count.p, 256 * sizeof(uint64_t)));
+    return sync_stream(c);
+}
+}  // namespace
+
+// Canonical k-mers per root prefix (key word 0 >> 56) of FASTQ bytes in host
+// memory, counted exactly on the context's device (every tile's histogram).
+int kc_internal_prefix_counts(kc_context* c, const uint8_t* host, uint64_t n, uint64_t* counts) {
+    if (!c || (!host && n) || !counts) return fail(KC_ERR_INVALID, "null argument");
+    CK(cudaSetDevice(c->device));
+    c->readbacks.clear();
+    c->mbox_up_off = c->mbox_down_off = 0;
+    return c->nw == 1 ? prefix_counts_impl<1>(c, host, n, counts)
+                      : (c->nw == 2 ? prefix_counts_impl<2>(c, host, n, counts) : prefix_counts_impl<4>(c, host, n, counts));
+}
+
 uint64_t kc_internal_record_bytes(const kc_context* c) { return c ? c->record_bytes : 0; }
+uint32_t kc_internal_k(const kc_context* c) { return c ? c->cfg.k : 0; }
 
 // ------------------------------------------------------------------ batches
 //

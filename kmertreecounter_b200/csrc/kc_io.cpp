@@ -191,6 +191,36 @@ int kc_count_fastq(const kc_config* cfg, const char* fastq_path, const char* out
     kc_context* ctx = nullptr;
     int rc = kc_create(cfg, &ctx);
     if (rc) return rc;
+    // a plain file streams from disk: pieces are read (parallel preads into a
+    // small pinned ring) while earlier batches are counted, and the input is
+    // not bounded by host memory; gzip input is inflated first
+    {
+        const int fd = ::open(fastq_path, O_RDONLY);
+        if (fd < 0) {
+            kc_destroy(ctx);
+            return io_fail(std::string("Failed to open file ") + fastq_path + ": " + std::strerror(errno));
+        }
+        unsigned char magic[2] = {0, 0};
+        struct stat st;
+        const bool plain = fstat(fd, &st) == 0 && S_ISREG(st.st_mode) &&
+                           !(::pread(fd, magic, 2, 0) == 2 && magic[0] == 0x1F && magic[1] == 0x8B);
+        if (plain) {
+            fs.low_fd = ::open((fs.dir + "low.bin").c_str(), O_WRONLY | O_CREAT | O_TRUNC, 0644);
+            if (fs.low_fd < 0) {
+                rc = io_fail("Failed to open export file: " + fs.dir + "low.bin");
+            } else {
+                rc = kc_internal_count_fd_stream(ctx, fd, (uint64_t)st.st_size, &FileSink::call, &fs, stats);
+                if (rc == KC_ERR_IO && !fs.err.empty()) io_fail(fs.err);
+                if (::close(fs.low_fd) != 0 && rc == KC_OK) rc = io_fail("close of low.bin failed");
+                if (fs.root_fd >= 0 && ::close(fs.root_fd) != 0 && rc == KC_OK)
+                    rc = io_fail("close of a root file failed");
+            }
+            ::close(fd);
+            kc_destroy(ctx);
+            return rc;
+        }
+        ::close(fd);
+    }
     uint8_t* data = nullptr;
     uint64_t n = 0;
     if ((rc = read_fastq(fastq_path, &data, &n)) == KC_OK) {

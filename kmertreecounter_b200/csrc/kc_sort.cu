@@ -1,4 +1,5 @@
-// Root-record radix sort (replaces sort/ExportRecordRadixSort.h:19-269).
+// Root-record radix sort (replaces sort/ExportRecordRadixSort.h:19-269), and
+// the same sort over bare keys (post-processing's sorted low keys).
 //
 // The reference's LSD radix sort orders ExportRecord<N> by key with 8-bit
 // digits, skipping bits shared by a leaf; here the records of all 256 root
@@ -51,23 +52,16 @@ __device__ __forceinline__ uint32_t digit_of(const uint64_t* rec, uint32_t bit) 
     }
 }
 
-template <int NW>
-struct Rec;
-template <>
-struct Rec<1> {
-    uint64_t w[2];  // key, count|pad
-};
-template <>
-struct Rec<2> {
-    uint64_t w[3];  // key word 0, key word 1, count|pad
-};
-template <>
-struct Rec<4> {
-    uint64_t w[5];  // key words 0..3, count|pad
+// A record of W 64-bit words whose first NW words are the key: an
+// ExportRecord<NW> (W = NW + 1: key words, then count|pad) or a bare key
+// (W = NW).
+template <int W>
+struct Rec {
+    uint64_t w[W];
 };
 
-template <int NW>
-__global__ void __launch_bounds__(SORT_THREADS) upsweep(const Rec<NW>* __restrict__ in, uint64_t n, uint32_t bit,
+template <int NW, int W>
+__global__ void __launch_bounds__(SORT_THREADS) upsweep(const Rec<W>* __restrict__ in, uint64_t n, uint32_t bit,
                                                          uint32_t* __restrict__ hist, uint64_t n_tiles) {
     __shared__ uint32_t h[RADIX];
     h[threadIdx.x] = 0;
@@ -82,8 +76,8 @@ __global__ void __launch_bounds__(SORT_THREADS) upsweep(const Rec<NW>* __restric
     hist[(uint64_t)threadIdx.x * n_tiles + blockIdx.x] = h[threadIdx.x];
 }
 
-template <int NW>
-__global__ void __launch_bounds__(SORT_THREADS) downsweep(const Rec<NW>* __restrict__ in, Rec<NW>* __restrict__ out,
+template <int NW, int W>
+__global__ void __launch_bounds__(SORT_THREADS) downsweep(const Rec<W>* __restrict__ in, Rec<W>* __restrict__ out,
                                                            uint64_t n, uint32_t bit, const uint64_t* __restrict__ offs,
                                                            uint64_t n_tiles) {
     __shared__ uint32_t base[RADIX];                        // running count per digit inside the tile
@@ -100,7 +94,7 @@ __global__ void __launch_bounds__(SORT_THREADS) downsweep(const Rec<NW>* __restr
         __syncthreads();
         const uint64_t i = t0 + (uint64_t)r * SORT_THREADS + tid;
         const bool valid = i < n;
-        Rec<NW> rec;
+        Rec<W> rec;
         uint32_t d = 0, rank_in_warp = 0;
         const uint32_t active = __ballot_sync(0xffffffffu, valid);
         if (valid) {
@@ -126,9 +120,9 @@ __global__ void __launch_bounds__(SORT_THREADS) downsweep(const Rec<NW>* __restr
     }
 }
 
-template <int NW>
+template <int NW, int W>
 int sort_impl(void* records, uint64_t n, uint32_t k, const KcSortScratch& w, cudaStream_t st) {
-    using R = Rec<NW>;
+    using R = Rec<W>;
     const uint32_t key_bits = 2 * k;
     const uint32_t lowbit = 64 * NW - key_bits;
     const uint32_t passes = (key_bits + 7) / 8;
@@ -142,12 +136,12 @@ int sort_impl(void* records, uint64_t n, uint32_t k, const KcSortScratch& w, cud
     uint64_t* sums = static_cast<uint64_t*>(w.sums);
     for (uint32_t p = 0; p < passes; ++p) {
         const uint32_t bit = lowbit + 8 * p;
-        upsweep<NW><<<n_tiles, SORT_THREADS, 0, st>>>(src, n, bit, hist, n_tiles);
+        upsweep<NW, W><<<n_tiles, SORT_THREADS, 0, st>>>(src, n, bit, hist, n_tiles);
         const uint64_t nb = (hn + kc::SCAN_TILE - 1) / kc::SCAN_TILE;
         kc::scan_reduce<uint32_t><<<nb, kc::SCAN_BLOCK, 0, st>>>(hist, hn, sums);
         kc::scan_sums<<<1, kc::SCAN_BLOCK, 0, st>>>(sums, nb, 0, nullptr);
         kc::scan_apply<uint32_t, uint64_t><<<nb, kc::SCAN_BLOCK, 0, st>>>(hist, hn, sums, offs);
-        downsweep<NW><<<n_tiles, SORT_THREADS, 0, st>>>(src, dst, n, bit, offs, n_tiles);
+        downsweep<NW, W><<<n_tiles, SORT_THREADS, 0, st>>>(src, dst, n, bit, offs, n_tiles);
         std::swap(src, dst);
     }
     cudaError_t e = cudaGetLastError();
@@ -174,10 +168,19 @@ void kc_sort_scratch_bytes(uint64_t n, uint64_t record_bytes, uint64_t* tmp, uin
 int kc_sort_roots(void* records, uint64_t n, uint64_t record_bytes, uint32_t k, const KcSortScratch& w,
                   cudaStream_t stream) {
     if (n < 2) return KC_OK;
-    if (record_bytes == 16 && k <= 32) return sort_impl<1>(records, n, k, w, stream);
-    if (record_bytes == 24 && k <= 64) return sort_impl<2>(records, n, k, w, stream);
-    if (record_bytes == 40 && k <= 128) return sort_impl<4>(records, n, k, w, stream);
+    if (record_bytes == 16 && k <= 32) return sort_impl<1, 2>(records, n, k, w, stream);
+    if (record_bytes == 24 && k <= 64) return sort_impl<2, 3>(records, n, k, w, stream);
+    if (record_bytes == 40 && k <= 128) return sort_impl<4, 5>(records, n, k, w, stream);
     g_sort_err = "unsupported record layout";
+    return KC_ERR_INVALID;
+}
+
+int kc_sort_keys(void* keys, uint64_t n, uint32_t nw, uint32_t k, const KcSortScratch& w, cudaStream_t stream) {
+    if (n < 2) return KC_OK;
+    if (nw == 1 && k <= 32) return sort_impl<1, 1>(keys, n, k, w, stream);
+    if (nw == 2 && k <= 64) return sort_impl<2, 2>(keys, n, k, w, stream);
+    if (nw == 4 && k <= 128) return sort_impl<4, 4>(keys, n, k, w, stream);
+    g_sort_err = "unsupported key width";
     return KC_ERR_INVALID;
 }
 

@@ -14,8 +14,11 @@
 // "Total read k-mer count: X" (src/main.cpp:266) and
 // "High frequency unique k-mer : R" (src/main.cpp:309).
 //
+// Before counting it prints the reference's Stage-0 lines ("Thread split",
+// "Average prefix count", "Classifier i total prefix count", "Max Bloom
+// Filter capacity"), computed from the reference's own sample and rules.
 // Extra environment knobs (not in the reference): KC_DEVICE, KC_BUCKETS,
-// KC_SORT (0/1), KC_OUT_DIR.
+// KC_SORT (0/1), KC_OUT_DIR, KC_STAGE0 (0: skip the Stage-0 report).
 
 #include <cstdio>
 #include <cstdlib>
@@ -85,17 +88,40 @@ int main(int argc, char* argv[]) {
     if (const char* s = std::getenv("KC_SORT")) cfg.sort_output = (uint32_t)std::atoi(s);
     const char* out_dir = std::getenv("KC_OUT_DIR");
 
+    // Stage 0 as the reference reports it (src/main.cpp:111-186): thread
+    // split, then the sampled prefix counts' average, the classifier loads and
+    // the largest filter.  Informational: the count below sizes its
+    // structures from exact per-bucket totals.  KC_STAGE0=0 skips it.
+    const char* s0 = std::getenv("KC_STAGE0");
+    if (!s0 || std::string(s0) != "0") {
+        const unsigned long parsers = n_thread / 8 > 0 ? n_thread / 8 : 1;
+        const unsigned long budget = n_thread - 2 - parsers;
+        const unsigned long classifiers = budget / 2 ? budget / 2 : 1;
+        std::cout << "Thread split:" << std::endl;
+        std::cout << "  parser threads: " << parsers << std::endl;
+        std::cout << "  classifier threads: " << classifiers << std::endl;
+        std::cout << "  task threads: " << budget - classifiers << std::endl;
+        kc_stage0 s;
+        const int src = kc_stage0_file(&cfg, filename.c_str(), (uint32_t)n_thread, &s);
+        if (src != KC_OK) {
+            std::cerr << kc_last_error() << std::endl;
+            return src == KC_ERR_INVALID ? 1 : 255;
+        }
+        std::cout << "Average prefix count: " << s.average_prefix_count << std::endl;
+        for (uint32_t i = 0; i < s.classifier_num; ++i)
+            std::cout << "Classifier " << s.load_order[i] << " total prefix count: "
+                      << s.classifier_load[s.load_order[i]] << std::endl;
+        std::cout << "Max Bloom Filter capacity: " << s.max_bloom_filter_capacity << std::endl;
+    }
+
     kc_stats st;
     const int rc = kc_count_fastq(&cfg, filename.c_str(), out_dir ? out_dir : "./tmp/", &st);
     if (rc != KC_OK) {
         std::cerr << kc_last_error() << std::endl;
         return rc == KC_ERR_INVALID ? 1 : 255;
     }
-    // Stage-0 figures of the reference (src/main.cpp:88-108, :186), here
-    // from the exact per-bucket totals instead of a 256 MB sample
-    std::cout << "Average prefix count: " << st.total_kmers / 256 << std::endl;
-    std::cout << "Max Bloom Filter capacity: " << st.max_bucket_filter_words << std::endl;
-    std::cout << "Max repeat table capacity: " << st.max_bucket_table_slots << std::endl;
+    std::cout << "Largest filter of this count (64-bit words): " << st.max_bucket_filter_words << std::endl;
+    std::cout << "Largest repeat table of this count (slots): " << st.max_bucket_table_slots << std::endl;
     std::cout << "Total read k-mer count: " << st.total_kmers << std::endl;
     std::cout << "Low frequency k-mer (low.bin records): " << st.low_records << std::endl;
     std::cout << "Device elapsed ms: " << st.device_ms << std::endl;

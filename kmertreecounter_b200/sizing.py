@@ -278,3 +278,72 @@ def relative_error(pred, true):
     pred = np.asarray(pred, np.float64)
     m = true > 0
     return np.abs(pred[m] - true[m]) / true[m]
+
+
+# ------------------------------------------------------------------ Stage-0 side by side
+
+def stage0_report(path, k, n_thread=8, model=None, device=0, read_len=150, bloom_bits=5.0):
+    """Per root prefix (key word 0 >> 56), the first-occurrence filter each
+    sizing rule gives for the FASTQ at `path`, in 64-bit words:
+
+      reference   the reference's Stage 0: its own 256 MB sample and
+                  calculate_bloom_filter_capacity (src/main.cpp:88-108),
+                  with its classifier owner (src/main.cpp:38-86)
+      sampled     this build's plain rule on the exact k-mer totals of the
+                  whole input: bit_ceil(k-mers x bloom_bits / 64), >= 256
+      learned     the sizing model's rule: bit_ceil(predicted distinct keys
+                  x 12 / 64), >= 256 (the model run on the first 1% of reads)
+      distinct    the exact number of distinct keys (the quantity both the
+                  reference's 4.81 bits and the learned 12 bits are per)
+
+    Returns a dict of numpy arrays of length 256 plus the KcStage0 record."""
+    from ._native import Counter
+    s0 = _native.stage0_file(path, k=k, n_thread=n_thread, device=device)
+    data = np.fromfile(path, np.uint8)
+    with Counter(k=k, device=device) as c:
+        c.count_host(data)
+        dist, _, km = bucket_loads(c)
+    per = MODEL_BUCKETS // 256
+    km256 = km.reshape(256, per).sum(axis=1).astype(np.float64)
+    d256 = dist.reshape(256, per).sum(axis=1).astype(np.float64)
+
+    def ceil2(x):
+        x = np.maximum(x.astype(np.float64), 256.0)
+        return (2.0 ** np.ceil(np.log2(x))).astype(np.int64)
+
+    out = {"prefix": np.arange(256), "reference": np.array(s0.bloom_filter_capacity, np.int64),
+           "owner": np.array(s0.prefix_owner, np.int64), "sampled": ceil2(km256 * bloom_bits / 64.0),
+           "distinct": d256.astype(np.int64), "kmers": km256.astype(np.int64), "stage0": s0}
+    if model is not None:
+        with Counter(k=k, device=device) as c:
+            d_pred, _ = predict_host(c, model, data, k, read_len)
+        out["learned"] = ceil2(np.asarray(d_pred, np.float64).reshape(256, per).sum(axis=1) * 12.0 / 64.0)
+    return out
+
+
+def _main(argv):
+    import argparse
+    ap = argparse.ArgumentParser(prog="python -m kmertreecounter_b200.sizing")
+    sub = ap.add_subparsers(dest="cmd", required=True)
+    st = sub.add_parser("stage0", help="the reference's Stage-0 filter sizes beside this build's rules")
+    st.add_argument("fastq")
+    st.add_argument("k", type=int)
+    st.add_argument("--threads", type=int, default=8)
+    st.add_argument("--read-len", type=int, default=150)
+    a = ap.parse_args(argv)
+    model = MLP.load() if os.path.exists(MODEL_PATH) else None
+    r = stage0_report(a.fastq, a.k, a.threads, model, read_len=a.read_len)
+    s0 = r["stage0"]
+    print(f"Average prefix count: {s0.average_prefix_count}")
+    for i, load in s0.loads_in_print_order():
+        print(f"Classifier {i} total prefix count: {load}")
+    print(f"Max Bloom Filter capacity: {s0.max_bloom_filter_capacity}")
+    cols = ["prefix", "owner", "kmers", "distinct", "reference", "sampled"] + (["learned"] if "learned" in r else [])
+    print("\t".join(cols))
+    for p in range(256):
+        print("\t".join(str(int(r[c][p])) for c in cols))
+
+
+if __name__ == "__main__":
+    import sys
+    _main(sys.argv[1:])

@@ -24,6 +24,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB = os.path.join(HERE, "_build", "libkmer_oracle.so")
 REF_TREE = os.path.join(HERE, "_ref", "Tree")
 REF_HIST = os.path.join(HERE, "_ref", "histogram_tool")
+REF_STAGE0 = os.path.join(HERE, "_ref", "stage0")
+REF_POST = os.path.join(HERE, "_ref", "postprocess")
 # where build() looks for the reference's sources (absent on machines that
 # only carry the prebuilt oracle/_ref binaries)
 REF_SRC = os.environ.get("KC_REFERENCE_SRC", "/root/reference")
@@ -37,7 +39,7 @@ def build():
     src = os.path.join(HERE, "kmer_oracle.cpp")
     if not os.path.exists(LIB) or os.path.getmtime(LIB) < os.path.getmtime(src):
         subprocess.check_call(["make", "-s", "-C", HERE, "oracle"])
-    if not os.path.exists(REF_TREE):
+    if not all(os.path.exists(p) for p in (REF_TREE, REF_STAGE0, REF_POST)):
         subprocess.call(["make", "-s", "-C", HERE, "ref", f"REF={REF_SRC}"])
 
 

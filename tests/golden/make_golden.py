@@ -13,10 +13,12 @@ source files).  For every case this script:
 The oracle itself is NOT used to produce the recorded values; the tests
 compare the oracle (CPU) and the GPU path against them.
 
-    python tests/golden/make_golden.py [--only name,name,...]
+    python tests/golden/make_golden.py [--only name,name,...] [--stage0-only]
 
 With --only, the named cases are (re)generated and merged into the existing
-golden.json; the others are kept as they are.  The full genome-scale case
+golden.json; the others are kept as they are.  --stage0-only adds the
+reference's Stage-0 report (average prefix count, classifier loads, largest
+Bloom filter; src/main.cpp:38-108, :174-186) to the cases of STAGE0_CASES.  The full genome-scale case
 needs ~40 GB of host memory and ~20 GB of disk for the reference's outputs.
 """
 import hashlib
@@ -52,6 +54,22 @@ CASES = [
 RESOURCES = {"genome_scale_full": (8, 40)}
 
 
+def stage0_lines(stdout, threads):
+    """The reference's Stage-0 report (src/main.cpp:174-186, :38-108): the
+    average prefix count, each classifier's load in print order and the
+    largest Bloom filter capacity."""
+    out = {"n_thread": threads, "loads": []}
+    for line in stdout.splitlines():
+        if line.startswith("Average prefix count:"):
+            out["average"] = int(line.split(":")[1])
+        elif line.startswith("Classifier ") and "total prefix count:" in line:
+            head, val = line.split(":")
+            out["loads"].append([int(head.split()[1]), int(val)])
+        elif line.startswith("Max Bloom Filter capacity:"):
+            out["max_capacity"] = int(line.split(":")[1])
+    return out
+
+
 def reference_case(fq, K_oracle, k, workdir, tries=4, threads=8, mem_gb=4):
     for attempt in range(tries):
         tmp = os.path.join(workdir, "tmp")
@@ -82,6 +100,7 @@ def reference_case(fq, K_oracle, k, workdir, tries=4, threads=8, mem_gb=4):
     with open(hist_file) as f:
         tool_hist = [int(line.split("\t")[1]) for line in f if line.strip()]
     return {
+        "stage0": stage0_lines(out, threads),
         "k": k,
         "K": K_ref,
         "D": int(keys.shape[0]),
@@ -95,6 +114,43 @@ def reference_case(fq, K_oracle, k, workdir, tries=4, threads=8, mem_gb=4):
     }
 
 
+# (case, k) pairs whose Stage-0 report is recorded by --stage0-only
+STAGE0_CASES = [("plain_small", 31), ("plain_small_s7", 21), ("plain_small_s7", 63), ("adversarial", 17),
+                ("adversarial", 33), ("genome_scale_s05", 31), ("large_long_s02", 63), ("genome_scale_full", 31)]
+
+
+def stage0_only(golden, wd):
+    """Add the reference's Stage-0 report to existing entries: two reference
+    runs must print the same report (its sampling threads could in principle
+    drop a block, as its counting threads do on small inputs)."""
+    for name, k in STAGE0_CASES:
+        if name not in golden or str(k) not in golden[name]["k"]:
+            continue
+        e = golden[name]
+        builder = next(b for n, b, kw, ks in CASES if n == name)
+        data = getattr(inputs, builder)(**e["kwargs"])
+        assert hashlib.sha256(data).hexdigest() == e["fastq_sha256"], "input generator drifted"
+        fq = os.path.join(wd, "in.fastq")
+        with open(fq, "wb") as f:
+            f.write(data)
+        del data
+        threads, mem_gb = RESOURCES.get(name, (8, 4))
+        reports = []
+        for _ in range(4):
+            out, rc = oracle.run_reference(fq, k, wd, threads=threads, mem_gb=mem_gb)
+            if rc == 0:
+                reports.append(stage0_lines(out, threads))
+            if len(reports) >= 2 and reports[-1] == reports[-2]:
+                break
+        else:
+            raise RuntimeError(f"{name} k={k}: no two matching Stage-0 reports")
+        print(f"{name} k={k}: {reports[-1]['average']} {reports[-1]['loads']} {reports[-1]['max_capacity']}", flush=True)
+        e["k"][str(k)]["stage0"] = reports[-1]
+        tmp = os.path.join(wd, "tmp")
+        for f in os.listdir(tmp):
+            os.remove(os.path.join(tmp, f))
+
+
 def main():
     oracle.build()
     only = None
@@ -105,6 +161,15 @@ def main():
     if only and os.path.exists(path):
         with open(path) as f:
             golden = json.load(f)
+    if "--stage0-only" in sys.argv:
+        with open(path) as f:
+            golden = json.load(f)
+        with tempfile.TemporaryDirectory(dir=os.environ.get("KC_GOLDEN_TMP")) as wd:
+            stage0_only(golden, wd)
+        with open(path, "w") as f:
+            json.dump(golden, f, indent=1, sort_keys=True)
+        print("wrote", path)
+        return
     with tempfile.TemporaryDirectory(dir=os.environ.get("KC_GOLDEN_TMP")) as wd:
         for name, builder, kw, ks in CASES:
             if only and name not in only:

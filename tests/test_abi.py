@@ -51,7 +51,8 @@ def test_struct_layout_matches_header(tmp_path):
     """Every ctypes mirror of a header struct has the C compiler's size and
     field offsets."""
     structs = {"kc_config": _native.KcConfig, "kc_stats": _native.KcStats,
-               "kc_set_desc": _native.KcSetDesc, "kc_set_result": _native.KcSetResult, "kc_peaks": _native.KcPeaks}
+               "kc_set_desc": _native.KcSetDesc, "kc_set_result": _native.KcSetResult, "kc_peaks": _native.KcPeaks,
+               "kc_stage0": _native.KcStage0, "kc_post_stats": _native.KcPostStats}
     lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "kmer_count.h"', '#include "kmer_peaks.h"',
              "int main(void) {"]
     for cname, py in structs.items():

@@ -266,3 +266,27 @@ def test_shared_prefix_keys(k):
     with kc.Counter(k=k) as c:
         c.count_host(data)
         parity.check_exact(c, data, k)
+
+
+@pytest.mark.parametrize("buckets", [256, 4096])
+@pytest.mark.parametrize("small_tables", [False, True])
+def test_windowed_count_matches_global_count(monkeypatch, buckets, small_tables):
+    """64-bit keys count in shared-memory table windows (kc_window.cuh) unless
+    KC_WINDOW_COUNT=0 selects the global-memory count kernel: both give the
+    oracle's exact counts, over several device passes, with buckets of one
+    and of many windows, and with tables small enough to overflow (the
+    windowed pass leaves overflowed keys to the global retry after growth)."""
+    p = synth.genome_scale(seed=12, scale=0.01)
+    data = synth.fastq(p)
+    want = oracle.count(data, 31)
+    for env in ("1", "0"):
+        monkeypatch.setenv("KC_WINDOW_COUNT", env)
+        # small tables: 1 filter bit and 0.002 repeat keys per k-mer against
+        # ~0.04 distinct repeated keys per k-mer at 30x
+        knobs = dict(bloom_bits=1.0, repeat_ratio=0.002) if small_tables else {}
+        with kc.Counter(k=31, n_buckets=buckets, batch_bytes=16 << 20, **knobs) as c:
+            st = c.count_host(data)
+            assert st.batches > 1
+            if small_tables:
+                assert st.rehashes > 0
+            parity.check_exact(c, data, 31, want)
