@@ -16,8 +16,11 @@ binary built from the reference sources into oracle/_ref, else the oracle
 port) on a bounded sample of the same workload, with all host threads.
 
 Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-Multi-GPU: one process per GPU under torch.distributed.run; each rank counts
-its own copy of the workload (weak scaling, no data-path collective).
+Multi-GPU: one process per GPU under torch.distributed.run; the ranks count
+ONE copy of the workload together (strong scaling): each routes its slice of
+whole records, one NCCL all-to-all sends every rank the keys of its range of
+root prefixes, each counts its range (kmertreecounter_b200/shard.py).
+`--shard` runs that form on one GPU too.
 """
 import argparse
 import ctypes
@@ -68,6 +71,9 @@ def parse():
     ap.add_argument("--ll-steps", type=int, default=3, help="timed steps of the long-key record")
     ap.add_argument("--no-file-to-file", action="store_true",
                     help="skip the command-line leg (bin/Tree vs the reference's Tree on the same file)")
+    ap.add_argument("--shard", action="store_true",
+                    help="time the sharded count (root-prefix owners, one NCCL all-to-all) even on one GPU; "
+                         "it is the default for more than one GPU")
     ap.add_argument("--write-sample", metavar="PATH", help=argparse.SUPPRESS)
     return ap.parse_args()
 
@@ -159,14 +165,20 @@ def make_workload(name, scale):
     return p, k, buckets, bases
 
 
+def sharded(args, world):
+    return world > 1 or args.shard
+
+
 def workload_config(args, world, fastq_bytes, bases, reads):
     """The `config` object of both arms' lines (the reference arm reports our
     arm's config: its steps are bounded samples of this workload)."""
     k, buckets = WORKLOADS[args.workload][1:]
     name = DESCRIBE[args.workload] if args.scale == 1.0 else f"{args.workload} scale={args.scale}"
+    par = (f"sharded x{world}: root-prefix owners, one NCCL all-to-all of routed keys" if sharded(args, world)
+           else "one GPU")
     return {"workload": name, "k": k, "n_buckets": buckets, "fastq_bytes": int(fastq_bytes), "bases": int(bases),
             "reads": int(reads), "l2": "inputs larger than L2 (FASTQ %.1f GB)" % (fastq_bytes / 1e9),
-            "parallelism": f"replica x{world}"}
+            "parallelism": par}
 
 
 def write_sample(name, scale, path):
@@ -257,7 +269,8 @@ def time_reference(path, data, k, bases, runs, workdir):
 # summarised in profiles/count_routed_genome_scale.md).  Reported only while
 # the kernel sources are unchanged since that capture.
 PROFILED_TRAFFIC = {
-    "genome_scale": {"sources_sha256": None, "bytes_per_step": None},
+    # workload: {stage: {"sources_sha256": ..., "bytes_per_step": ...}}
+    "genome_scale": {},
 }
 KERNEL_SOURCES = ("kmertreecounter_b200/csrc/kc_kernels.cuh", "kmertreecounter_b200/csrc/kc_engine.cu")
 
@@ -271,14 +284,66 @@ def kernel_sources_sha256():
     return h.hexdigest()
 
 
-def profile_traffic(args):
-    """(traffic bytes per step or None, note)."""
-    e = PROFILED_TRAFFIC.get(args.workload)
+def profile_traffic(args, stage):
+    """(traffic bytes per step of `stage` or None, note)."""
+    e = PROFILED_TRAFFIC.get(args.workload, {}).get(stage)
     if not e or args.scale != 1.0 or not e["bytes_per_step"]:
-        return None, "no capture of this workload"
+        return None, "no capture of this stage on this workload"
     if e["sources_sha256"] != kernel_sources_sha256():
         return None, "kernel sources changed since the last capture"
     return e["bytes_per_step"], "ncu capture of these kernel sources"
+
+
+STAGE_KERNELS = {
+    "extract_scatter": "extract_kernel<SCATTER> + fill_region_gaps",
+    "subroute": "subroute_count (1 chunk in 16) + window_caps + scan + subroute_scatter",
+    "count": "count_window (x2 phases) + count_routed on the spill area",
+    "pack_low": "pack_low",
+    "export": "export_count + export_write_bits",
+    "lines": "lines_per_tile",
+    "init": "init_slots (+ zero16)",
+}
+
+
+def stage_rooflines(stage_ms, stats, F, k, hbm_gbs, P, rec):
+    """Algorithmic bytes per step of every timed stage (the bytes its job has
+    to move, counted once) over its device time, against the HBM peak:
+
+      extract_scatter  F + 8N K          the FASTQ read once, every key written
+      subroute         2 x 8N K          every key read and written again, window-grouped
+      count            8N K + 8N L + 2 x 16 x cells x 9/8
+                                         (windowed count) every key read, first occurrences
+                                         written back, every table cell (16 B: key, count,
+                                         filter word) and its window's halo read and written;
+                       64 K + 64 (K - L) (global count, no windows) one 32 B filter sector read
+                                         + write per k-mer and one table sector per repeat
+      pack_low         8N L + P L        first occurrences read, packed low.bin written
+      export           16 cells + rec R  table read, root records written
+      lines            F
+      init             16 cells          table cells written"""
+    nw = 1 if k <= 32 else (2 if k <= 64 else 4)
+    K, L, R = stats["total_kmers"], stats["low_records"], stats["root_records"]
+    cells = stats["table_slots"]
+    windowed = stage_ms.get("subroute", 0.0) > 0
+    rules = {
+        "extract_scatter": (F + 8 * nw * K, "F + 8N K"),
+        "subroute": (2 * 8 * nw * K, "2 x 8N K"),
+        "count": ((8 * nw * K + 8 * nw * L + int(2 * 16 * cells * 9 / 8), "8N K + 8N L + 2 x 16 x cells x 9/8")
+                  if windowed else (64 * K + 64 * (K - L), "64 K + 64 (K - L)")),
+        "pack_low": (8 * nw * L + P * L, "8N L + P L"),
+        "export": (16 * cells + rec * R, "16 cells + rec R"),
+        "lines": (F, "F"),
+        "init": (16 * cells, "16 cells"),
+    }
+    out = {}
+    for s_, (b, rule) in rules.items():
+        ms = stage_ms.get(s_, 0.0)
+        if ms <= 0:
+            continue
+        gbs = b / (ms / 1e3) / 1e9
+        out[s_] = {"ms": ms, "alg_bytes": b, "rule": rule, "gbs": gbs, "frac": gbs / hbm_gbs,
+                   "kernels": STAGE_KERNELS[s_]}
+    return out
 
 
 def pipeline_roofline(dev_peaks, pk, F, K, L, R, P, rec, ms_step, count_ms):
@@ -367,19 +432,100 @@ def compare_batched(args, kc, torch):
     # batched: autotuned knobs and sets per pass
     best = autotune.tune(base, sets, 31, use_cache=False)
     knobs = {k: v for k, v in best.items() if k in ("table_load", "repeat_ratio", "bloom_bits")}
+    per_pass = best["sets_per_pass"]
     with kc.Counter(k=31, **knobs) as c:
-        autotune.count_in_passes(c, base, sets, best["sets_per_pass"])
+        autotune.count_in_passes(c, base, sets, per_pass)
         torch.cuda.synchronize()
         t = time.perf_counter()
-        _, res = autotune.count_in_passes(c, base, sets, best["sets_per_pass"])
+        grown = []
+        _, res = autotune.count_in_passes(c, base, sets, per_pass, grown)
         torch.cuda.synchronize()
         batched_ms = (time.perf_counter() - t) * 1e3
+        sums_batched = set_checksums(c, base, sets, per_pass, torch)
+    out = {"sets": len(sets), "bases": bases, "fastq_bytes": int(buf.size), "scale": args.batch_scale,
+           "plain": {"ms": plain_ms, "gbases_s": bases / plain_ms / 1e6},
+           "batched": {"ms": batched_ms, "gbases_s": bases / batched_ms / 1e6,
+                       "rehashes": sum(grown), "tuned": {k: v for k, v in best.items() if k != "trials"}},
+           "speedup": plain_ms / batched_ms, "kmers": int(sum(r.total_kmers for r in res))}
+    # batched + learned sizing: every pass first predicts its sets' loads (a
+    # batched count of their first 1% and one network pass), then counts
+    from kmertreecounter_b200 import sizing
+    if os.path.exists(sizing.MODEL_PATH):
+        model = sizing.MLP.load(max_batch=64)
+        read_lens = [int(p.read_len_min) for p, _ in specs]
+
+        def learned_passes(c, split):
+            st_all = []
+            for i in range(0, len(sets), per_pass):
+                t0 = time.perf_counter()
+                sizing.predict_sets(c, model, base, sets[i:i + per_pass], read_lens[i:i + per_pass])
+                torch.cuda.synchronize()
+                t1 = time.perf_counter()
+                st_all += c.count_sets(base, sets[i:i + per_pass])
+                torch.cuda.synchronize()
+                split[0] += (t1 - t0) * 1e3
+                split[1] += (time.perf_counter() - t1) * 1e3
+                split[2] += int(c.stats.rehashes)
+            return st_all
+
+        with kc.Counter(k=31, sizing=kc.KC_SIZING_LEARNED, **knobs) as c:
+            learned_passes(c, [0.0, 0.0, 0])
+            torch.cuda.synchronize()
+            split = [0.0, 0.0, 0]
+            t = time.perf_counter()
+            res_l = learned_passes(c, split)
+            torch.cuda.synchronize()
+            learned_ms = (time.perf_counter() - t) * 1e3
+            sums_learned = set_checksums(c, base, sets, per_pass, torch, learned=(model, read_lens))
+        out["batched_learned"] = {"ms": learned_ms, "gbases_s": bases / learned_ms / 1e6,
+                                  "speedup_vs_plain": plain_ms / learned_ms,
+                                  "speedup_vs_batched": batched_ms / learned_ms,
+                                  "predict_ms": split[0], "count_ms": split[1], "rehashes": split[2],
+                                  "identical_counts": sums_learned == sums_batched,
+                                  "kmers": int(sum(r.total_kmers for r in res_l))}
     del dev
-    return {"sets": len(sets), "bases": bases, "fastq_bytes": int(buf.size), "scale": args.batch_scale,
-            "plain": {"ms": plain_ms, "gbases_s": bases / plain_ms / 1e6},
-            "batched": {"ms": batched_ms, "gbases_s": bases / batched_ms / 1e6,
-                        "tuned": {k: v for k, v in best.items() if k != "trials"}},
-            "speedup": plain_ms / batched_ms, "kmers": int(sum(r.total_kmers for r in res))}
+    return out
+
+
+def set_checksums(c, base, sets, per_pass, torch, learned=None):
+    """Per set, a checksum of the exact (k-mer, count) multiset that does not
+    depend on how the first-occurrence filter split it between low.bin and
+    the root files: sum over low.bin keys of h(key) + sum over root records of
+    h(key) x count (mod 2^64), h = a 64-bit mixer, computed on the device."""
+    from kmertreecounter_b200 import sizing
+    sums = []
+    for i in range(0, len(sets), per_pass):
+        part = sets[i:i + per_pass]
+        if learned:
+            sizing.predict_sets(c, learned[0], base, part, learned[1][i:i + per_pass])
+        res = c.count_sets(base, part)
+        d_low, low_bytes, d_roots, n_roots = c.device_results()
+        low = torch.empty(max(low_bytes, 8), dtype=torch.uint8, device="cuda")
+        roots = torch.empty(max(n_roots * 16, 16), dtype=torch.uint8, device="cuda")
+        c.copy_low_into(low.data_ptr(), low_bytes)
+        c.copy_roots_into(roots.data_ptr(), n_roots * 16)
+        rr = roots[:n_roots * 16].view(torch.int64).view(-1, 2)
+        for (o, b, k), r in zip(part, res):
+            P = kc_packed(k)
+            lk = low[r.low_offset:r.low_offset + r.low_records * P].view(-1, P)
+            w = torch.zeros(lk.shape[0], dtype=torch.int64, device="cuda")
+            for q in range(P):  # the packed tail bytes sit at the top of the word
+                w |= lk[:, q].to(torch.int64) << (8 * (q + 8 - P))
+            rec = rr[r.root_offset:r.root_offset + r.root_records]
+            sums.append(int((_mix(w).sum() + (_mix(rec[:, 0]) * (rec[:, 1] & 0xFFFFFFFF)).sum()).item()) % (1 << 64))
+    return sums
+
+
+def kc_packed(k):
+    return (k // 32) * 8 + (2 * (k % 32) + 7) // 8
+
+
+def _mix(x):
+    """64-bit mixer in int64 arithmetic (wrapping), for set_checksums."""
+    x = x ^ ((x >> 31) & 0x1FFFFFFFF)
+    x = x * -7046029254386353131
+    x = x ^ ((x >> 29) & 0x7FFFFFFFF)
+    return x * -4658895280553007687
 
 
 def compare_sizing(args, kc, torch, dev, n, k, buckets, device_batch=None, steps=None):
@@ -463,7 +609,6 @@ def large_long_record(args, kc, torch, dev_peaks, pk):
         stats = st.as_dict()
         stats.pop("root_counts", None)
     K, L = stats["total_kmers"], stats["low_records"]
-    alg = 64 * K + 64 * (K - L)
     count_ms = stage_ms.get("count", 0.0) / steps
     roof = pipeline_roofline(dev_peaks, pk, n, K, L, stats["root_records"], kc.packed_bytes(k), kc.record_bytes(k),
                              ms_step, count_ms)
@@ -472,9 +617,8 @@ def large_long_record(args, kc, torch, dev_peaks, pk):
            "value": bases / (ms_step / 1e3) / 1e9, "unit": "Gbases/s", "ms_per_step": ms_step, "steps": steps,
            "distinct_kmers": distinct, "distinct_kmers_per_s": distinct / (ms_step / 1e3), "stats": stats,
            "stages_ms_per_step": {s_: v / steps for s_, v in stage_ms.items()},
-           "roofline": {"bound": "hbm", "kernel": "count_routed", "alg_bytes_per_step": alg,
-                        "achieved": alg / (count_ms / 1e3) / 1e9 if count_ms else None, "peak": pk["hbm_gbs"],
-                        "frac": alg / (count_ms / 1e3) / 1e9 / pk["hbm_gbs"] if count_ms else None},
+           "stage_rooflines": stage_rooflines({s_: v / steps for s_, v in stage_ms.items()}, stats, n, k,
+                                              pk["hbm_gbs"], kc.packed_bytes(k), kc.record_bytes(k)),
            "pipeline_roofline": roof.get("pipeline")}
     if not args.no_sizing:
         out["sizing"] = compare_sizing(args, kc, torch, dev, n, k, buckets, DEVICE_BATCH["large_long"], steps)
@@ -630,19 +774,19 @@ def run_ours(args):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_step = float(t.item())
 
-    # --- roofline of the dominant kernel (count_routed), in the fixed units of
-    # the workload definition: 64 B per k-mer (one 32 B filter sector read + write) and 64 B per
-    # repeat occurrence (one table sector read + write).
+    # --- rooflines: every stage's algorithmic bytes per step over its time
+    # (stage_rooflines), the dominant stage as the line's `roofline`, and the
+    # workload's fixed whole-step roofline (pipeline_roofline)
     from measured import peaks
     pk = peaks()
     K, L = stats["total_kmers"], stats["low_records"]
-    alg_bytes = 64 * K + 64 * (K - L)
     count_ms = stage_ms.get("count", 0.0) / args.steps
-    achieved = alg_bytes / (count_ms / 1e3) / 1e9 if count_ms > 0 else None
-    dominant = max(stage_ms, key=lambda s: stage_ms[s]) if stage_ms else None
+    per_stage = stage_rooflines({s_: v / args.steps for s_, v in stage_ms.items()}, stats, n, k, pk["hbm_gbs"],
+                                kc.packed_bytes(k), kc.record_bytes(k))
+    dominant = max(per_stage, key=lambda s_: per_stage[s_]["ms"]) if per_stage else None
     roof = pipeline_roofline(dev_peaks, pk, n, K, L, stats["root_records"], kc.packed_bytes(k), kc.record_bytes(k),
                              ms_step, count_ms)
-    traffic, traffic_note = profile_traffic(args)
+    traffic, traffic_note = profile_traffic(args, dominant)
 
     line = {
         "metric": "FASTQ Gbases/s to exact k-mer counts on 1 B200",
@@ -666,12 +810,15 @@ def run_ours(args):
         "e2e": {"value": bases * world / (e2e_step / 1e3) / 1e9, "unit": "Gbases/s", "ms_per_step": e2e_step,
                 "h2d_bytes_per_step": n, "d2h_bytes_per_step": lb + nr * rec,
                 "roofline_frac": (roof["pipeline"]["t_roof_e2e_ms"] / e2e_step) if roof.get("pipeline") else None},
-        "roofline": {"bound": "hbm", "kernel": "count_routed", "achieved": achieved, "peak": pk["hbm_gbs"],
-                     "unit": "GB/s", "frac": (achieved / pk["hbm_gbs"]) if achieved else None,
-                     "peak_source": pk["source"], "alg_bytes_per_launch": alg_bytes,
-                     "traffic": traffic, "traffic_source": traffic_note,
-                     "per": "step (all count_routed launches of one count)",
-                     "dominant_stage": dominant, "atomic": roof.get("count_routed_atomic")},
+        "roofline": dict({"bound": "hbm", "kernel": per_stage[dominant]["kernels"], "stage": dominant,
+                          "achieved": per_stage[dominant]["gbs"], "peak": pk["hbm_gbs"], "unit": "GB/s",
+                          "frac": per_stage[dominant]["frac"], "peak_source": pk["source"],
+                          "alg_bytes_per_launch": per_stage[dominant]["alg_bytes"],
+                          "alg_bytes_rule": per_stage[dominant]["rule"],
+                          "per": "step (all launches of the stage in one count)",
+                          "traffic": traffic, "traffic_source": traffic_note}) if dominant else None,
+        "stage_rooflines": per_stage,
+        "count_atomic_ceiling": roof.get("count_routed_atomic"),
         "pipeline_roofline": roof.get("pipeline"),
         "clocks": clk,
         "sizing": None,
@@ -721,6 +868,114 @@ def run_ours(args):
         print(json.dumps(line), flush=True)
 
 
+def run_sharded(args):
+    """One input over all ranks (strong scaling): every rank generates the
+    same seeded FASTQ, takes its slice of whole 4-line records
+    (shard.record_starts), and a step is route (kc_route_device on the slice)
+    -> one NCCL all-to-all of the routed keys (sent from the context's own
+    buffer) -> count of the owned root prefixes (kc_count_keys_device).
+    Timed with CUDA events around whole steps, max over ranks; value = the
+    input's bases / that time.  e2e adds, per step, the slice's host->device
+    copy from pinned memory and the device->host copy of the rank's outputs."""
+    import datetime
+    import torch
+    import torch.distributed as dist
+    import kmertreecounter_b200 as kc
+    from kmertreecounter_b200 import shard, synth
+
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    device = torch.device("cuda", local)
+    dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    try:
+        p, k, buckets, bases = make_workload(args.workload, args.scale)
+        n = synth.fastq_bytes(p)
+        host_ptr = kc.host_alloc(n)
+        synth.fastq(p, out=host_ptr)
+        host = np.ctypeslib.as_array((ctypes.c_uint8 * n).from_address(host_ptr))
+        cuts = shard.record_starts(host, world)
+        lo, hi = cuts[rank], cuts[rank + 1]
+        d_slice = torch.empty(max(hi - lo, 16), dtype=torch.uint8, device=device)[:hi - lo]
+        d_slice.copy_(torch.from_numpy(host[lo:hi]))
+        cfg = kc.default_config(k=k, n_buckets=buckets, device=local)
+        if args.workload in DEVICE_BATCH:
+            cfg.device_batch_bytes = DEVICE_BATCH[args.workload]
+        counter = kc.Counter(cfg)
+
+        launches = [0, 0]  # this rank's kernel launches: route, count (the library's counters)
+
+        def step(e2e=False):
+            if e2e:
+                d_slice.copy_(torch.from_numpy(host[lo:hi]), non_blocking=True)
+            route, count, nw = shard.gpu_stages(counter, None, device, d_slice=d_slice)
+
+            def route_counted():
+                r = route()
+                launches[0] = int(sum(v[1] for v in counter.stage_times().values()))
+                return r
+
+            st, ranges, _ = shard.exchange_and_count(route_counted, count, nw, device, dist)
+            launches[1] = int(sum(v[1] for v in counter.stage_times().values()))
+            out = 0
+            if e2e:
+                lb, nr, _ = counter.sizes()
+                out = lb + nr * kc.record_bytes(k)
+                low_h = torch.empty(max(lb, 1), dtype=torch.uint8, pin_memory=True)
+                counter.copy_low_into(low_h.data_ptr(), lb)
+                roots_h = torch.empty(max(nr * kc.record_bytes(k), 1), dtype=torch.uint8, pin_memory=True)
+                counter.copy_roots_into(roots_h.data_ptr(), nr * kc.record_bytes(k))
+            return st, out
+
+        def timed(steps, e2e=False):
+            dist.barrier()
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            out = 0
+            for _ in range(steps):
+                st, out = step(e2e)
+            torch.cuda.synchronize()
+            e1.record()
+            torch.cuda.synchronize()
+            t = torch.tensor([e0.elapsed_time(e1) / steps], device=device)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            return float(t.item()), st, out
+
+        for _ in range(max(args.warmup, 0)):
+            step()
+        clocks = ClockSampler(local)
+        clocks.start()
+        t_clk0 = time.perf_counter()
+        ms_step, st, _ = timed(args.steps)
+        clocks.mark(t_clk0, time.perf_counter())
+        clk = clocks.stop()
+        e2e_ms, _, out_bytes = timed(max(1, args.e2e_steps), e2e=True)
+        totals = torch.tensor([st.total_kmers, st.low_records, st.root_records, out_bytes], dtype=torch.int64,
+                              device=device)
+        dist.all_reduce(totals)
+        K, L, R, out_all = (int(x) for x in totals.tolist())
+        counter.close()
+        kc.host_free(host_ptr)
+        line = {
+            "metric": "FASTQ Gbases/s to exact k-mer counts on 1 B200",
+            "value": bases / (ms_step / 1e3) / 1e9, "unit": "Gbases/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "strong",
+            "vs_baseline": None, "dtype": "u64", "data": "synthetic (seeded generator, reference benchmark shape)",
+            "config": workload_config(args, world, n, bases, p.n_reads),
+            "stats": {"total_kmers": K, "low_records": L, "root_records": R},
+            "gpu_launches": (launches[0] + launches[1]) * args.steps,
+            "gpu_launches_note": "rank 0's kernel launches in the timed steps (route + count, all-to-all excluded)",
+            "e2e": {"value": bases / (e2e_ms / 1e3) / 1e9, "unit": "Gbases/s", "ms_per_step": e2e_ms,
+                    "h2d_bytes_per_step": n, "d2h_bytes_per_step": out_all},
+            "clocks": clk,
+        }
+        dist.barrier()
+        if rank == 0:
+            print(json.dumps(line), flush=True)
+    finally:
+        dist.destroy_process_group()
+
+
 # --------------------------------------------------------------- reference arm
 
 def run_reference(args):
@@ -768,6 +1023,8 @@ def main():
         return
     if args.impl == "reference":
         run_reference(args)
+    elif sharded(args, dist_env()[1]):
+        run_sharded(args)
     else:
         run_ours(args)
 

@@ -182,6 +182,12 @@ int kc_count_device(kc_context* ctx, const uint8_t* d_fastq, uint64_t n, kc_stat
  * n_keys).  Results as after kc_count_device. */
 int kc_route_device(kc_context* ctx, const uint8_t* d_fastq, uint64_t n, uint64_t* counts);
 int kc_copy_routed(kc_context* ctx, void* dst, uint64_t dst_bytes);
+/* kc_routed_keys: the routed keys where they are (device pointer into the
+ * context, 8N bytes per key, sum(counts) keys), e.g. as the send buffer of
+ * the exchange, without a copy.  Valid until the next call on the context;
+ * the caller must let its reads finish before that call (a later count on
+ * the context overwrites them). */
+int kc_routed_keys(kc_context* ctx, const void** d_keys, uint64_t* n_keys);
 int kc_count_keys_device(kc_context* ctx, const void* d_keys, uint64_t n_keys, const uint64_t* counts,
                          kc_stats* stats);
 

@@ -35,6 +35,20 @@ int kc_bucket_loads(kc_context* ctx, uint64_t* distinct, uint64_t* table_keys, u
  * on this context with cfg.sizing = KC_SIZING_LEARNED (NULL clears). */
 int kc_set_predicted_loads(kc_context* ctx, const double* distinct, const double* table_keys);
 
+/* ---- learned sizing of many read sets (kc_count_sets) -------------------
+ * Per set s, k-mers per model bucket (top 12 bits of the canonical key) of
+ * bytes [offset, offset + bytes) of each set descriptor (typically each set's
+ * first 1%): counts[s * KC_MODEL_BUCKETS + b].  No reference counterpart
+ * (the reference counts one file per process). */
+int kc_set_prefix_kmers(kc_context* ctx, const uint8_t* d_fastq, const kc_set_desc* sets, uint32_t n_sets,
+                        uint64_t* counts);
+
+/* Predicted distinct keys and table keys per (set, root bucket) -- n_sets x
+ * 256 entries each, set-major -- for the NEXT kc_count_sets of n_sets sets on
+ * this context with cfg.sizing = KC_SIZING_LEARNED (NULL clears).  A table a
+ * prediction left too small grows exactly as under the sampled rule. */
+int kc_set_predicted_set_loads(kc_context* ctx, uint32_t n_sets, const double* distinct, const double* table_keys);
+
 /* ---- the MLP ---------------------------------------------------------- */
 typedef struct kc_mlp kc_mlp;
 int kc_mlp_create(int in, int hidden, int out, int max_batch, uint64_t seed, kc_mlp** m);

@@ -30,7 +30,7 @@ ABI_SYMBOLS = (
     "kc_copy_roots", "kc_write_outputs", "kc_device_results", "kc_host_alloc", "kc_host_free", "kc_stream",
     "kc_set_profiling", "kc_stage_times", "kc_stage_name", "kc_count_device_noalloc", "kc_count_host_stream",
     "kc_histogram", "kc_count_sets", "kc_route_device", "kc_copy_routed", "kc_count_keys_device",
-    "kc_stage0_rule", "kc_stage0_file", "kc_post_process", "kc_post_process_dir",
+    "kc_stage0_rule", "kc_stage0_file", "kc_post_process", "kc_post_process_dir", "kc_routed_keys",
 )
 KC_SINK_LOW = 0
 KC_SINK_ROOT = 1
@@ -141,6 +141,7 @@ def _load():
         "kc_count_sets": (i32, [vp, vp, C.POINTER(KcSetDesc), u32, C.POINTER(KcSetResult), stp]),
         "kc_route_device": (i32, [vp, vp, u64, C.POINTER(u64)]),
         "kc_copy_routed": (i32, [vp, vp, u64]),
+        "kc_routed_keys": (i32, [vp, C.POINTER(vp), C.POINTER(u64)]),
         "kc_count_keys_device": (i32, [vp, vp, u64, C.POINTER(u64), stp]),
         "kc_measure_peaks": (i32, [i32, u64, C.POINTER(KcPeaks)]),
         "kc_stage0_rule": (i32, [C.POINTER(u64), u64, u32, C.POINTER(KcStage0)]),
@@ -260,6 +261,13 @@ class Counter:
     def copy_routed(self, addr, cap):
         """Copy the routed keys (prefix order) to addr (device or host)."""
         check(lib.kc_copy_routed(self._ctx, C.c_void_p(addr), cap))
+
+    def routed_keys(self):
+        """(device address, key count) of the routed keys inside the context
+        (valid until the next call on this context)."""
+        p, n = C.c_void_p(), C.c_uint64()
+        check(lib.kc_routed_keys(self._ctx, C.byref(p), C.byref(n)))
+        return p.value or 0, n.value
 
     def count_keys_device(self, dptr, n_keys, counts):
         """Count n_keys routed canonical keys in device memory as one input."""

@@ -45,8 +45,9 @@ def signature(sets):
     return hashlib.sha1(key.encode()).hexdigest()[:16]
 
 
-def count_in_passes(counter, dptr, sets, per_pass):
-    """kc_count_sets over `sets` in groups of `per_pass`; device ms total."""
+def count_in_passes(counter, dptr, sets, per_pass, rehashes=None):
+    """kc_count_sets over `sets` in groups of `per_pass`; device ms total.
+    `rehashes`, a list, receives each pass's table growth steps."""
     ms = 0.0
     results = []
     for i in range(0, len(sets), per_pass):
@@ -54,6 +55,8 @@ def count_in_passes(counter, dptr, sets, per_pass):
         base = group[0][0]
         res = counter.count_sets(dptr + base, [(o - base, b, k) for o, b, k in group])
         ms += counter.stats.device_ms
+        if rehashes is not None:
+            rehashes.append(int(counter.stats.rehashes))
         results.extend(res)
     return ms, results
 

@@ -184,6 +184,7 @@ struct kc_context {
     DevBuf low_packed;
     DevBuf roots, chunks, chunk_pass, chunk_off, root_count;
     DevBuf pass_bits;  // export: bit per table slot that passes min..max
+    DevBuf grow_jobs, grow_failed;  // table growth of many buckets at once
     DevBuf loads;      // kc_bucket_loads: per-model-bucket totals (kept: no cudaMalloc/cudaFree per call)
     uint64_t n_chunks = 0;  // entries of `chunks` (live table regions) of the last export
     // kc_route_device: keys held in `routed` (bucket order) and per routing bucket
@@ -192,6 +193,10 @@ struct kc_context {
     bool have_route = false;
     DevBuf sort_tmp, sort_hist, sort_offs, sort_sums;
     DevBuf set_tiles, tile_prefix, set_info;  // multi-set batches
+    std::vector<double> set_pred_distinct, set_pred_table;  // learned sizing per (set, root bucket)
+    cudaGraphExec_t sets_exec = nullptr;      // the multi-set scatter/gap/count graph, replayed
+    int sets_exec_nw = 0, sets_exec_nodes = 0;
+    uint64_t sets_instantiations = 0;         // times that graph had to be instantiated
     // windowed count of 64-bit keys (kc_window.cuh): window-grouped keys,
     // per-bucket window ids and per-window counts and key ranges
     bool window_count = true;    // KC_WINDOW_COUNT=0 in the environment: count_routed only
@@ -526,6 +531,71 @@ void launch_count(kc_context* c, uint64_t n_keys, int use_filter) {
     kc::count_routed<NW><<<tiles, kc::CNT_THREADS, 0, c->stream>>>(a);
 }
 
+// Grow the tables of the given buckets x4 (again x4 for a bucket whose keys
+// still met a full probe window): per round one arena growth for all of them,
+// their new tables initialised and filled by two launches, one
+// synchronisation; c->h_meta is updated (not uploaded).
+template <int NW>
+int grow_buckets(kc_context* c, const std::vector<uint32_t>& buckets) {
+    std::vector<uint32_t> pending = buckets;
+    std::vector<uint64_t> new_slots(buckets.size());
+    std::vector<uint32_t> idx(buckets.size());
+    for (size_t i = 0; i < buckets.size(); ++i) {
+        new_slots[i] = (c->h_meta[buckets[i]].tab_mask + 1) * 4;
+        idx[i] = (uint32_t)i;
+    }
+    std::vector<uint32_t> todo = idx;
+    for (int round = 0; !todo.empty(); ++round) {
+        if (round > 12) return fail(KC_ERR_OVERFLOW, "a table kept overflowing while it was grown");
+        uint64_t total = 0, max_slots = 0;
+        for (uint32_t i : todo) {
+            total += new_slots[i];
+            max_slots = std::max<uint64_t>(max_slots, new_slots[i]);
+        }
+        CK(c->table.grow_keep((c->table_slots_used + total) * c->slot_bytes, c->table_slots_used * c->slot_bytes,
+                              c->stream));
+        std::vector<kc::GrowJob> jobs(todo.size());
+        for (size_t j = 0; j < todo.size(); ++j) {
+            const kc::BucketMeta& m = c->h_meta[buckets[todo[j]]];
+            jobs[j] = kc::GrowJob{m.tab_off, m.tab_mask + 1, c->table_slots_used, new_slots[todo[j]] - 1};
+            c->table_slots_used += new_slots[todo[j]];
+        }
+        CK(c->grow_jobs.ensure(jobs.size() * sizeof(kc::GrowJob)));
+        CK(c->grow_failed.ensure(jobs.size() * sizeof(uint32_t)));
+        CK(cudaMemcpyAsync(c->grow_jobs.p, jobs.data(), jobs.size() * sizeof(kc::GrowJob), cudaMemcpyHostToDevice,
+                           c->stream));
+        CKR(fill_dev(c, c->grow_failed.p, jobs.size() * sizeof(uint32_t), 0));
+        std::vector<uint32_t> failed(jobs.size());
+        for (size_t j0 = 0; j0 < jobs.size(); j0 += 65535) {  // grid y limit
+            const uint32_t nj = (uint32_t)std::min<size_t>(65535, jobs.size() - j0);
+            const dim3 grid((uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(256, ceil_div(max_slots, 4096))), nj);
+            Stage st(c, KC_STAGE_REHASH, 2);
+            kc::grow_init<NW><<<grid, 256, 0, c->stream>>>(c->table.p, c->grow_jobs.as<kc::GrowJob>() + j0);
+            kc::grow_move<NW><<<grid, 256, 0, c->stream>>>(c->table.p, c->grow_jobs.as<kc::GrowJob>() + j0,
+                                                           c->grow_failed.as<uint32_t>() + j0);
+            CK(cudaGetLastError());
+        }
+        CK(cudaMemcpyAsync(failed.data(), c->grow_failed.p, jobs.size() * sizeof(uint32_t), cudaMemcpyDeviceToHost,
+                           c->stream));
+        CKR(sync_stream(c));
+        std::vector<uint32_t> again;
+        for (size_t j = 0; j < todo.size(); ++j) {
+            const uint32_t i = todo[j];
+            if (failed[j]) {  // pathological clustering: grow again
+                new_slots[i] *= 4;
+                again.push_back(i);
+                continue;
+            }
+            kc::BucketMeta& m = c->h_meta[buckets[i]];
+            m.tab_off = jobs[j].new_off;
+            m.tab_mask = new_slots[i] - 1;
+            ++c->rehashes;
+        }
+        todo.swap(again);
+    }
+    return KC_OK;
+}
+
 // Grow the tables of overflowed buckets (x4) and re-insert the keys that
 // met a full table, until none is left.
 template <int NW>
@@ -540,36 +610,7 @@ int rehash_loop(kc_context* c, uint64_t n_keys) {
         if (grow.empty()) return KC_OK;
         if (round > 24) return fail(KC_ERR_OVERFLOW, "repeat tables kept overflowing after %d growth rounds", round);
         CKR(fill_dev(c, c->overflow.p, nb * sizeof(uint32_t), 0));
-        CK(c->scalars.ensure(64));
-        uint32_t* d_failed = c->scalars.as<uint32_t>() + 8;
-        for (uint32_t b : grow) {
-            uint64_t old_slots = c->h_meta[b].tab_mask + 1;
-            uint64_t new_slots = old_slots * 4;
-            for (;;) {
-                const uint64_t need = (c->table_slots_used + new_slots) * c->slot_bytes;
-                CK(c->table.grow_keep(need, c->table_slots_used * c->slot_bytes, c->stream));
-                const uint64_t off = c->table_slots_used;
-                void* nt = c->table.as<uint8_t>() + off * c->slot_bytes;
-                const void* ot = c->table.as<uint8_t>() + c->h_meta[b].tab_off * c->slot_bytes;
-                Stage st(c, KC_STAGE_REHASH, 2);
-                kc::init_slots<NW><<<256, 256, 0, c->stream>>>(nt, new_slots);
-                CKR(fill_dev(c, d_failed, sizeof(uint32_t), 0));
-                kc::rehash_bucket<NW><<<std::max<uint64_t>(1, std::min<uint64_t>(1184, ceil_div(old_slots, 256))), 256, 0,
-                                        c->stream>>>(ot, old_slots, nt, new_slots - 1, d_failed);
-                CK(cudaGetLastError());
-                uint32_t h_failed = 0;
-                CKR(get(c, &h_failed, d_failed, sizeof(uint32_t)));
-                CKR(sync_stream(c));
-                c->table_slots_used += new_slots;
-                if (!h_failed) {
-                    c->h_meta[b].tab_off = off;
-                    c->h_meta[b].tab_mask = new_slots - 1;
-                    break;
-                }
-                new_slots *= 4;  // pathological clustering: grow again
-            }
-            ++c->rehashes;
-        }
+        CKR(grow_buckets<NW>(c, grow));
         CKR(put(c, c->meta.p, c->h_meta.data(), nb * sizeof(kc::BucketMeta)));
         c->win_ready = false;  // grown buckets leave the windowed count (their filter and table part)
         launch_count<NW>(c, n_keys, 0);
@@ -1444,6 +1485,7 @@ void kc_destroy(kc_context* c) {
                       &c->meta,   &c->bloom,     &c->table,     &c->low_packed,   &c->roots,         &c->chunks,
                       &c->root_count, &c->chunk_pass, &c->chunk_off, &c->sort_tmp, &c->sort_hist, &c->sort_offs, &c->sort_sums,
                       &c->set_tiles, &c->tile_prefix, &c->set_info, &c->pass_bits, &c->loads, &c->routed2,
+                      &c->grow_jobs, &c->grow_failed,
                       &c->bucket_win, &c->win_info, &c->win_count, &c->win_padded, &c->win_start, &c->win_cursor,
                       &c->win_end};
     for (DevBuf* b : bufs) b->release();
@@ -1463,6 +1505,7 @@ void kc_destroy(kc_context* c) {
         if (c->ev_ring[i]) cudaEventDestroy(c->ev_ring[i]);
         if (c->ring[i]) cudaFreeHost(c->ring[i]);
     }
+    if (c->sets_exec) cudaGraphExecDestroy(c->sets_exec);
     if (c->ev_pack) cudaEventDestroy(c->ev_pack);
     if (c->ev_mbox) cudaEventDestroy(c->ev_mbox);
     if (c->mbox_h) cudaFreeHost(c->mbox_h);
@@ -1660,6 +1703,15 @@ int kc_route_device(kc_context* c, const uint8_t* d_fastq, uint64_t n, uint64_t*
     collect_stage_times(c);
     for (int r = 0; r < 256; ++r) counts[r] = r < (int)c->route_counts.size() ? c->route_counts[r] : 0;
     c->have_route = true;
+    return KC_OK;
+}
+
+int kc_routed_keys(kc_context* c, const void** d_keys, uint64_t* n_keys) {
+    if (!c || !d_keys || !n_keys) return fail(KC_ERR_INVALID, "null argument");
+    if (!c->have_route) return fail(KC_ERR_STATE, "no routed keys: call kc_route_device first");
+    CK(cudaStreamSynchronize(c->stream));
+    *d_keys = c->routed.p;
+    *n_keys = c->routed_keys;
     return KC_OK;
 }
 
@@ -2125,6 +2177,11 @@ int count_sets_impl(kc_context* c, const uint8_t* buf, const kc_set_desc* sets, 
     uint64_t pos = 0;
     c->h_meta.assign(nbk, kc::BucketMeta{});
     uint64_t bw = 0, ts = 0, K = 0;
+    // learned sizing (kc_set_predicted_set_loads) when predictions for these
+    // n_sets sets were handed over: 12 filter bits per predicted distinct key,
+    // predicted table keys with 15% headroom at the target load; else the
+    // sampled rule on the exact per-bucket k-mer totals
+    const bool learned = g.sizing == KC_SIZING_LEARNED && c->set_pred_table.size() == nbk;
     for (uint32_t s = 0; s < n_sets; ++s) {
         pos = ceil_div(pos, SEG) * SEG;
         set_key0[s] = pos;
@@ -2134,8 +2191,15 @@ int count_sets_impl(kc_context* c, const uint8_t* buf, const kc_set_desc* sets, 
             start[(uint64_t)s * NB + b] = pos;
             pos += kb;
             K += kb;
-            const uint64_t words = pow2_at_least(std::max<uint64_t>((uint64_t)(kb * g.bloom_bits / 64.0), 64));
-            const uint64_t slots = pow2_at_least(std::max<uint64_t>((uint64_t)(kb * g.repeat_ratio / g.table_load), 64));
+            uint64_t words, slots;
+            if (learned) {
+                const uint64_t q = (uint64_t)s * NB + b;
+                words = pow2_at_least(std::max<uint64_t>((uint64_t)(c->set_pred_distinct[q] * 12.0 / 64.0), 64));
+                slots = pow2_at_least(std::max<uint64_t>((uint64_t)(c->set_pred_table[q] * 1.15 / g.table_load), 64));
+            } else {
+                words = pow2_at_least(std::max<uint64_t>((uint64_t)(kb * g.bloom_bits / 64.0), 64));
+                slots = pow2_at_least(std::max<uint64_t>((uint64_t)(kb * g.repeat_ratio / g.table_load), 64));
+            }
             c->h_meta[(uint64_t)s * NB + b] = kc::BucketMeta{bw, words - 1, ts, slots - 1};
             bw += words;
             ts += slots;
@@ -2196,12 +2260,15 @@ int count_sets_impl(kc_context* c, const uint8_t* buf, const kc_set_desc* sets, 
     ca.use_filter = 1;
     const uint64_t cgrid = ceil_div(n_keys, (uint64_t)CT * kc::CNT_SEGS_PER_WARP);
 
-    // scatter -> gap fill -> count as one graph
+    // scatter -> gap fill -> count as one graph.  The context keeps the
+    // instantiated graph: a later call captures its own launches (the same
+    // three kernels, new arguments and grids) and updates the instantiated
+    // graph in place (cudaGraphExecUpdate), instantiating only when the update
+    // is refused; the replay is one launch of the whole sequence.
     {
         Stage st(c, KC_STAGE_COUNT_ROUTED, 3);
         a.routed = c->routed.p;
         cudaGraph_t graph = nullptr;
-        cudaGraphExec_t exec = nullptr;
         CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
         if (nt)
             kc::extract_kernel<NW, kc::SCATTER>
@@ -2210,11 +2277,28 @@ int count_sets_impl(kc_context* c, const uint8_t* buf, const kc_set_desc* sets, 
         if (cgrid) kc::count_routed<NW><<<cgrid, kc::CNT_THREADS, 0, c->stream>>>(ca);
         const cudaError_t ce = cudaStreamEndCapture(c->stream, &graph);
         if (ce != cudaSuccess) return fail(KC_ERR_DEVICE, "graph capture failed: %s", cudaGetErrorString(ce));
-        cudaError_t e = cudaGraphInstantiate(&exec, graph, 0);
-        if (e == cudaSuccess) e = cudaGraphLaunch(exec, c->stream);
-        if (exec) cudaGraphExecDestroy(exec);
+        cudaError_t e = cudaSuccess;
+        bool updated = false;
+        if (c->sets_exec && c->sets_exec_nw == NW && c->sets_exec_nodes == (nt ? 3 : 2) + (cgrid ? 0 : -1)) {
+            cudaGraphExecUpdateResultInfo info{};
+            updated = cudaGraphExecUpdate(c->sets_exec, graph, &info) == cudaSuccess;
+            if (!updated) cudaGetLastError();
+        }
+        if (!updated) {
+            if (c->sets_exec) cudaGraphExecDestroy(c->sets_exec);
+            c->sets_exec = nullptr;
+            e = cudaGraphInstantiate(&c->sets_exec, graph, 0);
+            c->sets_exec_nw = NW;
+            c->sets_exec_nodes = (nt ? 3 : 2) + (cgrid ? 0 : -1);
+            ++c->sets_instantiations;
+        }
+        if (e == cudaSuccess) e = cudaGraphLaunch(c->sets_exec, c->stream);
         cudaGraphDestroy(graph);
-        if (e != cudaSuccess) return fail(KC_ERR_DEVICE, "graph launch failed: %s", cudaGetErrorString(e));
+        if (e != cudaSuccess) {
+            if (c->sets_exec) cudaGraphExecDestroy(c->sets_exec);
+            c->sets_exec = nullptr;
+            return fail(KC_ERR_DEVICE, "graph launch failed: %s", cudaGetErrorString(e));
+        }
     }
 
     // overflowed tables: grow x4, move, retry only the failed keys
@@ -2227,35 +2311,10 @@ int count_sets_impl(kc_context* c, const uint8_t* buf, const kc_set_desc* sets, 
         if (!any) break;
         if (round > 24) return fail(KC_ERR_OVERFLOW, "repeat tables kept overflowing");
         CK(cudaMemsetAsync(c->overflow.p, 0, nbk * sizeof(uint32_t), c->stream));
-        uint32_t* d_failed = c->scalars.as<uint32_t>() + 8;
-        for (uint64_t b = 0; b < nbk; ++b) {
-            if (!ov[b]) continue;
-            const uint64_t old_slots = c->h_meta[b].tab_mask + 1;
-            uint64_t new_slots = old_slots * 4;
-            for (;;) {
-                CK(c->table.grow_keep((c->table_slots_used + new_slots) * c->slot_bytes, c->table_slots_used * c->slot_bytes,
-                                      c->stream));
-                uint8_t* nt_ = c->table.as<uint8_t>() + c->table_slots_used * c->slot_bytes;
-                const uint8_t* ot = c->table.as<uint8_t>() + c->h_meta[b].tab_off * c->slot_bytes;
-                Stage st(c, KC_STAGE_REHASH, 2);
-                kc::init_slots<NW><<<64, 256, 0, c->stream>>>(nt_, new_slots);
-                CK(cudaMemsetAsync(d_failed, 0, sizeof(uint32_t), c->stream));
-                kc::rehash_bucket<NW><<<std::max<uint64_t>(1, std::min<uint64_t>(1184, ceil_div(old_slots, 256))), 256, 0,
-                                        c->stream>>>(ot, old_slots, nt_, new_slots - 1, d_failed);
-                uint32_t h_failed = 0;
-                CK(cudaMemcpyAsync(&h_failed, d_failed, sizeof h_failed, cudaMemcpyDeviceToHost, c->stream));
-                CK(cudaStreamSynchronize(c->stream));
-                const uint64_t off = c->table_slots_used;
-                c->table_slots_used += new_slots;
-                if (!h_failed) {
-                    c->h_meta[b].tab_off = off;
-                    c->h_meta[b].tab_mask = new_slots - 1;
-                    break;
-                }
-                new_slots *= 4;
-            }
-            ++c->rehashes;
-        }
+        std::vector<uint32_t> grow;
+        for (uint64_t b = 0; b < nbk; ++b)
+            if (ov[b]) grow.push_back((uint32_t)b);
+        if ((rc = grow_buckets<NW>(c, grow))) return rc;
         CK(cudaMemcpyAsync(c->meta.p, c->h_meta.data(), nbk * sizeof(kc::BucketMeta), cudaMemcpyHostToDevice, c->stream));
         ca.table = c->table.p;
         ca.use_filter = 0;
@@ -2347,7 +2406,8 @@ extern "C" int kc_count_sets(kc_context* c, const uint8_t* d_fastq, const kc_set
     if (c->n_buckets != 256) return fail(KC_ERR_INVALID, "read-set batches use 256 buckets per set");
     for (uint32_t s = 0; s < n_sets; ++s) {
         const uint32_t k = sets[s].k;
-        if (k < 1 || k > 64 || (k <= 32) != (c->cfg.k <= 32))
+        const uint32_t nw = k <= 32 ? 1 : (k <= 64 ? 2 : 4);
+        if (k < 1 || k > 128 || nw != c->nw)
             return fail(KC_ERR_INVALID, "set %u: k=%u must be in the key width of the context's k (%u)", s, k, c->cfg.k);
         if (sets[s].offset % 16) return fail(KC_ERR_INVALID, "set %u: offset must be 16-byte aligned", s);
     }
@@ -2361,7 +2421,8 @@ extern "C" int kc_count_sets(kc_context* c, const uint8_t* d_fastq, const kc_set
     c->input_bytes = bytes;
     c->batches = 1;
     rc = c->nw == 1 ? count_sets_impl<1>(c, d_fastq, sets, n_sets, results)
-                    : count_sets_impl<2>(c, d_fastq, sets, n_sets, results);
+                    : (c->nw == 2 ? count_sets_impl<2>(c, d_fastq, sets, n_sets, results)
+                                  : count_sets_impl<4>(c, d_fastq, sets, n_sets, results));
     if (rc) return rc;
     CK(cudaEventRecord(c->ev1, c->stream));
     CK(cudaEventSynchronize(c->ev1));
@@ -2371,5 +2432,86 @@ extern "C" int kc_count_sets(kc_context* c, const uint8_t* d_fastq, const kc_set
     const double wall = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
     fill_stats(c, stats, ms, wall);
     if (stats) stats->low_records = c->low_total;
+    return KC_OK;
+}
+
+namespace {
+
+// Per set, k-mers per model bucket (the top 12 bits of the canonical key) of
+// bytes [offset, offset + bytes) of each set: the extraction's histogram pass
+// over per-set tiles.
+template <int NW>
+int set_prefix_kmers_impl(kc_context* c, const uint8_t* buf, const kc_set_desc* sets, uint32_t n_sets, uint64_t* counts) {
+    constexpr uint32_t NB = KC_MODEL_BUCKETS;
+    std::vector<kc::SetTile> tiles;
+    for (uint32_t s = 0; s < n_sets; ++s) {
+        const uint32_t first = (uint32_t)tiles.size();
+        for (uint64_t off = 0; off < sets[s].bytes; off += kc::EXT_TILE)
+            tiles.push_back(kc::SetTile{sets[s].offset + off, sets[s].offset + sets[s].bytes, s, sets[s].k, first, 0});
+    }
+    const uint64_t nt = tiles.size(), nbk = (uint64_t)n_sets * NB;
+    CK(c->set_tiles.ensure(std::max<uint64_t>(nt, 1) * sizeof(kc::SetTile)));
+    CK(c->tile_nl.ensure(std::max<uint64_t>(nt, 1) * sizeof(uint32_t)));
+    CK(c->tile_line.ensure(std::max<uint64_t>(nt, 1) * sizeof(uint64_t)));
+    CK(c->tile_prefix.ensure(std::max<uint64_t>(nt, 1) * sizeof(uint64_t)));
+    CK(c->scalars.ensure(64));
+    CK(c->bucket_count.ensure(nbk * sizeof(uint64_t)));
+    CK(cudaMemsetAsync(c->bucket_count.p, 0, nbk * sizeof(uint64_t), c->stream));
+    CK(cudaMemsetAsync(c->scalars.as<uint32_t>() + 12, 0, sizeof(uint32_t), c->stream));
+    if (nt) {
+        CK(cudaMemcpyAsync(c->set_tiles.p, tiles.data(), nt * sizeof(kc::SetTile), cudaMemcpyHostToDevice, c->stream));
+        const kc::SetTile* d_tiles = c->set_tiles.as<kc::SetTile>();
+        kc::lines_per_set_tile<<<nt, kc::EXT_THREADS, 0, c->stream>>>(buf, d_tiles, c->tile_nl.as<uint32_t>());
+        int rc;
+        if ((rc = device_scan<uint32_t, uint64_t>(c, c->tile_nl.as<uint32_t>(), nt, c->tile_prefix.as<uint64_t>(), 0,
+                                                  c->scalars.as<uint64_t>())))
+            return rc;
+        kc::rebase_set_lines<<<std::min<uint64_t>(ceil_div(nt, 256), 1184), 256, 0, c->stream>>>(
+            c->tile_prefix.as<uint64_t>(), d_tiles, nt, c->tile_line.as<uint64_t>());
+        kc::ExtractArgs a{};
+        a.tiles = d_tiles;
+        a.buf = buf;
+        a.tile_line = c->tile_line.as<uint64_t>();
+        a.bucket_shift = 64 - 12;
+        a.n_buckets = NB;
+        a.bucket_count = c->bucket_count.as<unsigned long long>();
+        a.error = c->scalars.as<uint32_t>() + 12;
+        kc::extract_kernel<NW, kc::HIST><<<nt, kc::EXT_THREADS, kc::extract_smem_bytes<NW, kc::HIST>(NB), c->stream>>>(a);
+        CK(cudaGetLastError());
+    }
+    CK(cudaMemcpyAsync(counts, c->bucket_count.p, nbk * sizeof(uint64_t), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    return KC_OK;
+}
+
+}  // namespace
+
+extern "C" int kc_set_prefix_kmers(kc_context* c, const uint8_t* d_fastq, const kc_set_desc* sets, uint32_t n_sets,
+                                   uint64_t* counts) {
+    if (!c || !sets || !counts || n_sets == 0 || !d_fastq) return fail(KC_ERR_INVALID, "null argument");
+    for (uint32_t s = 0; s < n_sets; ++s) {
+        const uint32_t k = sets[s].k;
+        const uint32_t nw = k <= 32 ? 1 : (k <= 64 ? 2 : 4);
+        if (k < 1 || k > 128 || nw != c->nw)
+            return fail(KC_ERR_INVALID, "set %u: k=%u must be in the key width of the context's k (%u)", s, k, c->cfg.k);
+        if (sets[s].offset % 16) return fail(KC_ERR_INVALID, "set %u: offset must be 16-byte aligned", s);
+    }
+    CK(cudaSetDevice(c->device));
+    return c->nw == 1 ? set_prefix_kmers_impl<1>(c, d_fastq, sets, n_sets, counts)
+                      : (c->nw == 2 ? set_prefix_kmers_impl<2>(c, d_fastq, sets, n_sets, counts)
+                                    : set_prefix_kmers_impl<4>(c, d_fastq, sets, n_sets, counts));
+}
+
+extern "C" int kc_set_predicted_set_loads(kc_context* c, uint32_t n_sets, const double* distinct,
+                                          const double* table_keys) {
+    if (!c) return fail(KC_ERR_INVALID, "null context");
+    if (!distinct || !table_keys || n_sets == 0) {
+        c->set_pred_distinct.clear();
+        c->set_pred_table.clear();
+        return KC_OK;
+    }
+    const uint64_t n = (uint64_t)n_sets * 256;
+    c->set_pred_distinct.assign(distinct, distinct + n);
+    c->set_pred_table.assign(table_keys, table_keys + n);
     return KC_OK;
 }

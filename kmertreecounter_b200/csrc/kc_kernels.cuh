@@ -11,9 +11,10 @@
 //                       on the routed array, bucket by bucket:     filter and
 //                       the working set of in-flight CTAs stays    tables stay
 //                       within one or two buckets, i.e. in L2      L2-resident)
-//   rehash_bucket,      after the host grew an overflowed bucket's table:
-//   count_routed        move its keys, then re-insert the keys that met the
-//     (table only)      full table
+//   grow_init,          after the host grew the overflowed buckets' tables
+//   grow_move,          (all of them in one arena growth): move their keys,
+//   count_routed        then re-insert the keys that met a full table
+//     (table only)      (rehash_bucket: the same for one bucket)
 //   pack_low            first occurrences -> packed low.bin bytes
 //   export_count,       table slots -> ExportRecord<N> grouped by root id
 //   export_write_bits   (per-chunk counts and a bitmap of passing slots, then
@@ -1419,6 +1420,72 @@ __global__ void rehash_bucket(const void* old_tab, uint64_t old_slots, void* new
     }
 }
 
+// One bucket's table growth: its old table (old_off, old_slots slots) moves
+// into a new table of new_mask + 1 slots at new_off (slot offsets in the
+// table arena).
+struct GrowJob {
+    uint64_t old_off, old_slots, new_off, new_mask;
+};
+
+template <int NW>
+__device__ __forceinline__ void init_slot(typename SlotOf<NW>::T& s) {
+    if constexpr (NW == 1) {
+        s.key = EMPTY;
+        s.count = 0;
+        s.pad = 0;
+    } else if constexpr (NW == 2) {
+        s.w0 = EMPTY;
+        s.w1 = EMPTY;
+        s.count = 0;
+        s.pad[0] = s.pad[1] = s.pad[2] = 0;
+    } else {
+        s.w0 = s.w1 = s.w2 = s.w3 = 0;
+        s.count = 0;
+        s.state = SLOT_EMPTY;
+        s.mark = 0;
+    }
+}
+
+// Many growths at once: blockIdx.y = job; the new tables are initialised by
+// grow_init, then grow_move moves every occupied old slot (failed[job] = 1
+// when a key met a full probe window of the new table).
+template <int NW>
+__global__ void grow_init(void* table, const GrowJob* __restrict__ jobs) {
+    using S = typename SlotOf<NW>::T;
+    const GrowJob j = jobs[blockIdx.y];
+    S* t = reinterpret_cast<S*>(table) + j.new_off;
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i <= j.new_mask;
+         i += (uint64_t)gridDim.x * blockDim.x) {
+        S s;
+        init_slot<NW>(s);
+        t[i] = s;
+    }
+}
+
+template <int NW>
+__global__ void grow_move(void* table, const GrowJob* __restrict__ jobs, uint32_t* __restrict__ failed) {
+    using S = typename SlotOf<NW>::T;
+    const GrowJob j = jobs[blockIdx.y];
+    const S* src = reinterpret_cast<const S*>(table) + j.old_off;
+    S* dst = reinterpret_cast<S*>(table) + j.new_off;
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < j.old_slots;
+         i += (uint64_t)gridDim.x * blockDim.x) {
+        const S s = src[i];
+        if constexpr (NW == 1) {
+            if (s.key == EMPTY) continue;
+            if (!table_add(dst, j.new_mask, hash_key(s.key), s.key, s.count)) failed[blockIdx.y] = 1u;
+        } else if constexpr (NW == 2) {
+            if (s.w0 == EMPTY && s.w1 == EMPTY) continue;
+            const Key2 k{s.w0, s.w1};
+            if (!table_add(dst, j.new_mask, hash_key(k), k, s.count)) failed[blockIdx.y] = 1u;
+        } else {
+            if (s.state != SLOT_READY) continue;
+            const Key4 k{s.w0, s.w1, s.w2, s.w3};
+            if (!table_add(dst, j.new_mask, hash_key(k), k, s.count)) failed[blockIdx.y] = 1u;
+        }
+    }
+}
+
 // Initialise table slots to EMPTY with count 0.
 template <int NW>
 __global__ void init_slots(void* tab, uint64_t n) {
@@ -2040,23 +2107,25 @@ __global__ void pack_low_sets(const void* routed, const uint32_t* seg_low, const
         uint8_t* dst0 = out + low_byte_base[lo] + (seg_low_prefix[sg] - first) * P;
         for (uint32_t i = lane; i < n; i += 32) {
             const K key = keys[sg * (uint64_t)SEG + i];
-            uint64_t w0, w1;
+            uint64_t w[4] = {0, 0, 0, 0};
             if constexpr (NW == 1) {
-                w0 = key;
-                w1 = 0;
+                w[0] = key;
+            } else if constexpr (NW == 2) {
+                w[0] = key.w0;
+                w[1] = key.w1;
             } else {
-                w0 = key.w0;
-                w1 = key.w1;
+                w[0] = key.w0;
+                w[1] = key.w1;
+                w[2] = key.w2;
+                w[3] = key.w3;
             }
+            // byte by byte: a set's low.bin bytes start at any byte offset
             uint8_t* d = dst0 + (uint64_t)i * P;
             uint32_t q = 0;
-            if (full) {
-                for (uint32_t b = 0; b < 8; ++b) d[q++] = (uint8_t)(w0 >> (8 * b));
-                if (full == 2)
-                    for (uint32_t b = 0; b < 8; ++b) d[q++] = (uint8_t)(w1 >> (8 * b));
-            }
+            for (uint32_t f = 0; f < full; ++f)
+                for (uint32_t b = 0; b < 8; ++b) d[q++] = (uint8_t)(w[f] >> (8 * b));
             if (tail_bytes) {
-                const uint64_t tw = (full ? w1 : w0) & tmask;
+                const uint64_t tw = (full < 4 ? w[full] : 0ull) & tmask;
                 for (uint32_t b = 8 - tail_bytes; b < 8; ++b) d[q++] = (uint8_t)(tw >> (8 * b));
             }
         }

@@ -153,25 +153,42 @@ def merge_outputs(rank_dirs, ranges, out_dir):
             shutil.copyfile(os.path.join(rank_dirs[r], f"root_{p}.bin"), os.path.join(out_dir, f"root_{p}.bin"))
 
 
-def gpu_stages(counter, slice_bytes, device):
+class _DeviceWords:
+    """A device buffer of int64 words seen by torch without a copy
+    (__cuda_array_interface__)."""
+
+    def __init__(self, ptr, n):
+        self.__cuda_array_interface__ = {"shape": (n,), "typestr": "<i8", "data": (ptr, False), "version": 3,
+                                         "strides": None}
+
+
+def routed_tensor(counter, nw, device):
+    """The context's routed keys as an int64 tensor on `device` (no copy;
+    valid until the next call on the counter)."""
+    import torch
+    ptr, n = counter.routed_keys()
+    if n == 0:
+        return torch.empty(0, dtype=torch.int64, device=device)
+    return torch.as_tensor(_DeviceWords(ptr, n * nw), device=device)
+
+
+def gpu_stages(counter, slice_bytes, device, d_slice=None):
     """route() and count() for exchange_and_count on this rank's GPU: the
-    slice (host uint8 array) goes to the device, kc_route_device routes it,
-    kc_copy_routed hands the keys to torch for the exchange, and
-    kc_count_keys_device counts the owned keys."""
+    slice (host uint8 array, or d_slice already on the device) is routed by
+    kc_route_device, the context's routed keys are the exchange's send buffer
+    as they are (kc_routed_keys, no copy), and kc_count_keys_device counts
+    the owned keys once the exchange has finished reading them."""
     import torch
     from ._native import KcError  # noqa: F401  (errors surface as KcError)
     nw = 1 if counter.cfg.k <= 32 else (2 if counter.cfg.k <= 64 else 4)
 
     def route():
-        d = torch.from_numpy(np.ascontiguousarray(slice_bytes)).to(device)
+        d = d_slice if d_slice is not None else torch.from_numpy(np.ascontiguousarray(slice_bytes)).to(device)
         counts = counter.route_device(d.data_ptr(), d.numel())
-        n = int(counts.sum())
-        keys = torch.empty(max(n * nw, 1), dtype=torch.int64, device=device)
-        counter.copy_routed(keys.data_ptr(), keys.numel() * 8)
-        torch.cuda.synchronize(device)
-        return keys[:n * nw], counts
+        return routed_tensor(counter, nw, device), counts
 
     def count(owned, own_counts):
+        torch.cuda.synchronize(device)  # the exchange has read the send buffer the count overwrites
         n = owned.numel() // nw
         return counter.count_keys_device(owned.data_ptr() if n else 0, n, own_counts)
 

@@ -64,6 +64,8 @@ _SIG = {
     "kc_mlp_train_step": (C.c_int, [C.c_void_p, _f, _f, C.c_int, C.c_float, _f]),
     "kc_mlp_last_error": (C.c_char_p, []),
     "kc_mlp_set_under_weight": (C.c_int, [C.c_void_p, C.c_float]),
+    "kc_set_prefix_kmers": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(_native.KcSetDesc), C.c_uint32, _u64]),
+    "kc_set_predicted_set_loads": (C.c_int, [C.c_void_p, C.c_uint32, _d, _d]),
 }
 for _n, (_r, _a) in _SIG.items():
     getattr(lib, _n).restype = _r
@@ -260,6 +262,44 @@ def predict_device(counter, model, dptr, n, k, read_len):
         counter.count_device(dptr, pn)
         return pn
     return predict_on(counter, model, k, read_len, n, run)
+
+
+def predict_sets(counter, model, dptr, sets, read_lens):
+    """Learned sizing of a batch of read sets (kc_count_sets): the first 1%
+    of every set is counted in one batched call (its k-mers, first
+    occurrences and table keys per set) and histogrammed per model bucket
+    (kc_set_prefix_kmers); the network runs on all sets at once and its
+    per-set, per-root-bucket loads go to the counter for its next
+    kc_count_sets of these sets (the counter must use KC_SIZING_LEARNED).
+    `sets` is a list of (offset, bytes, k), `read_lens` the sets' read
+    lengths.  Returns (distinct, table keys), each (n_sets, 256)."""
+    n = len(sets)
+    check(lib.kc_set_predicted_set_loads(counter._ctx, 0, None, None))
+    pre = [(o, prefix_len(b), k) for o, b, k in sets]
+    res = counter.count_sets(dptr, pre)
+    desc = (_native.KcSetDesc * n)(*[_native.KcSetDesc(o, b, k, 0) for o, b, k in pre])
+    km = np.zeros(n * MODEL_BUCKETS, np.uint64)
+    check(lib.kc_set_prefix_kmers(counter._ctx, C.c_void_p(dptr), desc, n, km.ctypes.data_as(_u64)))
+    km = km.reshape(n, MODEL_BUCKETS).astype(np.float64)
+    x = np.zeros((n, N_IN), np.float32)
+    for i, ((o, b, k), r) in enumerate(zip(sets, res)):
+        # the prefix's distinct keys are its first occurrences (a filter
+        # false positive moves a few into the table), its table keys its
+        # root records
+        kp = max(km[i].sum(), 1.0)
+        loads = (km[i] * (r.low_records / kp), km[i] * (r.root_records / kp), km[i])
+        x[i] = features(loads, k, read_lens[i], b, pre[i][1])
+    y = model.forward(x)
+    per = MODEL_BUCKETS // 256
+    dist = np.zeros((n, 256))
+    tab = np.zeros((n, 256))
+    for i, (o, b, k) in enumerate(sets):
+        d, t = decode(y[i], km[i] * (b / max(pre[i][1], 1)))
+        dist[i] = d.reshape(256, per).sum(axis=1)
+        tab[i] = (t * model.margin).reshape(256, per).sum(axis=1)
+    dd, tt = np.ascontiguousarray(dist.ravel()), np.ascontiguousarray(tab.ravel())
+    check(lib.kc_set_predicted_set_loads(counter._ctx, n, dd.ctypes.data_as(_d), tt.ctypes.data_as(_d)))
+    return dist, tab
 
 
 def apply(counter, pred):

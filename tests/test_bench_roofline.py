@@ -44,3 +44,19 @@ def test_pipeline_roofline_terms(bench):
 
 def test_pipeline_roofline_absent_without_peaks(bench):
     assert bench.pipeline_roofline(None, {"hbm_gbs": 1.0, "source": "x"}, 1, 1, 0, 0, 8, 16, 1.0, 1.0) == {}
+
+
+def test_stage_rooflines(bench):
+    """Per-stage algorithmic bytes: the windowed count (a subroute stage ran)
+    moves keys, first occurrences and table cells; without windows the count
+    is charged the workload definition's 64 B per k-mer + 64 B per repeat."""
+    stats = {"total_kmers": 2_000, "low_records": 600, "root_records": 100, "table_slots": 1_000}
+    ms = {"extract_scatter": 2.0, "subroute": 1.0, "count": 4.0, "pack_low": 0.5}
+    r = bench.stage_rooflines(ms, stats, 6_000, 31, 1.0, 8, 16)
+    assert r["extract_scatter"]["alg_bytes"] == 6_000 + 8 * 2_000
+    assert r["subroute"]["alg_bytes"] == 2 * 8 * 2_000
+    assert r["count"]["alg_bytes"] == 8 * 2_000 + 8 * 600 + int(2 * 16 * 1_000 * 9 / 8)
+    assert r["pack_low"]["alg_bytes"] == 8 * 600 + 8 * 600
+    assert r["count"]["gbs"] == pytest.approx(r["count"]["alg_bytes"] / 4e-3 / 1e9)
+    r2 = bench.stage_rooflines({"count": 4.0}, stats, 6_000, 63, 1.0, 16, 24)
+    assert r2["count"]["alg_bytes"] == 64 * 2_000 + 64 * 1_400 and r2["count"]["rule"].startswith("64 K")

@@ -46,7 +46,8 @@ def check_sets(c, res, sets, datas):
 
 
 @pytest.mark.parametrize("ks,cfg", [([21, 31] * 12, {}), ([31, 21, 25] * 5, {"repeat_ratio": 1e-6}),
-                                    ([33, 63, 47, 64] * 4, {"k": 63})])
+                                    ([33, 63, 47, 64] * 4, {"k": 63}), ([65, 100, 127, 128] * 3, {"k": 101}),
+                                    ([70, 99] * 3, {"k": 101, "repeat_ratio": 1e-6})])
 def test_sets_match_oracle(ks, cfg):
     buf, sets, datas = make_sets(ks, seed=len(ks))
     d = torch.from_numpy(buf).cuda()
@@ -72,3 +73,32 @@ def test_sets_equal_single_counts():
                           roots_all[r.root_offset:r.root_offset + r.root_records], k)
         b = parity.merged(low1, roots1, k)
         assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1])
+
+
+def test_sets_graph_is_replayed():
+    """The scatter/gap/count graph of kc_count_sets is instantiated once and
+    updated for later calls with other sets (same three kernels)."""
+    buf, sets, datas = make_sets([21, 31] * 4, seed=3)
+    d = torch.from_numpy(buf).cuda()
+    with kc.Counter(k=31) as c:
+        for part in (sets, sets[:5], sets[2:]):
+            res = c.count_sets(d.data_ptr(), part)
+            check_sets(c, res, part, [datas[sets.index(x)] for x in part])
+
+
+def test_sets_learned_sizing_is_exact():
+    """Batched learned sizing (sizing.predict_sets: a batched count of every
+    set's first 1%, one network pass, per-set per-bucket loads) sizes the
+    tables of kc_count_sets; the counts stay the oracle's."""
+    import os
+    from kmertreecounter_b200 import sizing
+    if not os.path.exists(sizing.MODEL_PATH):
+        pytest.skip("no trained sizing model")
+    buf, sets, datas = make_sets([21, 31] * 8, seed=5)
+    d = torch.from_numpy(buf).cuda()
+    model = sizing.MLP.load(max_batch=64)
+    with kc.Counter(k=31, sizing=kc.KC_SIZING_LEARNED) as c:
+        dist, tab = sizing.predict_sets(c, model, d.data_ptr(), sets, [150] * len(sets))
+        assert dist.shape == (len(sets), 256) and np.all(tab >= 0)
+        res = c.count_sets(d.data_ptr(), sets)
+        check_sets(c, res, sets, datas)

@@ -133,3 +133,25 @@ def test_shard_command_line_one_rank(tmp_path):
     wk, wc, K = oracle.count(data, 31)
     assert np.array_equal(mk, wk) and np.array_equal(mc, wc.astype(np.uint64))
     assert '"total_kmers": %d' % K in p.stdout
+
+
+def test_sharded_bench_one_rank():
+    """bench.py's several-GPU form (route the slice, one NCCL all-to-all of
+    keys sent from the context's own buffer, count the owned prefixes) under
+    torch.distributed.run with one rank: its line reports the input's exact
+    k-mer total and strong scaling."""
+    import json
+    import os
+    import subprocess
+    import sys
+    from conftest import ROOT
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", "--nproc-per-node", "1", "--master-addr",
+           "127.0.0.1", "--master-port", "29533", os.path.join(ROOT, "bench.py"), "--gpus", "1", "--shard",
+           "--scale", "0.01", "--steps", "2", "--warmup", "1", "--e2e-steps", "1"]
+    p = subprocess.run(cmd, capture_output=True, text=True, timeout=600, cwd=ROOT)
+    assert p.returncode == 0, p.stderr[-2000:]
+    line = json.loads(p.stdout.strip().splitlines()[-1])
+    assert line["scaling"] == "strong" and line["config"]["parallelism"].startswith("sharded x1")
+    data = synth.fastq(synth.genome_scale(scale=0.01))
+    assert line["stats"]["total_kmers"] == oracle.total_kmers(data, 31)
+    assert line["gpu_launches"] > 0 and line["e2e"]["h2d_bytes_per_step"] == data.size
