@@ -62,15 +62,19 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-peaks", action="store_true", help="skip the atomic/link microbenchmark")
     ap.add_argument("--sample-scale", type=float, default=0.1, help="CPU sample size, fraction of the workload")
-    ap.add_argument("--batch-scale", type=float, default=0.05,
+    ap.add_argument("--batch-scale", type=float, default=1.0,
                     help="read-set batch comparison: shrink genomes and read counts of the 512 sets")
     ap.add_argument("--no-batched", action="store_true")
     ap.add_argument("--no-sizing", action="store_true", help="skip the learned-vs-sampled sizing comparison")
     ap.add_argument("--no-large-long", action="store_true",
                     help="skip the long-key record (200 Mbp, 50x, k=63, 4096 buckets) of the default run")
     ap.add_argument("--ll-steps", type=int, default=3, help="timed steps of the long-key record")
+    ap.add_argument("--ll-pass-gib", type=float, default=None,
+                    help="device pass size of the long-key record in GiB (default: the workload's)")
     ap.add_argument("--no-file-to-file", action="store_true",
                     help="skip the command-line leg (bin/Tree vs the reference's Tree on the same file)")
+    ap.add_argument("--no-reference-full", action="store_true",
+                    help="in the command-line leg, skip the reference's Tree on the full-size file (about a minute)")
     ap.add_argument("--shard", action="store_true",
                     help="time the sharded count (root-prefix owners, one NCCL all-to-all) even on one GPU; "
                          "it is the default for more than one GPU")
@@ -272,7 +276,8 @@ PROFILED_TRAFFIC = {
     # workload: {stage: {"sources_sha256": ..., "bytes_per_step": ...}}
     "genome_scale": {},
 }
-KERNEL_SOURCES = ("kmertreecounter_b200/csrc/kc_kernels.cuh", "kmertreecounter_b200/csrc/kc_engine.cu")
+KERNEL_SOURCES = ("kmertreecounter_b200/csrc/kc_kernels.cuh", "kmertreecounter_b200/csrc/kc_window.cuh",
+                  "kmertreecounter_b200/csrc/kc_engine.cu")
 
 
 def kernel_sources_sha256():
@@ -401,22 +406,28 @@ def compare_batched(args, kc, torch):
     plain: one kc_count_device call per set (per-set launches and host syncs);
     batched: kc_count_sets over autotuned groups of sets, one launch per stage
     per group.  Both wall-clock on the host around device-synchronous calls."""
+    from concurrent.futures import ThreadPoolExecutor
     from kmertreecounter_b200 import autotune, synth
     specs = synth.batched_sets(n_sets=512, seed=3, scale=args.batch_scale)
-    datas = [synth.fastq(p) for p, _ in specs]
     ks = [k for _, k in specs]
+    sizes = [synth.fastq_bytes(p) for p, _ in specs]
     offs, pos = [], 0
-    for d in datas:
+    for nb in sizes:
         offs.append(pos)
-        pos += (d.size + 15) // 16 * 16
+        pos += (nb + 15) // 16 * 16
     buf = np.full(pos, ord("\n"), np.uint8)
-    for o, d in zip(offs, datas):
-        buf[o:o + d.size] = d
+    with ThreadPoolExecutor(max_workers=min(32, os.cpu_count() or 1)) as ex:  # the generator releases the GIL
+        list(ex.map(lambda i: synth.fastq(specs[i][0], out=buf.ctypes.data + offs[i]), range(len(specs))))
     bases = int(sum(int(p.n_reads) * int(p.read_len_min) for p, _ in specs))
     dev = torch.from_numpy(buf).cuda()
     torch.cuda.synchronize()
-    sets = [(o, d.size, k) for o, d, k in zip(offs, datas, ks)]
+    del buf
+    sets = [(o, nb, k) for o, nb, k in zip(offs, sizes, ks)]
     base = dev.data_ptr()
+    # a pass's keys, segments, filters and tables take up to about 8 bytes
+    # per FASTQ byte: passes hold what fits 40% of the memory left
+    free, _ = torch.cuda.mem_get_info()
+    max_bytes = int(free * 0.4 / 8)
     # plain: one context per k, one call per set
     ctx = {k: kc.Counter(k=k) for k in sorted(set(ks))}
     for o, nb, k in sets[:8]:
@@ -430,19 +441,21 @@ def compare_batched(args, kc, torch):
     for c in ctx.values():
         c.close()
     # batched: autotuned knobs and sets per pass
-    best = autotune.tune(base, sets, 31, use_cache=False)
+    best = autotune.tune(base, sets, 31, use_cache=False, max_bytes=max_bytes)
     knobs = {k: v for k, v in best.items() if k in ("table_load", "repeat_ratio", "bloom_bits")}
     per_pass = best["sets_per_pass"]
+    groups = autotune.passes(sets, per_pass, max_bytes)
     with kc.Counter(k=31, **knobs) as c:
-        autotune.count_in_passes(c, base, sets, per_pass)
+        autotune.count_in_passes(c, base, sets, per_pass, max_bytes=max_bytes)
         torch.cuda.synchronize()
         t = time.perf_counter()
         grown = []
-        _, res = autotune.count_in_passes(c, base, sets, per_pass, grown)
+        _, res = autotune.count_in_passes(c, base, sets, per_pass, grown, max_bytes=max_bytes)
         torch.cuda.synchronize()
         batched_ms = (time.perf_counter() - t) * 1e3
-        sums_batched = set_checksums(c, base, sets, per_pass, torch)
-    out = {"sets": len(sets), "bases": bases, "fastq_bytes": int(buf.size), "scale": args.batch_scale,
+        sums_batched = set_checksums(c, base, sets, groups, torch)
+    out = {"sets": len(sets), "bases": bases, "fastq_bytes": int(pos), "scale": args.batch_scale,
+           "passes": len(groups), "max_pass_fastq_bytes": max_bytes,
            "plain": {"ms": plain_ms, "gbases_s": bases / plain_ms / 1e6},
            "batched": {"ms": batched_ms, "gbases_s": bases / batched_ms / 1e6,
                        "rehashes": sum(grown), "tuned": {k: v for k, v in best.items() if k != "trials"}},
@@ -456,12 +469,12 @@ def compare_batched(args, kc, torch):
 
         def learned_passes(c, split):
             st_all = []
-            for i in range(0, len(sets), per_pass):
+            for i, j in groups:
                 t0 = time.perf_counter()
-                sizing.predict_sets(c, model, base, sets[i:i + per_pass], read_lens[i:i + per_pass])
+                sizing.predict_sets(c, model, base, sets[i:j], read_lens[i:j])
                 torch.cuda.synchronize()
                 t1 = time.perf_counter()
-                st_all += c.count_sets(base, sets[i:i + per_pass])
+                st_all += c.count_sets(base, sets[i:j])
                 torch.cuda.synchronize()
                 split[0] += (t1 - t0) * 1e3
                 split[1] += (time.perf_counter() - t1) * 1e3
@@ -476,7 +489,7 @@ def compare_batched(args, kc, torch):
             res_l = learned_passes(c, split)
             torch.cuda.synchronize()
             learned_ms = (time.perf_counter() - t) * 1e3
-            sums_learned = set_checksums(c, base, sets, per_pass, torch, learned=(model, read_lens))
+            sums_learned = set_checksums(c, base, sets, groups, torch, learned=(model, read_lens))
         out["batched_learned"] = {"ms": learned_ms, "gbases_s": bases / learned_ms / 1e6,
                                   "speedup_vs_plain": plain_ms / learned_ms,
                                   "speedup_vs_batched": batched_ms / learned_ms,
@@ -487,24 +500,25 @@ def compare_batched(args, kc, torch):
     return out
 
 
-def set_checksums(c, base, sets, per_pass, torch, learned=None):
+def set_checksums(c, base, sets, groups, torch, learned=None):
     """Per set, a checksum of the exact (k-mer, count) multiset that does not
     depend on how the first-occurrence filter split it between low.bin and
     the root files: sum over low.bin keys of h(key) + sum over root records of
     h(key) x count (mod 2^64), h = a 64-bit mixer, computed on the device."""
     from kmertreecounter_b200 import sizing
     sums = []
-    for i in range(0, len(sets), per_pass):
-        part = sets[i:i + per_pass]
+    for i, j in groups:
+        part = sets[i:j]
         if learned:
-            sizing.predict_sets(c, learned[0], base, part, learned[1][i:i + per_pass])
+            sizing.predict_sets(c, learned[0], base, part, learned[1][i:j])
         res = c.count_sets(base, part)
         d_low, low_bytes, d_roots, n_roots = c.device_results()
-        low = torch.empty(max(low_bytes, 8), dtype=torch.uint8, device="cuda")
-        roots = torch.empty(max(n_roots * 16, 16), dtype=torch.uint8, device="cuda")
-        c.copy_low_into(low.data_ptr(), low_bytes)
-        c.copy_roots_into(roots.data_ptr(), n_roots * 16)
-        rr = roots[:n_roots * 16].view(torch.int64).view(-1, 2)
+        # the context's own buffers, seen by torch without a copy
+        low = torch.as_tensor(_DeviceBytes(d_low, low_bytes), device="cuda") if low_bytes else \
+            torch.empty(0, dtype=torch.uint8, device="cuda")
+        roots = torch.as_tensor(_DeviceBytes(d_roots, n_roots * 16), device="cuda") if n_roots else \
+            torch.empty(0, dtype=torch.uint8, device="cuda")
+        rr = roots.view(torch.int64).view(-1, 2)
         for (o, b, k), r in zip(part, res):
             P = kc_packed(k)
             lk = low[r.low_offset:r.low_offset + r.low_records * P].view(-1, P)
@@ -514,6 +528,14 @@ def set_checksums(c, base, sets, per_pass, torch, learned=None):
             rec = rr[r.root_offset:r.root_offset + r.root_records]
             sums.append(int((_mix(w).sum() + (_mix(rec[:, 0]) * (rec[:, 1] & 0xFFFFFFFF)).sum()).item()) % (1 << 64))
     return sums
+
+
+class _DeviceBytes:
+    """n bytes of device memory at ptr, for torch.as_tensor without a copy."""
+
+    def __init__(self, ptr, n):
+        self.__cuda_array_interface__ = {"shape": (n,), "typestr": "|u1", "data": (ptr, False), "version": 3,
+                                         "strides": None}
 
 
 def kc_packed(k):
@@ -550,12 +572,19 @@ def compare_sizing(args, kc, torch, dev, n, k, buckets, device_batch=None, steps
         elif args.workload in DEVICE_BATCH:
             cfg.device_batch_bytes = DEVICE_BATCH[args.workload]
         with kc.Counter(cfg) as c:
+            split = []
+
             def step():
+                t0 = time.perf_counter()
                 if rule == "learned":
                     sizing.predict_device(c, model, dev.data_ptr(), n, k, 150)
-                return c.count_device(dev.data_ptr(), n)
+                t1 = time.perf_counter()
+                st_ = c.count_device(dev.data_ptr(), n)
+                split.append(((t1 - t0) * 1e3, st_.device_ms))
+                return st_
             step()
             times = []
+            split.clear()
             for _ in range(max(steps or args.steps, 1)):
                 torch.cuda.synchronize()
                 t = time.perf_counter()
@@ -563,7 +592,9 @@ def compare_sizing(args, kc, torch, dev, n, k, buckets, device_batch=None, steps
                 times.append((time.perf_counter() - t) * 1e3)
             hist[rule] = c.histogram(1, 1000)
             out[rule] = dict(ms_per_step=statistics.median(times), rehashes=st.rehashes, table_slots=st.table_slots,
-                             filter_words=st.filter_words, table_keys=st.table_keys)
+                             filter_words=st.filter_words, table_keys=st.table_keys,
+                             predict_ms=statistics.median(x[0] for x in split),
+                             count_device_ms=statistics.median(x[1] for x in split))
     out["identical_counts"] = bool(np.array_equal(hist["sampled"][0], hist["learned"][0])
                                    and hist["sampled"][1] == hist["learned"][1])
     out["margin"] = model.margin
@@ -588,7 +619,8 @@ def large_long_record(args, kc, torch, dev_peaks, pk):
     del data
     torch.cuda.synchronize()
     k, buckets = 63, 4096
-    cfg = kc.default_config(k=k, n_buckets=buckets, device_batch_bytes=DEVICE_BATCH["large_long"])
+    pass_bytes = int(args.ll_pass_gib * (1 << 30)) if args.ll_pass_gib else DEVICE_BATCH["large_long"]
+    cfg = kc.default_config(k=k, n_buckets=buckets, device_batch_bytes=pass_bytes)
     steps = max(1, args.ll_steps)
     stage_ms = {}
     with kc.Counter(cfg) as c:
@@ -613,7 +645,7 @@ def large_long_record(args, kc, torch, dev_peaks, pk):
     roof = pipeline_roofline(dev_peaks, pk, n, K, L, stats["root_records"], kc.packed_bytes(k), kc.record_bytes(k),
                              ms_step, count_ms)
     out = {"config": {"workload": DESCRIBE["large_long"], "k": k, "n_buckets": buckets, "fastq_bytes": n,
-                      "bases": bases, "reads": int(p.n_reads), "device_pass_bytes": DEVICE_BATCH["large_long"]},
+                      "bases": bases, "reads": int(p.n_reads), "device_pass_bytes": pass_bytes},
            "value": bases / (ms_step / 1e3) / 1e9, "unit": "Gbases/s", "ms_per_step": ms_step, "steps": steps,
            "distinct_kmers": distinct, "distinct_kmers_per_s": distinct / (ms_step / 1e3), "stats": stats,
            "stages_ms_per_step": {s_: v / steps for s_, v in stage_ms.items()},
@@ -621,19 +653,20 @@ def large_long_record(args, kc, torch, dev_peaks, pk):
                                               pk["hbm_gbs"], kc.packed_bytes(k), kc.record_bytes(k)),
            "pipeline_roofline": roof.get("pipeline")}
     if not args.no_sizing:
-        out["sizing"] = compare_sizing(args, kc, torch, dev, n, k, buckets, DEVICE_BATCH["large_long"], steps)
+        out["sizing"] = compare_sizing(args, kc, torch, dev, n, k, buckets, pass_bytes, steps)
     del dev
     torch.cuda.empty_cache()
     return out
 
 
-def file_to_file(args, sample_path, sample_bases, k, ref_sample_gbs, full_path, full_bases):
+def file_to_file(args, sample_path, sample_bases, k, ref_sample_gbs, full_path, full_bases, full_kmers=None):
     """This build's drop-in command line (`bin/Tree <fastq> <k> <n_thread>
     <mem_gb>`) timed like the reference's `Tree`: wall clock of the whole
     process, from reading the FASTQ file to low.bin and root_0..255.bin
     written under ./tmp/, device set-up included.  On the reference's own
     sample file (beside the reference's time on it) and on the full workload's
-    file."""
+    file, where the reference's `Tree` is also run once (all host threads;
+    accepted only when the k-mer total it prints equals `full_kmers`)."""
     tree = os.path.join(ROOT, "kmertreecounter_b200", "bin", "Tree")
     threads = str(max(6, host_facts()["cores"] or 6))
 
@@ -656,6 +689,23 @@ def file_to_file(args, sample_path, sample_bases, k, ref_sample_gbs, full_path, 
                      "ratio": ours["gbases_s"] / ref_sample_gbs if "gbases_s" in ours and ref_sample_gbs else None}
     if full_path:
         out["full"] = {"ours": run(full_path, full_bases, 2)}
+        if ref_sample_gbs and not args.no_reference_full:
+            sys.path.insert(0, os.path.join(ROOT, "oracle"))
+            import oracle
+            cores = host_facts()["cores"] or 1
+            mem = max(4, int(os.sysconf("SC_PAGE_SIZE") * os.sysconf("SC_PHYS_PAGES") / 2**30 * 0.7))
+            with tempfile.TemporaryDirectory(dir=os.path.dirname(full_path)) as wd:
+                t = time.perf_counter()
+                stdout, rc = oracle.run_reference(full_path, k, wd, threads=max(6, cores), mem_gb=mem)
+                dt = time.perf_counter() - t
+            got = oracle.reference_total(stdout) if rc == 0 else None
+            ref = {"seconds": dt, "gbases_s": full_bases / dt / 1e9, "threads": max(6, cores), "runs": 1,
+                   "kmers_reported": got, "kmers_expected": full_kmers}
+            if rc != 0 or (full_kmers is not None and got != full_kmers):
+                ref["rejected"] = f"exit {rc}, k-mer total {got} (expected {full_kmers})"
+            out["full"]["reference"] = ref
+            if "gbases_s" in out["full"]["ours"] and "rejected" not in ref:
+                out["full"]["ratio"] = out["full"]["ours"]["gbases_s"] / ref["gbases_s"]
     return out
 
 
@@ -857,7 +907,7 @@ def run_ours(args):
                                     "host": host_facts()}
             if not args.no_file_to_file:
                 line["file_to_file"] = file_to_file(args, path, sbases, kk, best if kind == "reference" else None,
-                                                    full_path, bases)
+                                                    full_path, bases, stats["total_kmers"])
     if ftf_dir is not None:
         ftf_dir.cleanup()
     if world > 1:

@@ -43,11 +43,15 @@ int kc_set_predicted_loads(kc_context* ctx, const double* distinct, const double
 int kc_set_prefix_kmers(kc_context* ctx, const uint8_t* d_fastq, const kc_set_desc* sets, uint32_t n_sets,
                         uint64_t* counts);
 
-/* Predicted distinct keys and table keys per (set, root bucket) -- n_sets x
- * 256 entries each, set-major -- for the NEXT kc_count_sets of n_sets sets on
- * this context with cfg.sizing = KC_SIZING_LEARNED (NULL clears).  A table a
- * prediction left too small grows exactly as under the sampled rule. */
-int kc_set_predicted_set_loads(kc_context* ctx, uint32_t n_sets, const double* distinct, const double* table_keys);
+/* Predicted distinct keys and table keys PER K-MER of each (set, root
+ * bucket) -- n_sets x 256 entries each, set-major -- for the NEXT
+ * kc_count_sets of n_sets sets on this context with cfg.sizing =
+ * KC_SIZING_LEARNED (NULL clears).  kc_count_sets multiplies them by the
+ * bucket's exact k-mer total (from its extraction histogram); a negative
+ * entry keeps the sampled rule for that bucket.  A table a prediction left
+ * too small grows exactly as under the sampled rule. */
+int kc_set_predicted_set_rates(kc_context* ctx, uint32_t n_sets, const double* distinct_per_kmer,
+                               const double* table_keys_per_kmer);
 
 /* ---- the MLP ---------------------------------------------------------- */
 typedef struct kc_mlp kc_mlp;

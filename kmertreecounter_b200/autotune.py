@@ -45,13 +45,28 @@ def signature(sets):
     return hashlib.sha1(key.encode()).hexdigest()[:16]
 
 
-def count_in_passes(counter, dptr, sets, per_pass, rehashes=None):
-    """kc_count_sets over `sets` in groups of `per_pass`; device ms total.
-    `rehashes`, a list, receives each pass's table growth steps."""
+def passes(sets, per_pass, max_bytes=None):
+    """Consecutive groups [i, j) of at most `per_pass` sets and (but for a
+    single set) at most `max_bytes` FASTQ bytes."""
+    out, i = [], 0
+    while i < len(sets):
+        j, nb = i, 0
+        while j < len(sets) and j - i < per_pass and (j == i or max_bytes is None or nb + sets[j][1] <= max_bytes):
+            nb += sets[j][1]
+            j += 1
+        out.append((i, j))
+        i = j
+    return out
+
+
+def count_in_passes(counter, dptr, sets, per_pass, rehashes=None, max_bytes=None):
+    """kc_count_sets over `sets` in groups of `per_pass` (and `max_bytes`);
+    device ms total.  `rehashes`, a list, receives each pass's table growth
+    steps."""
     ms = 0.0
     results = []
-    for i in range(0, len(sets), per_pass):
-        group = sets[i:i + per_pass]
+    for i, j in passes(sets, per_pass, max_bytes):
+        group = sets[i:j]
         base = group[0][0]
         res = counter.count_sets(dptr + base, [(o - base, b, k) for o, b, k in group])
         ms += counter.stats.device_ms
@@ -61,10 +76,11 @@ def count_in_passes(counter, dptr, sets, per_pass, rehashes=None):
     return ms, results
 
 
-def tune(dptr, sets, k, sample=64, repeats=2, use_cache=True):
+def tune(dptr, sets, k, sample=64, repeats=2, use_cache=True, max_bytes=None):
     """Best knob setting for these sets: dict of kc_config fields plus
-    `sets_per_pass`."""
-    sig = f"{_gpu_name()}|{signature(sets)}|{k}"
+    `sets_per_pass` (knobs timed on a sample of the sets, the sets per pass
+    on all of them; passes hold at most `max_bytes` FASTQ bytes)."""
+    sig = f"{_gpu_name()}|{signature(sets)}|{k}|{max_bytes}"
     cache = {}
     if use_cache and os.path.exists(CACHE):
         try:
@@ -81,16 +97,21 @@ def tune(dptr, sets, k, sample=64, repeats=2, use_cache=True):
     trials = []
     for knobs in GRID:
         with Counter(k=k, **knobs) as c:
-            count_in_passes(c, dptr, sub, len(sub))  # warm-up: sizes every buffer
-            t = min(count_in_passes(c, dptr, sub, len(sub))[0] for _ in range(repeats))
+            count_in_passes(c, dptr, sub, len(sub), max_bytes=max_bytes)  # warm-up: sizes every buffer
+            t = min(count_in_passes(c, dptr, sub, len(sub), max_bytes=max_bytes)[0] for _ in range(repeats))
         trials.append(dict(knobs, ms=t))
         if t < best_ms:
             best, best_ms = dict(knobs), t
     per_best, per_ms = SETS_PER_PASS[-1], float("inf")
     with Counter(k=k, **best) as c:
+        seen = set()
         for per in SETS_PER_PASS:
-            count_in_passes(c, dptr, sub, per)
-            t = min(count_in_passes(c, dptr, sub, per)[0] for _ in range(repeats))
+            layout = tuple(passes(sets, per, max_bytes))
+            if layout in seen:  # the byte limit made it the same passes
+                continue
+            seen.add(layout)
+            count_in_passes(c, dptr, sets, per, max_bytes=max_bytes)
+            t = min(count_in_passes(c, dptr, sets, per, max_bytes=max_bytes)[0] for _ in range(repeats))
             trials.append(dict(best, sets_per_pass=per, ms=t))
             if t < per_ms:
                 per_best, per_ms = per, t

@@ -193,7 +193,7 @@ struct kc_context {
     bool have_route = false;
     DevBuf sort_tmp, sort_hist, sort_offs, sort_sums;
     DevBuf set_tiles, tile_prefix, set_info;  // multi-set batches
-    std::vector<double> set_pred_distinct, set_pred_table;  // learned sizing per (set, root bucket)
+    std::vector<double> set_pred_distinct, set_pred_table;  // learned rates per (set, root bucket)
     cudaGraphExec_t sets_exec = nullptr;      // the multi-set scatter/gap/count graph, replayed
     int sets_exec_nw = 0, sets_exec_nodes = 0;
     uint64_t sets_instantiations = 0;         // times that graph had to be instantiated
@@ -201,10 +201,11 @@ struct kc_context {
     // per-bucket window ids and per-window counts and key ranges
     bool window_count = true;    // KC_WINDOW_COUNT=0 in the environment: count_routed only
     bool win_ready = false;      // windows built for the current table layout
-    uint64_t n_wins = 0;
+    uint64_t n_wins = 0, n_wins_phase0 = 0;
     std::vector<kc::BucketWin> h_bucket_win;
     std::vector<kc::WinInfo> h_win_info;
-    DevBuf routed2, bucket_win, win_info, win_count, win_padded, win_start, win_cursor, win_end;
+    std::vector<uint32_t> h_win_order;  // windows in launch order: phase 0, then phase 1
+    DevBuf routed2, bucket_win, win_info, win_order, win_count, win_padded, win_start, win_cursor, win_end;
     uint64_t window_spill = 0;   // keys counted from the spill area (all batches of the run)
 
     // host mirrors
@@ -635,6 +636,17 @@ bool build_windows(kc_context* c) {
         for (uint32_t q = 0; q < n; ++q) c->h_win_info.push_back(kc::WinInfo{b, q});
     }
     c->n_wins = c->h_win_info.size();
+    // launch order: the first phase's windows (one-window buckets and even
+    // windows), then the second's (odd windows)
+    c->h_win_order.clear();
+    for (int ph = 0; ph < 2; ++ph) {
+        for (uint32_t r = 0; r < (uint32_t)c->n_wins; ++r) {
+            const kc::WinInfo& wi = c->h_win_info[r];
+            const bool single = c->h_bucket_win[wi.bucket].zshift >= kc::WIN_SINGLE;
+            if ((single ? 0u : (wi.sub & 1u)) == (uint32_t)ph) c->h_win_order.push_back(r);
+        }
+        if (ph == 0) c->n_wins_phase0 = c->h_win_order.size();
+    }
     return true;
 }
 
@@ -677,6 +689,9 @@ int window_count(kc_context* c, uint64_t& n_keys) {
     if (!c->win_ready) {
         CK(c->bucket_win.ensure(c->n_buckets * sizeof(kc::BucketWin)));
         CK(c->win_info.ensure(nw * sizeof(kc::WinInfo)));
+        CK(c->win_order.ensure(nw * sizeof(uint32_t)));
+        CK(cudaMemcpyAsync(c->win_order.p, c->h_win_order.data(), nw * sizeof(uint32_t), cudaMemcpyHostToDevice,
+                           c->stream));
         CK(cudaMemcpyAsync(c->bucket_win.p, c->h_bucket_win.data(), c->n_buckets * sizeof(kc::BucketWin),
                            cudaMemcpyHostToDevice, c->stream));
         CK(cudaMemcpyAsync(c->win_info.p, c->h_win_info.data(), nw * sizeof(kc::WinInfo), cudaMemcpyHostToDevice,
@@ -767,6 +782,7 @@ int window_count(kc_context* c, uint64_t& n_keys) {
     a.win_fill = c->win_cursor.as<unsigned long long>();
     a.win_cap = c->win_padded.as<uint32_t>();
     a.wins = c->win_info.as<kc::WinInfo>();
+    a.order = c->win_order.as<uint32_t>();
     a.bw = bwin;
     a.meta = meta;
     a.table = c->table.as<kc::Slot1>();
@@ -777,7 +793,9 @@ int window_count(kc_context* c, uint64_t& n_keys) {
         Stage st(c, KC_STAGE_COUNT_ROUTED, 2);
         for (uint32_t ph = 0; ph < 2; ++ph) {
             a.phase = ph;
-            kc::count_window<<<nw, kc::WIN_THREADS, kc::window_smem_bytes(), c->stream>>>(a);
+            a.order_base = ph ? (uint32_t)c->n_wins_phase0 : 0u;
+            const uint64_t grid = ph ? nw - c->n_wins_phase0 : c->n_wins_phase0;
+            if (grid) kc::count_window<<<grid, kc::WIN_THREADS, kc::window_smem_bytes(), c->stream>>>(a);
         }
         CK(cudaGetLastError());
     }
@@ -1486,7 +1504,7 @@ void kc_destroy(kc_context* c) {
                       &c->root_count, &c->chunk_pass, &c->chunk_off, &c->sort_tmp, &c->sort_hist, &c->sort_offs, &c->sort_sums,
                       &c->set_tiles, &c->tile_prefix, &c->set_info, &c->pass_bits, &c->loads, &c->routed2,
                       &c->grow_jobs, &c->grow_failed,
-                      &c->bucket_win, &c->win_info, &c->win_count, &c->win_padded, &c->win_start, &c->win_cursor,
+                      &c->bucket_win, &c->win_info, &c->win_order, &c->win_count, &c->win_padded, &c->win_start, &c->win_cursor,
                       &c->win_end};
     for (DevBuf* b : bufs) b->release();
     for (cudaEvent_t e : c->ev_pool) cudaEventDestroy(e);
@@ -2177,10 +2195,11 @@ int count_sets_impl(kc_context* c, const uint8_t* buf, const kc_set_desc* sets, 
     uint64_t pos = 0;
     c->h_meta.assign(nbk, kc::BucketMeta{});
     uint64_t bw = 0, ts = 0, K = 0;
-    // learned sizing (kc_set_predicted_set_loads) when predictions for these
-    // n_sets sets were handed over: 12 filter bits per predicted distinct key,
-    // predicted table keys with 15% headroom at the target load; else the
-    // sampled rule on the exact per-bucket k-mer totals
+    // learned sizing (kc_set_predicted_set_rates) when predictions for these
+    // n_sets sets were handed over: predicted rates x the bucket's exact
+    // k-mer total, 12 filter bits per distinct key, table keys with 15%
+    // headroom at the target load; else (and for a negative rate) the sampled
+    // rule on the exact per-bucket k-mer totals
     const bool learned = g.sizing == KC_SIZING_LEARNED && c->set_pred_table.size() == nbk;
     for (uint32_t s = 0; s < n_sets; ++s) {
         pos = ceil_div(pos, SEG) * SEG;
@@ -2192,10 +2211,12 @@ int count_sets_impl(kc_context* c, const uint8_t* buf, const kc_set_desc* sets, 
             pos += kb;
             K += kb;
             uint64_t words, slots;
-            if (learned) {
-                const uint64_t q = (uint64_t)s * NB + b;
-                words = pow2_at_least(std::max<uint64_t>((uint64_t)(c->set_pred_distinct[q] * 12.0 / 64.0), 64));
-                slots = pow2_at_least(std::max<uint64_t>((uint64_t)(c->set_pred_table[q] * 1.15 / g.table_load), 64));
+            const uint64_t q = (uint64_t)s * NB + b;
+            if (learned && c->set_pred_distinct[q] >= 0.0 && c->set_pred_table[q] >= 0.0) {
+                const double d = std::min(c->set_pred_distinct[q], 1.0) * (double)kb;
+                const double t = std::min(c->set_pred_table[q], 1.0) * (double)kb;
+                words = pow2_at_least(std::max<uint64_t>((uint64_t)(d * 12.0 / 64.0), 64));
+                slots = pow2_at_least(std::max<uint64_t>((uint64_t)(t * 1.15 / g.table_load), 64));
             } else {
                 words = pow2_at_least(std::max<uint64_t>((uint64_t)(kb * g.bloom_bits / 64.0), 64));
                 slots = pow2_at_least(std::max<uint64_t>((uint64_t)(kb * g.repeat_ratio / g.table_load), 64));
@@ -2502,7 +2523,7 @@ extern "C" int kc_set_prefix_kmers(kc_context* c, const uint8_t* d_fastq, const 
                                     : set_prefix_kmers_impl<4>(c, d_fastq, sets, n_sets, counts));
 }
 
-extern "C" int kc_set_predicted_set_loads(kc_context* c, uint32_t n_sets, const double* distinct,
+extern "C" int kc_set_predicted_set_rates(kc_context* c, uint32_t n_sets, const double* distinct,
                                           const double* table_keys) {
     if (!c) return fail(KC_ERR_INVALID, "null context");
     if (!distinct || !table_keys || n_sets == 0) {

@@ -69,12 +69,23 @@ struct WinInfo {
     uint32_t sub;
 };
 
-__device__ __forceinline__ uint32_t window_of(uint64_t key, uint32_t bucket_shift, const BucketMeta* __restrict__ meta,
-                                              const BucketWin* __restrict__ bw, uint32_t* bucket_out) {
+// Window of a key, with the chunk's first bucket's entries held in registers
+// (a chunk's keys lie in that bucket but for a few at its edges).
+struct WinCache {
+    uint32_t bucket;
+    BucketWin w;
+    uint64_t mask;
+};
+__device__ __forceinline__ uint32_t window_of(uint64_t key, uint32_t bucket_shift, const WinCache& c,
+                                              const BucketMeta* __restrict__ meta, const BucketWin* __restrict__ bw) {
     const uint32_t b = (uint32_t)(key >> bucket_shift);
-    const BucketWin w = bw[b];
-    const uint64_t cell = (hash_key(key) >> 17) & __ldg(&meta[b].tab_mask);
-    *bucket_out = b;
+    BucketWin w = c.w;
+    uint64_t m = c.mask;
+    if (b != c.bucket) {
+        w = bw[b];
+        m = __ldg(&meta[b].tab_mask);
+    }
+    const uint64_t cell = (hash_key(key) >> 17) & m;
     return w.range_base + (w.zshift >= WIN_SINGLE ? 0u : (uint32_t)(cell >> w.zshift));
 }
 
@@ -115,12 +126,12 @@ __global__ void __launch_bounds__(SUB_THREADS) subroute_count(const uint64_t* __
     __syncthreads();
     const uint32_t bmin = chunk_min_bucket(k, bucket_shift, &s_min);
     if (bmin == 0xFFFFFFFFu) return;  // block-uniform: no key in this chunk
-    const uint32_t r0 = bw[bmin].range_base;
+    const WinCache wc{bmin, bw[bmin], __ldg(&meta[bmin].tab_mask)};
+    const uint32_t r0 = wc.w.range_base;
 #pragma unroll
     for (int j = 0; j < SUB_ITEMS; ++j) {
         if (k[j] == EMPTY) continue;
-        uint32_t b;
-        const uint32_t r = window_of(k[j], bucket_shift, meta, bw, &b);
+        const uint32_t r = window_of(k[j], bucket_shift, wc, meta, bw);
         if (r - r0 < (uint32_t)SUB_BINS) atomicAdd(&hist[r - r0], 1u);
         else atomicAdd(&win_count[r], 1u);
     }
@@ -215,7 +226,12 @@ __global__ void __launch_bounds__(SCAT_THREADS, 2) subroute_scatter(ScatterArgs 
     __syncthreads();
     const uint32_t bmin = misc[0];
     if (bmin == 0xFFFFFFFFu) return;  // block-uniform: no key in this chunk
-    const uint32_t r0 = a.bw[bmin].range_base;
+    // the first bucket's entries in shared memory (registers are short here)
+    __shared__ WinCache s_wc;
+    if (threadIdx.x == 0) s_wc = WinCache{bmin, a.bw[bmin], a.meta[bmin].tab_mask};
+    __syncthreads();
+    const WinCache& wc = s_wc;
+    const uint32_t r0 = wc.w.range_base;
     // per key: staged bin (high 16 bits) and place inside it (low 16), or
     // FAR for a window outside the staged span (placed one by one later)
     constexpr uint32_t FAR = 0xFFFFFFFFu;
@@ -224,8 +240,7 @@ __global__ void __launch_bounds__(SCAT_THREADS, 2) subroute_scatter(ScatterArgs 
     for (int j = 0; j < SCAT_ITEMS; ++j) {
         slot[j] = FAR;
         if (k[j] == EMPTY) continue;
-        uint32_t b;
-        const uint32_t l = window_of(k[j], a.bucket_shift, a.meta, a.bw, &b) - r0;
+        const uint32_t l = window_of(k[j], a.bucket_shift, wc, a.meta, a.bw) - r0;
         if (l < (uint32_t)SCAT_BINS) slot[j] = (l << 16) | atomicAdd(&hist[l], 1u);
     }
     __syncthreads();
@@ -283,8 +298,7 @@ __global__ void __launch_bounds__(SCAT_THREADS, 2) subroute_scatter(ScatterArgs 
             stage[pos] = k[j];
             stage_bin[pos] = (uint16_t)l;
         } else {  // far window: one key at a time
-            uint32_t b;
-            const uint32_t w = window_of(k[j], a.bucket_shift, a.meta, a.bw, &b);
+            const uint32_t w = window_of(k[j], a.bucket_shift, wc, a.meta, a.bw);
             const unsigned long long g = atomicAdd(&a.win_cursor[w], 1ull);
             if (g < a.win_end[w]) {
                 a.out[g] = k[j];
@@ -315,6 +329,8 @@ struct WindowArgs {
     const unsigned long long* win_fill;  // place after the last key the scatter put there
     const uint32_t* win_cap;         // capacity (multiple of WIN_SEG) of each window
     const WinInfo* wins;
+    const uint32_t* order;           // windows in launch order (phase 0's, then phase 1's)
+    uint32_t order_base;             // this launch's first entry of `order`
     const BucketWin* bw;
     const BucketMeta* meta;
     Slot1* table;                    // filter words in the cells' pad fields
@@ -336,18 +352,18 @@ __device__ __forceinline__ void cp_async4(void* smem, const void* gmem) {
 }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 
-// One CTA per window of the current phase.
+// One CTA per window of the current phase (the launch's list of windows).
 __global__ void __launch_bounds__(WIN_THREADS, 3) count_window(WindowArgs a) {
     extern __shared__ __align__(16) uint8_t win_smem[];
     unsigned long long* s_key = reinterpret_cast<unsigned long long*>(win_smem);
     uint32_t* s_cnt = reinterpret_cast<uint32_t*>(win_smem + (size_t)WIN_CELLS * 8);
     uint32_t* s_pad = s_cnt + WIN_CELLS;
 
-    const uint32_t r = blockIdx.x;
+    const uint32_t r = a.order[a.order_base + blockIdx.x];
     const WinInfo wi = a.wins[r];
     const BucketWin bw = a.bw[wi.bucket];
     const bool single = bw.zshift >= WIN_SINGLE;
-    if ((single ? 0u : (wi.sub & 1u)) != a.phase) return;
+    if ((single ? 0u : (wi.sub & 1u)) != a.phase) return;  // never: the launch lists this phase's windows
     const uint64_t k0 = a.win_start[r];
     const uint32_t capk = a.win_cap[r];
     const uint32_t cnt = (uint32_t)min((unsigned long long)capk, a.win_fill[r] - k0);
@@ -364,6 +380,22 @@ __global__ void __launch_bounds__(WIN_THREADS, 3) count_window(WindowArgs a) {
     const uint64_t base = single ? 0 : ((uint64_t)wi.sub << bw.zshift);
     const uint32_t W = single ? (uint32_t)(M + 1) : (uint32_t)WIN_CELLS;
 
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    constexpr int ITEMS = 2 * WIN_GROUP;  // keys per lane: 2 per segment
+    constexpr uint32_t GSTEP = (WIN_THREADS / 32) * WIN_GROUP;
+    // a warp's keys of segment group g (EMPTY past the window's keys); the
+    // loads of the next group are issued before the current one is counted,
+    // the first group's before the window's cells are staged
+    auto load_group = [&](uint32_t g, uint64_t (&dst)[ITEMS]) {
+#pragma unroll
+        for (int j = 0; j < ITEMS; ++j) {
+            const uint32_t idx = (g + j / 2) * WIN_SEG + (j & 1) * 32 + lane;
+            dst[j] = (g < nseg && idx < cnt) ? __ldcs(a.keys + k0 + idx) : EMPTY;
+        }
+    };
+    uint64_t nxt[ITEMS];
+    load_group((uint32_t)warp * WIN_GROUP, nxt);
+
     // stage the window (wrapping at the table's end: the last window's
     // halo) with asynchronous copies straight into the shared-memory arrays,
     // every cell's copies in flight at once
@@ -376,19 +408,18 @@ __global__ void __launch_bounds__(WIN_THREADS, 3) count_window(WindowArgs a) {
     cp_async_wait_all();
     __syncthreads();
 
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const uint32_t lt = (1u << lane) - 1u;
     const uint32_t limit = (uint32_t)min((uint64_t)PROBE_LIMIT, M + 1);
-    constexpr int ITEMS = 2 * WIN_GROUP;  // keys per lane: 2 per segment
-    for (uint32_t g = (uint32_t)warp * WIN_GROUP; g < nseg; g += (WIN_THREADS / 32) * WIN_GROUP) {
+    for (uint32_t g = (uint32_t)warp * WIN_GROUP; g < nseg; g += GSTEP) {
         uint64_t it[ITEMS];
         uint32_t mult[ITEMS];
 #pragma unroll
         for (int j = 0; j < ITEMS; ++j) {
             const uint32_t idx = (g + j / 2) * WIN_SEG + (j & 1) * 32 + lane;
             mult[j] = idx < cnt ? 1u : 0u;
-            it[j] = mult[j] ? __ldcs(a.keys + k0 + idx) : EMPTY;
+            it[j] = nxt[j];
         }
+        load_group(g + GSTEP, nxt);  // other segments: never written below
         __syncwarp();  // every read of these segments precedes the in-place writes
         // hot keys arrive in runs: merge equal neighbours' keys first, so the
         // shared-memory atomics of a run are one per distinct key

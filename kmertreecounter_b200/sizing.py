@@ -65,7 +65,7 @@ _SIG = {
     "kc_mlp_last_error": (C.c_char_p, []),
     "kc_mlp_set_under_weight": (C.c_int, [C.c_void_p, C.c_float]),
     "kc_set_prefix_kmers": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(_native.KcSetDesc), C.c_uint32, _u64]),
-    "kc_set_predicted_set_loads": (C.c_int, [C.c_void_p, C.c_uint32, _d, _d]),
+    "kc_set_predicted_set_rates": (C.c_int, [C.c_void_p, C.c_uint32, _d, _d]),
 }
 for _n, (_r, _a) in _SIG.items():
     getattr(lib, _n).restype = _r
@@ -190,18 +190,30 @@ def prefix_bytes(data, fraction=PREFIX_FRACTION):
 def features(prefix_loads, k, read_len, fastq_bytes, prefix_nbytes):
     """Model input from the prefix's per-bucket loads (distinct, table, kmers)."""
     d, t, km = (np.asarray(a, np.float64) for a in prefix_loads)
-    Kp, Dp, Tp = km.sum(), d.sum(), t.sum()
-    x = np.zeros(N_IN, np.float32)
-    if Kp > 0:
-        x[:MODEL_BUCKETS] = np.log1p(MODEL_BUCKETS * km / Kp) / 4.0
-    x[MODEL_BUCKETS + 0] = k / 64.0
-    x[MODEL_BUCKETS + 1] = read_len / 300.0
-    x[MODEL_BUCKETS + 2] = math.log(max(fastq_bytes, 1)) / IN_SCALE
-    x[MODEL_BUCKETS + 3] = math.log1p(Kp) / IN_SCALE
-    x[MODEL_BUCKETS + 4] = Dp / Kp if Kp > 0 else 1.0
-    x[MODEL_BUCKETS + 5] = Tp / Kp if Kp > 0 else 0.0
-    x[MODEL_BUCKETS + 6] = math.sqrt(Tp / Kp) if Kp > 0 else 0.0
-    x[MODEL_BUCKETS + 7] = math.log(max(fastq_bytes, 1) / max(prefix_nbytes, 1)) / 10.0
+    return features_batch(km[None, :], [d.sum()], [t.sum()], [k], [read_len], [fastq_bytes], [prefix_nbytes])[0]
+
+
+def features_batch(km, Dp, Tp, k, read_len, fastq_bytes, prefix_nbytes):
+    """features() for many inputs at once: km (n, MODEL_BUCKETS) prefix
+    k-mers per model bucket; the others per input (prefix distinct and table
+    keys, k, read length, file bytes, prefix bytes)."""
+    km = np.asarray(km, np.float64)
+    n = km.shape[0]
+    Dp, Tp, k, rl, fb, pb = (np.asarray(a, np.float64).reshape(n) for a in (Dp, Tp, k, read_len, fastq_bytes,
+                                                                         prefix_nbytes))
+    Kp = km.sum(axis=1)
+    has = Kp > 0
+    Ks = np.where(has, Kp, 1.0)
+    x = np.zeros((n, N_IN), np.float32)
+    x[:, :MODEL_BUCKETS] = np.where(has[:, None], np.log1p(MODEL_BUCKETS * km / Ks[:, None]) / 4.0, 0.0)
+    x[:, MODEL_BUCKETS + 0] = k / 64.0
+    x[:, MODEL_BUCKETS + 1] = rl / 300.0
+    x[:, MODEL_BUCKETS + 2] = np.log(np.maximum(fb, 1)) / IN_SCALE
+    x[:, MODEL_BUCKETS + 3] = np.log1p(Kp) / IN_SCALE
+    x[:, MODEL_BUCKETS + 4] = np.where(has, Dp / Ks, 1.0)
+    x[:, MODEL_BUCKETS + 5] = np.where(has, Tp / Ks, 0.0)
+    x[:, MODEL_BUCKETS + 6] = np.where(has, np.sqrt(np.maximum(Tp / Ks, 0.0)), 0.0)
+    x[:, MODEL_BUCKETS + 7] = np.log(np.maximum(fb, 1) / np.maximum(pb, 1)) / 10.0
     return x
 
 
@@ -264,41 +276,52 @@ def predict_device(counter, model, dptr, n, k, read_len):
     return predict_on(counter, model, k, read_len, n, run)
 
 
-def predict_sets(counter, model, dptr, sets, read_lens):
+MIN_SET_PREFIX = 128 << 10  # smallest prefix (bytes) a set's learned sizing is made from
+
+
+def predict_sets(counter, model, dptr, sets, read_lens, min_prefix_bytes=MIN_SET_PREFIX):
     """Learned sizing of a batch of read sets (kc_count_sets): the first 1%
     of every set is counted in one batched call (its k-mers, first
     occurrences and table keys per set) and histogrammed per model bucket
     (kc_set_prefix_kmers); the network runs on all sets at once and its
-    per-set, per-root-bucket loads go to the counter for its next
-    kc_count_sets of these sets (the counter must use KC_SIZING_LEARNED).
-    `sets` is a list of (offset, bytes, k), `read_lens` the sets' read
-    lengths.  Returns (distinct, table keys), each (n_sets, 256)."""
+    per-set, per-root-bucket rates (distinct and table keys per k-mer, the
+    table's with the model's margin) go to the counter for its next
+    kc_count_sets of these sets (the counter must use KC_SIZING_LEARNED),
+    which multiplies them by each bucket's exact k-mer total.  A set whose
+    1% is under `min_prefix_bytes` keeps the sampled rule (rate -1): a few
+    hundred reads say too little.  `sets` is a list of (offset, bytes, k),
+    `read_lens` the sets' read lengths.  Returns the rates (distinct, table
+    keys), each (n_sets, 256)."""
     n = len(sets)
-    check(lib.kc_set_predicted_set_loads(counter._ctx, 0, None, None))
-    pre = [(o, prefix_len(b), k) for o, b, k in sets]
-    res = counter.count_sets(dptr, pre)
-    desc = (_native.KcSetDesc * n)(*[_native.KcSetDesc(o, b, k, 0) for o, b, k in pre])
-    km = np.zeros(n * MODEL_BUCKETS, np.uint64)
-    check(lib.kc_set_prefix_kmers(counter._ctx, C.c_void_p(dptr), desc, n, km.ctypes.data_as(_u64)))
-    km = km.reshape(n, MODEL_BUCKETS).astype(np.float64)
-    x = np.zeros((n, N_IN), np.float32)
-    for i, ((o, b, k), r) in enumerate(zip(sets, res)):
+    check(lib.kc_set_predicted_set_rates(counter._ctx, 0, None, None))
+    dist = np.full((n, 256), -1.0)
+    tab = np.full((n, 256), -1.0)
+    use = [i for i, (_, b, _) in enumerate(sets) if prefix_len(b) >= min_prefix_bytes]
+    if use:
+        m = len(use)
+        pre = [(sets[i][0], prefix_len(sets[i][1]), sets[i][2]) for i in use]
+        res = counter.count_sets(dptr, pre)
+        desc = (_native.KcSetDesc * m)(*[_native.KcSetDesc(o, b, k, 0) for o, b, k in pre])
+        km = np.zeros(m * MODEL_BUCKETS, np.uint64)
+        check(lib.kc_set_prefix_kmers(counter._ctx, C.c_void_p(dptr), desc, m, km.ctypes.data_as(_u64)))
+        km = km.reshape(m, MODEL_BUCKETS).astype(np.float64)
         # the prefix's distinct keys are its first occurrences (a filter
         # false positive moves a few into the table), its table keys its
         # root records
-        kp = max(km[i].sum(), 1.0)
-        loads = (km[i] * (r.low_records / kp), km[i] * (r.root_records / kp), km[i])
-        x[i] = features(loads, k, read_lens[i], b, pre[i][1])
-    y = model.forward(x)
-    per = MODEL_BUCKETS // 256
-    dist = np.zeros((n, 256))
-    tab = np.zeros((n, 256))
-    for i, (o, b, k) in enumerate(sets):
-        d, t = decode(y[i], km[i] * (b / max(pre[i][1], 1)))
-        dist[i] = d.reshape(256, per).sum(axis=1)
-        tab[i] = (t * model.margin).reshape(256, per).sum(axis=1)
+        x = features_batch(km, [r.low_records for r in res], [r.root_records for r in res], [p[2] for p in pre],
+                           [read_lens[i] for i in use], [sets[i][1] for i in use], [p[1] for p in pre])
+        y = np.asarray(model.forward(x), np.float64)
+        rd = _from_y(y[:, :MODEL_BUCKETS])
+        rt = _from_y(y[:, MODEL_BUCKETS:]) * model.margin
+        # a root bucket's rate: its model buckets' rates weighted by their
+        # prefix k-mers (plain mean where the prefix has none)
+        per = MODEL_BUCKETS // 256
+        w = (km + 1e-3).reshape(m, 256, per)
+        ws = w.sum(axis=2)
+        dist[use] = (rd.reshape(m, 256, per) * w).sum(axis=2) / ws
+        tab[use] = (rt.reshape(m, 256, per) * w).sum(axis=2) / ws
     dd, tt = np.ascontiguousarray(dist.ravel()), np.ascontiguousarray(tab.ravel())
-    check(lib.kc_set_predicted_set_loads(counter._ctx, n, dd.ctypes.data_as(_d), tt.ctypes.data_as(_d)))
+    check(lib.kc_set_predicted_set_rates(counter._ctx, n, dd.ctypes.data_as(_d), tt.ctypes.data_as(_d)))
     return dist, tab
 
 

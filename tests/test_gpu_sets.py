@@ -86,10 +86,12 @@ def test_sets_graph_is_replayed():
             check_sets(c, res, part, [datas[sets.index(x)] for x in part])
 
 
-def test_sets_learned_sizing_is_exact():
+@pytest.mark.parametrize("min_prefix", [0, 1 << 40])
+def test_sets_learned_sizing_is_exact(min_prefix):
     """Batched learned sizing (sizing.predict_sets: a batched count of every
-    set's first 1%, one network pass, per-set per-bucket loads) sizes the
-    tables of kc_count_sets; the counts stay the oracle's."""
+    set's first 1%, one network pass, per-set per-bucket rates) sizes the
+    tables of kc_count_sets -- every set (min_prefix 0) or none (all keep the
+    sampled rule); the counts stay the oracle's."""
     import os
     from kmertreecounter_b200 import sizing
     if not os.path.exists(sizing.MODEL_PATH):
@@ -98,7 +100,11 @@ def test_sets_learned_sizing_is_exact():
     d = torch.from_numpy(buf).cuda()
     model = sizing.MLP.load(max_batch=64)
     with kc.Counter(k=31, sizing=kc.KC_SIZING_LEARNED) as c:
-        dist, tab = sizing.predict_sets(c, model, d.data_ptr(), sets, [150] * len(sets))
-        assert dist.shape == (len(sets), 256) and np.all(tab >= 0)
+        dist, tab = sizing.predict_sets(c, model, d.data_ptr(), sets, [150] * len(sets), min_prefix_bytes=min_prefix)
+        assert dist.shape == (len(sets), 256)
+        if min_prefix == 0:
+            assert np.all((tab >= 0) & (tab <= model.margin)) and np.all((dist >= 0) & (dist <= 1))
+        else:
+            assert np.all(tab == -1) and np.all(dist == -1)
         res = c.count_sets(d.data_ptr(), sets)
         check_sets(c, res, sets, datas)
