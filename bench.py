@@ -44,10 +44,11 @@ WORKLOADS = {
     "plain_small": ("plain_small", 31, 256),
     "large_long": ("large_long", 63, 4096),
 }
-# device passes per workload (the 21 GB, k=63 input keeps ~53 GB of packed
-# first occurrences and ~50 GB of tables on the device; 2 GiB passes keep the
-# routed keys at ~9 GB)
-DEVICE_BATCH = {"large_long": 2 << 30}
+# device passes per workload (the 21 GB, k=63 input keeps ~44 GB of packed
+# first occurrences and ~48 GB of tables on the device; 4 GiB passes keep the
+# routed keys at ~18 GB: 383 ms per step against 401 ms in 2 GiB passes,
+# 6 and 8 GiB passes run out of device memory)
+DEVICE_BATCH = {"large_long": 4 << 30}
 
 
 def parse():
@@ -61,7 +62,7 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-peaks", action="store_true", help="skip the atomic/link microbenchmark")
-    ap.add_argument("--sample-scale", type=float, default=0.1, help="CPU sample size, fraction of the workload")
+    ap.add_argument("--sample-scale", type=float, default=0.5, help="CPU sample size, fraction of the workload")
     ap.add_argument("--batch-scale", type=float, default=1.0,
                     help="read-set batch comparison: shrink genomes and read counts of the 512 sets")
     ap.add_argument("--no-batched", action="store_true")
@@ -449,16 +450,22 @@ def compare_batched(args, kc, torch):
         autotune.count_in_passes(c, base, sets, per_pass, max_bytes=max_bytes)
         torch.cuda.synchronize()
         t = time.perf_counter()
-        grown = []
-        _, res = autotune.count_in_passes(c, base, sets, per_pass, grown, max_bytes=max_bytes)
+        grown, slots = [], []
+        _, res = autotune.count_in_passes(c, base, sets, per_pass, grown, max_bytes=max_bytes, table_slots=slots)
         torch.cuda.synchronize()
         batched_ms = (time.perf_counter() - t) * 1e3
+        stages = {}
+        c.set_profiling(True)  # one more run, with stage events, for the breakdown
+        autotune.count_in_passes(c, base, sets, per_pass, max_bytes=max_bytes, stages=stages)
+        c.set_profiling(False)
         sums_batched = set_checksums(c, base, sets, groups, torch)
     out = {"sets": len(sets), "bases": bases, "fastq_bytes": int(pos), "scale": args.batch_scale,
            "passes": len(groups), "max_pass_fastq_bytes": max_bytes,
            "plain": {"ms": plain_ms, "gbases_s": bases / plain_ms / 1e6},
            "batched": {"ms": batched_ms, "gbases_s": bases / batched_ms / 1e6,
-                       "rehashes": sum(grown), "tuned": {k: v for k, v in best.items() if k != "trials"}},
+                       "rehashes": sum(grown), "table_slots_largest_pass": max(slots, default=0),
+                       "tuned": {k: v for k, v in best.items() if k != "trials"},
+                       "stages_ms": {s_: round(v, 3) for s_, v in stages.items() if v}},
            "speedup": plain_ms / batched_ms, "kmers": int(sum(r.total_kmers for r in res))}
     # batched + learned sizing: every pass first predicts its sets' loads (a
     # batched count of their first 1% and one network pass), then counts
@@ -479,12 +486,13 @@ def compare_batched(args, kc, torch):
                 split[0] += (t1 - t0) * 1e3
                 split[1] += (time.perf_counter() - t1) * 1e3
                 split[2] += int(c.stats.rehashes)
+                split[3] = max(split[3], int(c.stats.table_slots))
             return st_all
 
         with kc.Counter(k=31, sizing=kc.KC_SIZING_LEARNED, **knobs) as c:
-            learned_passes(c, [0.0, 0.0, 0])
+            learned_passes(c, [0.0, 0.0, 0, 0])
             torch.cuda.synchronize()
-            split = [0.0, 0.0, 0]
+            split = [0.0, 0.0, 0, 0]
             t = time.perf_counter()
             res_l = learned_passes(c, split)
             torch.cuda.synchronize()
@@ -494,6 +502,7 @@ def compare_batched(args, kc, torch):
                                   "speedup_vs_plain": plain_ms / learned_ms,
                                   "speedup_vs_batched": batched_ms / learned_ms,
                                   "predict_ms": split[0], "count_ms": split[1], "rehashes": split[2],
+                                  "table_slots_largest_pass": split[3],
                                   "identical_counts": sums_learned == sums_batched,
                                   "kmers": int(sum(r.total_kmers for r in res_l))}
     del dev
@@ -553,9 +562,11 @@ def _mix(x):
 def compare_sizing(args, kc, torch, dev, n, k, buckets, device_batch=None, steps=None):
     """Learned vs sampled sizing on the same resident FASTQ, each timed end to
     end per step by wall clock on its own context (every count call returns
-    synchronised).  A learned step counts the first 1% of the reads (plain
-    rule), runs the sizing MLP on the library's kernels and counts the whole
-    input with the predicted sizes; a sampled step only counts.  Rehashes and
+    synchronised).  A learned step counts the whole input with predicted
+    sizes; the prediction (the first 1% of the reads counted with the plain
+    rule on a helper context, the sizing MLP on the library's kernels) is
+    made inside the step, at its sizing point, beside its k-mer extraction; a
+    sampled step only counts.  Rehashes and
     structure memory for both rules; counts are identical by construction
     (checked by histogram)."""
     from kmertreecounter_b200 import sizing
@@ -573,14 +584,16 @@ def compare_sizing(args, kc, torch, dev, n, k, buckets, device_batch=None, steps
             cfg.device_batch_bytes = DEVICE_BATCH[args.workload]
         with kc.Counter(cfg) as c:
             split = []
+            # learned: the prediction (the first 1% counted on a helper
+            # context, the network's forward pass) runs inside every step,
+            # beside the count's k-mer extraction (sizing.BesideSizing)
+            beside = sizing.BesideSizing(c, model, k, 150) if rule == "learned" else None
+            if beside:
+                beside.target = (dev.data_ptr(), n)
 
             def step():
-                t0 = time.perf_counter()
-                if rule == "learned":
-                    sizing.predict_device(c, model, dev.data_ptr(), n, k, 150)
-                t1 = time.perf_counter()
                 st_ = c.count_device(dev.data_ptr(), n)
-                split.append(((t1 - t0) * 1e3, st_.device_ms))
+                split.append((beside.last_ms if beside else 0.0, st_.device_ms))
                 return st_
             step()
             times = []
@@ -593,8 +606,12 @@ def compare_sizing(args, kc, torch, dev, n, k, buckets, device_batch=None, steps
             hist[rule] = c.histogram(1, 1000)
             out[rule] = dict(ms_per_step=statistics.median(times), rehashes=st.rehashes, table_slots=st.table_slots,
                              filter_words=st.filter_words, table_keys=st.table_keys,
-                             predict_ms=statistics.median(x[0] for x in split),
+                             predict_beside_ms=statistics.median(x[0] for x in split),
                              count_device_ms=statistics.median(x[1] for x in split))
+            if beside:
+                if beside.error:
+                    raise beside.error
+                beside.close()
     out["identical_counts"] = bool(np.array_equal(hist["sampled"][0], hist["learned"][0])
                                    and hist["sampled"][1] == hist["learned"][1])
     out["margin"] = model.margin
@@ -605,7 +622,7 @@ def large_long_record(args, kc, torch, dev_peaks, pk):
     """The long-key shape at full size (seeded 200 Mbp genome, 40% GC, 30%
     repeat families, 50x of 150 bp = 66.7M reads, 10 Gbases, 21 GB FASTQ,
     1% substitution; canonical k=63, 128-bit keys, 4096 buckets), FASTQ
-    resident in HBM and counted in 2 GiB device passes: Gbases/s over
+    resident in HBM and counted in 4 GiB device passes: Gbases/s over
     --ll-steps steps timed with CUDA events on the library's stream, stage
     times, the count kernel's roofline in the same units as the main line,
     and learned vs sampled sizing on the same input."""

@@ -35,6 +35,19 @@ int kc_bucket_loads(kc_context* ctx, uint64_t* distinct, uint64_t* table_keys, u
  * on this context with cfg.sizing = KC_SIZING_LEARNED (NULL clears). */
 int kc_set_predicted_loads(kc_context* ctx, const double* distinct, const double* table_keys);
 
+/* A callback for learned sizing beside the count: with cfg.sizing =
+ * KC_SIZING_LEARNED, every count on this context calls fn(user, ctx) at its
+ * sizing point -- after the first batch's k-mer extraction has been enqueued
+ * and before any filter or table is laid out -- so that work the callback
+ * does (a prefix count on ANOTHER context, the network's forward pass) runs
+ * while that extraction does.  The callback hands its predictions with
+ * kc_set_predicted_loads(ctx, ...) and returns 0; a non-zero return fails the
+ * count with KC_ERR_INVALID; no prediction keeps the sampled rule.  It must
+ * not start a count on ctx.  fn = NULL removes it.  No reference
+ * counterpart. */
+typedef int (*kc_sizing_fn)(void* user, kc_context* ctx);
+int kc_set_sizing_callback(kc_context* ctx, kc_sizing_fn fn, void* user);
+
 /* ---- learned sizing of many read sets (kc_count_sets) -------------------
  * Per set s, k-mers per model bucket (top 12 bits of the canonical key) of
  * bytes [offset, offset + bytes) of each set descriptor (typically each set's

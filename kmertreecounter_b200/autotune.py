@@ -59,10 +59,11 @@ def passes(sets, per_pass, max_bytes=None):
     return out
 
 
-def count_in_passes(counter, dptr, sets, per_pass, rehashes=None, max_bytes=None):
+def count_in_passes(counter, dptr, sets, per_pass, rehashes=None, max_bytes=None, stages=None, table_slots=None):
     """kc_count_sets over `sets` in groups of `per_pass` (and `max_bytes`);
-    device ms total.  `rehashes`, a list, receives each pass's table growth
-    steps."""
+    device ms total.  `rehashes` and `table_slots`, lists, receive each
+    pass's table growth steps and table slots; `stages`, a dict, accumulates
+    the passes' stage times (ms) when the counter's profiling is on."""
     ms = 0.0
     results = []
     for i, j in passes(sets, per_pass, max_bytes):
@@ -72,6 +73,11 @@ def count_in_passes(counter, dptr, sets, per_pass, rehashes=None, max_bytes=None
         ms += counter.stats.device_ms
         if rehashes is not None:
             rehashes.append(int(counter.stats.rehashes))
+        if table_slots is not None:
+            table_slots.append(int(counter.stats.table_slots))
+        if stages is not None:
+            for name, (ms_, _) in counter.stage_times().items():
+                stages[name] = stages.get(name, 0.0) + ms_
         results.extend(res)
     return ms, results
 

@@ -58,7 +58,7 @@ def build(force=False, verbose_ptxas=False):
         _run(["g++", "-O3", "-std=c++20", "-fPIC", "-shared", "-o", SYNTH, os.path.join(CSRC, "synth.cpp"),
               "-lpthread"])
     if force or _stale(TREE, _deps("tree_main.cpp") + [LIB]):
-        _run(["g++", "-O2", "-std=c++20", "-o", TREE, os.path.join(CSRC, "tree_main.cpp"), "-L" + HERE,
+        _run(["g++", "-O2", "-std=c++20", "-pthread", "-o", TREE, os.path.join(CSRC, "tree_main.cpp"), "-L" + HERE,
               "-lkmertree_b200", "-Wl,-rpath,$ORIGIN/.."])
     if force or _stale(POST, _deps("post_main.cpp") + [LIB]):
         _run(["g++", "-O2", "-std=c++20", "-o", POST, os.path.join(CSRC, "post_main.cpp"), "-L" + HERE,

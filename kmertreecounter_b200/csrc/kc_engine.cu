@@ -231,6 +231,9 @@ struct kc_context {
 
     // optional learned sizing hook (per-bucket repeat-key predictions)
     std::vector<double> pred_distinct, pred_table;  // learned sizing, per model bucket (4096)
+    kc_sizing_fn sizing_cb = nullptr;  // learned sizing: called at each count's sizing point
+    void* sizing_user = nullptr;
+    bool side_in_ready = false;        // ev_side_in already recorded for this sizing
 
     // control-path mailbox: mapped pinned memory, [0, MBOX_UP) for uploads and
     // [MBOX_UP, MBOX_UP + MBOX_DOWN) for readbacks (put / get / sync_stream)
@@ -484,10 +487,13 @@ int size_structures(kc_context* c, const std::vector<uint64_t>& kb, double scale
         const bool beside = init_bytes < 4 * batch_bytes;
         cudaStream_t is = c->stream;
         if (beside) {
-            CK(cudaEventRecord(c->ev_side_in, c->stream));
+            // after the work queued before this batch's extraction (recorded
+            // before it when sizing follows the extraction's launch)
+            if (!c->side_in_ready) CK(cudaEventRecord(c->ev_side_in, c->stream));
             CK(cudaStreamWaitEvent(c->side, c->ev_side_in, 0));
             is = c->side;
         }
+        c->side_in_ready = false;
         Stage st(c, KC_STAGE_INIT, bw ? 2 : 1, is);
         const int ig = c->sm_count * (beside ? 2 : 8);
         if (bw) kc::zero16<<<ig, 256, 0, is>>>(c->bloom.as<uint4>(), bw / 2);  // bw: a sum of powers of two >= 256
@@ -926,11 +932,13 @@ int process_batch(kc_context* c, const uint8_t* buf, uint64_t n, int has_halo, b
         }
         // at least 65536 keys: one CTA's run of a bucket (<= 8192 keys) always fits
         const uint64_t ovf_cap = est ? std::max<uint64_t>(1ull << 16, total_cap / 32) : 0;
-        if (!c->sized && !route_only) {
-            double scale = 1.0;
-            if (c->expected_total_bytes > n && n > 0) scale = (double)c->expected_total_bytes / (double)n;
-            if ((rc = size_structures(c, kest, scale, n))) return rc;
-        }
+        // filter and tables are sized from these totals after the extraction
+        // is enqueued (it does not read them), so that a learned-sizing
+        // callback's work and the structures' initialisation run beside it
+        const bool size_here = !c->sized && !route_only;
+        const double scale =
+            (c->expected_total_bytes > n && n > 0) ? (double)c->expected_total_bytes / (double)n : 1.0;
+        if (size_here && !total_cap && (rc = size_structures(c, kest, scale, n))) return rc;
         if (!total_cap) {  // no k-mers in this batch
             if (route_only) c->routed_keys = 0;
             return KC_OK;
@@ -948,7 +956,16 @@ int process_batch(kc_context* c, const uint8_t* buf, uint64_t n, int has_halo, b
             CKR(put(c, d_scal + 2, &total_cap, sizeof(uint64_t)));
             CKR(fill_dev(c, c->region_fill.p, rb * sizeof(uint64_t), 0xFFFFFFFFu));
         }
+        if (size_here) {
+            CK(cudaEventRecord(c->ev_side_in, c->stream));
+            c->side_in_ready = true;
+        }
         if ((rc = launch_extract<NW>(c, buf, n, has_halo, kc::SCATTER, rb, 1, est, total_cap, cap_keys))) return rc;
+        if (size_here) {
+            if (c->cfg.sizing == KC_SIZING_LEARNED && c->sizing_cb && c->sizing_cb(c->sizing_user, c) != 0)
+                return fail(KC_ERR_INVALID, "the sizing callback failed");
+            if ((rc = size_structures(c, kest, scale, n))) return rc;
+        }
         if (!est) {
             n_keys = kb = total_cap;
             break;
@@ -1482,6 +1499,9 @@ int kc_create(const kc_config* cfg, kc_context** out) {
     cudaFuncSetAttribute(kc::extract_kernel<4, kc::SCATTER>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)kc::extract_smem_bytes<4, kc::SCATTER>(4096));
     cudaFuncSetAttribute(kc::count_window, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kc::window_smem_bytes());
+    cudaFuncSetAttribute(kc::loads_table_pass<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kc::loads_table_smem());
+    cudaFuncSetAttribute(kc::loads_table_pass<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kc::loads_table_smem());
+    cudaFuncSetAttribute(kc::loads_table_pass<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kc::loads_table_smem());
     cudaFuncSetAttribute(kc::subroute_scatter, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)kc::scatter_smem_bytes());
     if ((e = cudaGetLastError()) != cudaSuccess) {
@@ -1923,11 +1943,15 @@ template <int NW>
 void loads_kernels(kc_context* c, unsigned long long* dd) {
     const int grid = c->sm_count * 8;
     kc::hist_clear_marks<NW><<<grid, 256, 0, c->stream>>>(c->table.p, c->table_slots_used);
-    kc::loads_low_pass<NW><<<grid, 256, 0, c->stream>>>(c->low_packed.as<uint8_t>(), c->low_total, c->cfg.k,
-                                                        c->meta.as<kc::BucketMeta>(), c->bucket_shift, c->table.p, dd,
-                                                        dd + 2 * KC_MODEL_BUCKETS);
+    // per-CTA shared-memory totals: a few CTAs per SM, each flushing 4096 bins once
+    const uint64_t lgrid = std::max<uint64_t>(1, std::min<uint64_t>(ceil_div(c->low_total, 4096),
+                                                                      (uint64_t)c->sm_count * 2));
+    kc::loads_low_pass<NW><<<lgrid, 512, kc::loads_low_smem(), c->stream>>>(
+        c->low_packed.as<uint8_t>(), c->low_total, c->cfg.k, c->meta.as<kc::BucketMeta>(), c->bucket_shift,
+        c->table.p, dd, dd + 2 * KC_MODEL_BUCKETS);
     if (c->n_chunks)
-        kc::loads_table_pass<NW><<<std::min<uint64_t>(c->n_chunks, (uint64_t)grid), 256, 0, c->stream>>>(
+        kc::loads_table_pass<NW><<<std::min<uint64_t>(c->n_chunks, (uint64_t)c->sm_count * 2), 512,
+                                   kc::loads_table_smem(), c->stream>>>(
             c->table.p, c->chunks.as<kc::ExportChunk>(), c->n_chunks, dd, dd + KC_MODEL_BUCKETS,
             dd + 2 * KC_MODEL_BUCKETS);
 }
@@ -2521,6 +2545,13 @@ extern "C" int kc_set_prefix_kmers(kc_context* c, const uint8_t* d_fastq, const 
     return c->nw == 1 ? set_prefix_kmers_impl<1>(c, d_fastq, sets, n_sets, counts)
                       : (c->nw == 2 ? set_prefix_kmers_impl<2>(c, d_fastq, sets, n_sets, counts)
                                     : set_prefix_kmers_impl<4>(c, d_fastq, sets, n_sets, counts));
+}
+
+extern "C" int kc_set_sizing_callback(kc_context* c, kc_sizing_fn fn, void* user) {
+    if (!c) return fail(KC_ERR_INVALID, "null context");
+    c->sizing_cb = fn;
+    c->sizing_user = fn ? user : nullptr;
+    return KC_OK;
 }
 
 extern "C" int kc_set_predicted_set_rates(kc_context* c, uint32_t n_sets, const double* distinct,

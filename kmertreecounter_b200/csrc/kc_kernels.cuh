@@ -1990,10 +1990,27 @@ __global__ void hist_table_pass(const void* table, const ExportChunk* chunks, ui
 // Per model bucket (key word 0 >> 52) loads of the last result: low keys,
 // looked up in their table (marked as in hist_low_pass), then every table
 // key.  distinct = low keys + unmarked table keys; kmers = occurrences.
+// model buckets of the sizing loads (the top 12 bits of the key)
+constexpr uint32_t KC_LOADS_BINS = 4096;
+// dynamic shared memory of loads_low_pass / loads_table_pass
+constexpr size_t loads_low_smem() { return KC_LOADS_BINS * (8 + 4); }
+constexpr size_t loads_table_smem() { return KC_LOADS_BINS * (8 + 4 + 4); }
+
 template <int NW>
 __global__ void loads_low_pass(const uint8_t* low, uint64_t n_low, uint32_t k, const BucketMeta* meta,
                                uint32_t bucket_shift, void* table, unsigned long long* distinct,
                                unsigned long long* kmers) {
+    // per-CTA totals per model bucket in shared memory (consecutive low keys
+    // share their model bucket, so global atomics would serialise on it),
+    // added to the global totals once per CTA
+    extern __shared__ unsigned long long ld_smem[];
+    unsigned long long* s_kmers = ld_smem;                                        // [KC_LOADS_BINS]
+    uint32_t* s_distinct = reinterpret_cast<uint32_t*>(ld_smem + KC_LOADS_BINS);  // [KC_LOADS_BINS]
+    for (uint32_t i = threadIdx.x; i < KC_LOADS_BINS; i += blockDim.x) {
+        s_kmers[i] = 0;
+        s_distinct[i] = 0;
+    }
+    __syncthreads();
     using K = typename KeyOf<NW>::T;
     using S = typename SlotOf<NW>::T;
     const uint32_t full = k / 32, tail_bits = 2 * (k % 32), tail_bytes = (tail_bits + 7) / 8;
@@ -2010,14 +2027,30 @@ __global__ void loads_low_pass(const uint8_t* low, uint64_t n_low, uint32_t k, c
             else if constexpr (NW == 2) tab[at].pad[0] = 1;
             else tab[at].mark = 1;
         }
-        atomicAdd(distinct + (key_hi(key) >> 52), 1ull);
-        atomicAdd(kmers + (key_hi(key) >> 52), occ);
+        const uint32_t bin = (uint32_t)(key_hi(key) >> 52);
+        atomicAdd(s_distinct + bin, 1u);
+        atomicAdd(s_kmers + bin, occ);
+    }
+    __syncthreads();
+    for (uint32_t i = threadIdx.x; i < KC_LOADS_BINS; i += blockDim.x) {
+        if (s_distinct[i]) atomicAdd(distinct + i, (unsigned long long)s_distinct[i]);
+        if (s_kmers[i]) atomicAdd(kmers + i, s_kmers[i]);
     }
 }
 
 template <int NW>
 __global__ void loads_table_pass(const void* table, const ExportChunk* chunks, uint64_t n_chunks,
                                  unsigned long long* distinct, unsigned long long* tkeys, unsigned long long* kmers) {
+    extern __shared__ unsigned long long ld_smem[];
+    unsigned long long* s_kmers = ld_smem;                                        // [KC_LOADS_BINS]
+    uint32_t* s_distinct = reinterpret_cast<uint32_t*>(ld_smem + KC_LOADS_BINS);  // [KC_LOADS_BINS]
+    uint32_t* s_tkeys = s_distinct + KC_LOADS_BINS;                               // [KC_LOADS_BINS]
+    for (uint32_t i = threadIdx.x; i < KC_LOADS_BINS; i += blockDim.x) {
+        s_kmers[i] = 0;
+        s_distinct[i] = 0;
+        s_tkeys[i] = 0;
+    }
+    __syncthreads();
     using S = typename SlotOf<NW>::T;
     for (uint64_t c = blockIdx.x; c < n_chunks; c += gridDim.x)
     for (uint32_t q = threadIdx.x; q < chunks[c].n_slots; q += blockDim.x) {
@@ -2038,11 +2071,18 @@ __global__ void loads_table_pass(const void* table, const ExportChunk* chunks, u
             hi = s.w0;
         }
         if (!used) continue;
-        atomicAdd(tkeys + (hi >> 52), 1ull);
+        const uint32_t bin = (uint32_t)(hi >> 52);
+        atomicAdd(s_tkeys + bin, 1u);
         if (!marked) {
-            atomicAdd(distinct + (hi >> 52), 1ull);
-            atomicAdd(kmers + (hi >> 52), (unsigned long long)s.count);
+            atomicAdd(s_distinct + bin, 1u);
+            atomicAdd(s_kmers + bin, (unsigned long long)s.count);
         }
+    }
+    __syncthreads();
+    for (uint32_t i = threadIdx.x; i < KC_LOADS_BINS; i += blockDim.x) {
+        if (s_tkeys[i]) atomicAdd(tkeys + i, (unsigned long long)s_tkeys[i]);
+        if (s_distinct[i]) atomicAdd(distinct + i, (unsigned long long)s_distinct[i]);
+        if (s_kmers[i]) atomicAdd(kmers + i, s_kmers[i]);
     }
 }
 

@@ -25,6 +25,7 @@
 #include <iostream>
 #include <limits>
 #include <string>
+#include <thread>
 
 #include "../../include/kmer_count.h"
 
@@ -91,9 +92,26 @@ int main(int argc, char* argv[]) {
     // Stage 0 as the reference reports it (src/main.cpp:111-186): thread
     // split, then the sampled prefix counts' average, the classifier loads and
     // the largest filter.  Informational: the count below sizes its
-    // structures from exact per-bucket totals.  KC_STAGE0=0 skips it.
+    // structures from exact per-bucket totals, so the report is computed on a
+    // second thread while the count runs and printed before the count's
+    // lines.  KC_STAGE0=0 skips it.
     const char* s0 = std::getenv("KC_STAGE0");
-    if (!s0 || std::string(s0) != "0") {
+    const bool stage0 = !s0 || std::string(s0) != "0";
+    kc_stage0 s{};
+    int src = KC_OK;
+    std::string s0_err;
+    std::thread s0_thread;
+    if (stage0)
+        s0_thread = std::thread([&] {
+            src = kc_stage0_file(&cfg, filename.c_str(), (uint32_t)n_thread, &s);
+            if (src != KC_OK) s0_err = kc_last_error();
+        });
+
+    kc_stats st;
+    const int rc = kc_count_fastq(&cfg, filename.c_str(), out_dir ? out_dir : "./tmp/", &st);
+    const std::string count_err = rc != KC_OK ? kc_last_error() : "";
+    if (stage0) {
+        s0_thread.join();
         const unsigned long parsers = n_thread / 8 > 0 ? n_thread / 8 : 1;
         const unsigned long budget = n_thread - 2 - parsers;
         const unsigned long classifiers = budget / 2 ? budget / 2 : 1;
@@ -101,10 +119,8 @@ int main(int argc, char* argv[]) {
         std::cout << "  parser threads: " << parsers << std::endl;
         std::cout << "  classifier threads: " << classifiers << std::endl;
         std::cout << "  task threads: " << budget - classifiers << std::endl;
-        kc_stage0 s;
-        const int src = kc_stage0_file(&cfg, filename.c_str(), (uint32_t)n_thread, &s);
         if (src != KC_OK) {
-            std::cerr << kc_last_error() << std::endl;
+            std::cerr << s0_err << std::endl;
             return src == KC_ERR_INVALID ? 1 : 255;
         }
         std::cout << "Average prefix count: " << s.average_prefix_count << std::endl;
@@ -113,11 +129,8 @@ int main(int argc, char* argv[]) {
                       << s.classifier_load[s.load_order[i]] << std::endl;
         std::cout << "Max Bloom Filter capacity: " << s.max_bloom_filter_capacity << std::endl;
     }
-
-    kc_stats st;
-    const int rc = kc_count_fastq(&cfg, filename.c_str(), out_dir ? out_dir : "./tmp/", &st);
     if (rc != KC_OK) {
-        std::cerr << kc_last_error() << std::endl;
+        std::cerr << count_err << std::endl;
         return rc == KC_ERR_INVALID ? 1 : 255;
     }
     std::cout << "Largest filter of this count (64-bit words): " << st.max_bucket_filter_words << std::endl;

@@ -66,6 +66,7 @@ _SIG = {
     "kc_mlp_set_under_weight": (C.c_int, [C.c_void_p, C.c_float]),
     "kc_set_prefix_kmers": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(_native.KcSetDesc), C.c_uint32, _u64]),
     "kc_set_predicted_set_rates": (C.c_int, [C.c_void_p, C.c_uint32, _d, _d]),
+    "kc_set_sizing_callback": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
 }
 for _n, (_r, _a) in _SIG.items():
     getattr(lib, _n).restype = _r
@@ -242,20 +243,66 @@ def decode(y, kmers_est):
     return _from_y(y[:MODEL_BUCKETS]) * kest, _from_y(y[MODEL_BUCKETS:]) * kest
 
 
-def predict_on(counter, model, k, read_len, total_bytes, run_prefix):
+def predict_on(counter, model, k, read_len, total_bytes, run_prefix, target=None):
     """Profile a prefix on `counter` (plain rule), predict the full run's
-    per-bucket loads, hand them to `counter` (KC_SIZING_LEARNED) for its next
-    count.  run_prefix() counts the prefix and returns its byte length.
-    Returns (distinct, table keys) as handed over (margin applied)."""
-    check(lib.kc_set_predicted_loads(counter._ctx, None, None))
+    per-bucket loads, hand them to `target` (default: `counter`; it must use
+    KC_SIZING_LEARNED) for its next count.  run_prefix() counts the prefix
+    and returns its byte length.  Returns (distinct, table keys) as handed
+    over (margin applied)."""
+    target = counter if target is None else target
+    check(lib.kc_set_predicted_loads(target._ctx, None, None))
     pbytes = run_prefix()
     loads = bucket_loads(counter)
     x = features(loads, k, read_len, total_bytes, pbytes)
     scale = total_bytes / max(pbytes, 1)
     d, t = decode(model.forward(x[None, :])[0], loads[2].astype(np.float64) * scale)
     t = t * model.margin
-    apply(counter, (d, t))
+    apply(target, (d, t))
     return d, t
+
+
+_SIZING_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_void_p)
+
+
+class BesideSizing:
+    """Learned sizing run beside the count (kc_set_sizing_callback): every
+    count of device-resident FASTQ on `counter` (KC_SIZING_LEARNED) calls
+    back at its sizing point, after its k-mer extraction is enqueued; the
+    callback counts the first 1% of the same FASTQ on a helper context (plain
+    rule), runs the network and hands the predictions to `counter`, while the
+    extraction runs.  Set `target = (device pointer, bytes)` before each
+    count; `last_ms` is the callback's own wall time."""
+
+    def __init__(self, counter, model, k, read_len, device=0):
+        from ._native import Counter
+        self.counter, self.model, self.k, self.read_len = counter, model, k, read_len
+        self.helper = Counter(k=k, device=device)
+        self.target = None
+        self.last_ms = 0.0
+        self.error = None
+        self._cb = _SIZING_FN(self._call)  # kept alive as long as the registration
+        check(lib.kc_set_sizing_callback(counter._ctx, C.cast(self._cb, C.c_void_p), None))
+
+    def _call(self, user, ctx):
+        import time
+        t0 = time.perf_counter()
+        try:
+            dptr, n = self.target
+            pn = prefix_len(n)
+
+            def run():
+                self.helper.count_device(dptr, pn)
+                return pn
+            predict_on(self.helper, self.model, self.k, self.read_len, n, run, target=self.counter)
+        except Exception as e:  # reported by the count as KC_ERR_INVALID
+            self.error = e
+            return 1
+        self.last_ms = (time.perf_counter() - t0) * 1e3
+        return 0
+
+    def close(self):
+        check(lib.kc_set_sizing_callback(self.counter._ctx, None, None))
+        self.helper.close()
 
 
 def predict_host(counter, model, data, k, read_len):

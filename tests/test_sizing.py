@@ -129,3 +129,40 @@ def test_learned_sizing_avoids_rehashes_beyond_training_scale():
     print(r)
     assert r["exact_match"]
     assert r["rehash_sampled"] > 0 and r["rehash_learned"] == 0
+
+
+@pytest.mark.skipif(not os.path.exists(sizing.MODEL_PATH), reason="trained sizing model not present")
+def test_sizing_beside_the_count():
+    """kc_set_sizing_callback (sizing.BesideSizing): the count calls back at
+    its sizing point with its extraction already enqueued; the prefix is
+    counted on a helper context and the predictions size this count's
+    structures (the same sizes as predicting first); counts are the oracle's;
+    a failing callback fails the count and the context stays usable."""
+    import torch
+    p = synth.plain_small(seed=81, scale=0.3)
+    data = synth.fastq(p)
+    d = torch.from_numpy(data).cuda()
+    model = sizing.MLP.load()
+    keys, counts, _ = oracle.count(data, 31)
+    want = [int(v) for v in oracle.histogram(counts, 1, 200)]
+    with kc.Counter(k=31, sizing=kc.KC_SIZING_LEARNED) as first:
+        sizing.predict_device(first, model, d.data_ptr(), data.size, 31, 150)
+        st_first = first.count_device(d.data_ptr(), data.size)
+    with kc.Counter(k=31, sizing=kc.KC_SIZING_LEARNED) as c:
+        beside = sizing.BesideSizing(c, model, 31, 150)
+        beside.target = (d.data_ptr(), data.size)
+        for _ in range(2):
+            beside.last_ms = 0.0
+            st = c.count_device(d.data_ptr(), data.size)
+            assert beside.error is None and beside.last_ms > 0
+            assert st.table_slots == st_first.table_slots and st.filter_words == st_first.filter_words
+            h, distinct = c.histogram(1, 200)
+            assert distinct == keys.shape[0] and [int(v) for v in h] == want
+        beside.target = None  # the callback raises: the count fails
+        with pytest.raises(kc.KcError) as e:
+            c.count_device(d.data_ptr(), data.size)
+        assert e.value.code == kc.KC_ERR_INVALID
+        beside.close()
+        c.count_device(d.data_ptr(), data.size)  # no callback: the last predictions handed over
+        h, distinct = c.histogram(1, 200)
+        assert distinct == keys.shape[0] and [int(v) for v in h] == want
