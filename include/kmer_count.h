@@ -353,7 +353,7 @@ const char* kc_stage_name(int stage);
  * KC_NOALLOC_MAX_FASTQ_BYTES, 256 buckets, k 1..64, canonical only) on
  * `stream` (a cudaStream_t, NULL = default stream) and writes the packed
  * low.bin bytes to d_low and the root records, grouped by root id, to d_roots
- * (device buffers with the given byte capacities); stats receives the
+ * (16-byte aligned device buffers with the given byte capacities); stats receives the
  * counters.  All scratch comes from one static device array of
  * KC_NOALLOC_SCRATCH_BYTES per GPU, held until exit.  With CUDA's lazy module
  * loading (the default since CUDA 12.2) that array is reserved when the first
@@ -361,7 +361,7 @@ const char* kc_stage_name(int stage);
  * that first call before the caller's allocator claims the device budget (or
  * run with CUDA_MODULE_LOADING=EAGER), and before any stream capture.  Calls
  * share the array: overlapping calls on the GPU race and must be serialised
- * by the caller.  Larger inputs, other k or bucket counts, an unaligned input
+ * by the caller.  Larger inputs, other k or bucket counts, unaligned buffers
  * and output buffers too small for the result are rejected with
  * KC_ERR_INVALID; a table that outgrows the array ends the call with
  * KC_ERR_OVERFLOW. */

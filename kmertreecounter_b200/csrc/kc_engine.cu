@@ -2383,8 +2383,9 @@ int count_sets_impl(kc_context* c, const uint8_t* buf, const kc_set_desc* sets, 
     if (ext_err) return fail(KC_ERR_DEVICE, "internal error: routing bucket disagreed with its reservation");
     std::vector<uint64_t> lowbase(n_sets);
     uint64_t lb = 0, total_low = 0;
-    for (uint32_t s = 0; s < n_sets; ++s) {
+    for (uint32_t s = 0; s < n_sets; ++s) {  // each set's low.bin bytes start 16-byte aligned
         total_low += lows[s];
+        lb = (lb + 15) & ~15ull;
         lowbase[s] = lb;
         lb += lows[s] * kc_packed_bytes(sets[s].k);
     }
@@ -2392,7 +2393,8 @@ int count_sets_impl(kc_context* c, const uint8_t* buf, const kc_set_desc* sets, 
     CK(c->low_packed.ensure(lb + 64));
     if (nsegs) {
         Stage st(c, KC_STAGE_PACK_LOW);
-        kc::pack_low_sets<NW><<<std::min<uint64_t>(ceil_div(nsegs, 8), 148 * 16), 256, 0, c->stream>>>(
+        kc::pack_low_sets<NW><<<std::min<uint64_t>(ceil_div(nsegs, 8 * 32), (uint64_t)c->sm_count * 16), 256, 0,
+                                c->stream>>>(
             c->routed.p, c->tile_low.as<uint32_t>(), c->tile_low_prefix.as<uint64_t>(), nsegs, d_seg, d_k, d_lowbase,
             n_sets, c->low_packed.as<uint8_t>());
     }

@@ -1514,13 +1514,16 @@ __global__ void init_slots(void* tab, uint64_t n) {
 
 // ------------------------------------------------------------------ export
 
+// Bytes of one low.bin record for k.
+KC_HD uint32_t kc_packed(uint32_t k) { return (k / 32) * 8 + (2 * (k % 32) + 7) / 8; }
+
 // low.bin packing (src/ExportWriter.h:522-550): k/32 full words as raw
 // little-endian u64, then the top ceil(2(k%32)/8) bytes of the tail word
 // (masked to its 2(k%32) high bits), in little-endian byte order.
 // One key packed at d (P bytes; full = k/32 whole words, tail_bytes of the
 // masked tail word).
 template <int NW>
-__device__ __forceinline__ void pack_key(const typename KeyOf<NW>::T& key, uint8_t* d, uint32_t full,
+KC_HD void pack_key(const typename KeyOf<NW>::T& key, uint8_t* d, uint32_t full,
                                          uint32_t tail_bytes, uint32_t P, uint64_t tmask) {
     // word f of the key (f < 4; words past the key's width read 0)
     auto word = [&](uint32_t f) -> uint64_t {
@@ -1539,15 +1542,23 @@ __device__ __forceinline__ void pack_key(const typename KeyOf<NW>::T& key, uint8
         reinterpret_cast<uint64_t*>(d)[1] = full == 2 ? word(1) : (word(1) & tmask);
     } else {
         // k/32 whole words little-endian, then the top tail_bytes bytes
-        // of the masked tail word (src/ExportWriter.h:522-550)
-        uint32_t q = 0;
-        for (uint32_t f = 0; f < full; ++f) {
-            const uint64_t w = word(f);
-            for (uint32_t b = 0; b < 8; ++b) d[q++] = (uint8_t)(w >> (8 * b));
-        }
-        if (tail_bytes) {
-            const uint64_t tw = (full < 4 ? word(full) : 0ull) & tmask;
-            for (uint32_t b = 8 - tail_bytes; b < 8; ++b) d[q++] = (uint8_t)(tw >> (8 * b));
+        // of the masked tail word (src/ExportWriter.h:522-550): the record is
+        // the little-endian byte string of the words w_0..w_{full-1}, t with
+        // t = the masked tail word's top tail_bytes bytes.  d is a multiple
+        // of P from an 8-byte aligned base, so it is aligned to P's lowest
+        // set bit: stores of that width (1, 2 or 4 bytes) never straddle a
+        // word of the string.
+        const uint64_t t = tail_bytes ? (((full < 4 ? word(full) : 0ull) & tmask) >> (8 * (8 - tail_bytes))) : 0ull;
+        auto sw = [&](uint32_t f) -> uint64_t { return f < full ? word(f) : t; };
+        const uint32_t W = P & (0u - P);
+        if (W >= 4) {
+            for (uint32_t q = 0; q < P; q += 4)
+                *reinterpret_cast<uint32_t*>(d + q) = (uint32_t)(sw(q >> 3) >> (8 * (q & 7)));
+        } else if (W == 2) {
+            for (uint32_t q = 0; q < P; q += 2)
+                *reinterpret_cast<uint16_t*>(d + q) = (uint16_t)(sw(q >> 3) >> (8 * (q & 7)));
+        } else {
+            for (uint32_t q = 0; q < P; ++q) d[q] = (uint8_t)(sw(q >> 3) >> (8 * (q & 7)));
         }
     }
 }
@@ -2120,53 +2131,56 @@ __global__ void fill_set_gaps(void* routed, const uint64_t* set_end_key, const u
 }
 
 // Pack first occurrences of a multi-set batch: segment sg of set s writes at
-// low_byte_base[s] + (prefix[sg] - prefix[first segment of s]) * P(k_s).
+// low_byte_base[s] (a multiple of 16) + (prefix[sg] - prefix[first segment
+// of s]) * P(k_s).  A warp takes 32 segments at a time (each lane finds its
+// segment's set and output place), then packs the segments that have first
+// occurrences one after another, every lane a key.
 template <int NW>
 __global__ void pack_low_sets(const void* routed, const uint32_t* seg_low, const uint64_t* seg_low_prefix, uint64_t n_segs,
                               const uint64_t* set_seg_start, const uint32_t* set_k, const uint64_t* low_byte_base,
                               uint32_t n_sets, uint8_t* out) {
     using K = typename KeyOf<NW>::T;
     constexpr int SEG = count_seg<NW>();
-    const K* keys = reinterpret_cast<const K*>(routed);
+    constexpr int PER = SEG / 32;  // keys per lane per segment
+    const K* __restrict__ keys = reinterpret_cast<const K*>(routed);
     const int lane = threadIdx.x & 31;
     const uint64_t warps = (uint64_t)gridDim.x * (blockDim.x >> 5);
-    for (uint64_t sg = (uint64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); sg < n_segs; sg += warps) {
-        const uint32_t n = seg_low[sg];
-        if (!n) continue;
-        uint32_t lo = 0, hi = n_sets;
-        while (hi - lo > 1) {
-            const uint32_t mid = (lo + hi) / 2;
-            if (set_seg_start[mid] <= sg) lo = mid;
-            else hi = mid;
-        }
-        const uint32_t k = set_k[lo];
-        const uint32_t full = k / 32, tail_bits = 2 * (k % 32), tail_bytes = (tail_bits + 7) / 8;
-        const uint32_t P = full * 8 + tail_bytes;
-        const uint64_t tmask = tail_bits ? (~0ull << (64 - tail_bits)) : 0ull;
-        const uint64_t first = seg_low_prefix[set_seg_start[lo]];
-        uint8_t* dst0 = out + low_byte_base[lo] + (seg_low_prefix[sg] - first) * P;
-        for (uint32_t i = lane; i < n; i += 32) {
-            const K key = keys[sg * (uint64_t)SEG + i];
-            uint64_t w[4] = {0, 0, 0, 0};
-            if constexpr (NW == 1) {
-                w[0] = key;
-            } else if constexpr (NW == 2) {
-                w[0] = key.w0;
-                w[1] = key.w1;
-            } else {
-                w[0] = key.w0;
-                w[1] = key.w1;
-                w[2] = key.w2;
-                w[3] = key.w3;
+    for (uint64_t g = ((uint64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)) * 32; g < n_segs;
+         g += warps * 32) {
+        const uint64_t my = g + lane;
+        uint32_t n_l = 0, k_l = 1;
+        uint64_t dst_l = 0;
+        if (my < n_segs && (n_l = seg_low[my]) != 0) {
+            uint32_t lo = 0, hi = n_sets;
+            while (hi - lo > 1) {
+                const uint32_t mid = (lo + hi) / 2;
+                if (set_seg_start[mid] <= my) lo = mid;
+                else hi = mid;
             }
-            // byte by byte: a set's low.bin bytes start at any byte offset
-            uint8_t* d = dst0 + (uint64_t)i * P;
-            uint32_t q = 0;
-            for (uint32_t f = 0; f < full; ++f)
-                for (uint32_t b = 0; b < 8; ++b) d[q++] = (uint8_t)(w[f] >> (8 * b));
-            if (tail_bytes) {
-                const uint64_t tw = (full < 4 ? w[full] : 0ull) & tmask;
-                for (uint32_t b = 8 - tail_bytes; b < 8; ++b) d[q++] = (uint8_t)(tw >> (8 * b));
+            k_l = set_k[lo];
+            dst_l = low_byte_base[lo] + (seg_low_prefix[my] - seg_low_prefix[set_seg_start[lo]]) * kc_packed(k_l);
+        }
+        uint32_t todo = __ballot_sync(0xffffffffu, n_l != 0);
+        while (todo) {
+            const int q = __ffs(todo) - 1;
+            todo &= todo - 1;
+            const uint32_t n = __shfl_sync(0xffffffffu, n_l, q);
+            const uint32_t k = __shfl_sync(0xffffffffu, k_l, q);
+            const uint64_t dst = __shfl_sync(0xffffffffu, dst_l, q);
+            const uint32_t full = k / 32, tail_bits = 2 * (k % 32), tail_bytes = (tail_bits + 7) / 8;
+            const uint32_t P = full * 8 + tail_bytes;
+            const uint64_t tmask = tail_bits ? (~0ull << (64 - tail_bits)) : 0ull;
+            const uint64_t s0 = (g + (uint64_t)q) * (uint64_t)SEG;
+            K v[PER];
+#pragma unroll
+            for (int j = 0; j < PER; ++j) {
+                const uint32_t i = j * 32 + lane;
+                if (i < n) v[j] = keys[s0 + i];
+            }
+#pragma unroll
+            for (int j = 0; j < PER; ++j) {
+                const uint32_t i = j * 32 + lane;
+                if (i < n) pack_key<NW>(v[j], out + dst + (uint64_t)i * P, full, tail_bytes, P, tmask);
             }
         }
     }

@@ -333,6 +333,9 @@ extern "C" int kc_count_device_noalloc(const kc_config* cfg, const uint8_t* d_fa
     if (n > KC_NOALLOC_MAX_FASTQ_BYTES)
         return err(KC_ERR_INVALID, "input larger than KC_NOALLOC_MAX_FASTQ_BYTES (1 MiB) for the no-alloc entry point");
     if (reinterpret_cast<uintptr_t>(d_fastq) % 16) return err(KC_ERR_INVALID, "device FASTQ must be 16-byte aligned");
+    // the packing and export kernels store whole words into the outputs
+    if (reinterpret_cast<uintptr_t>(d_low) % 16 || reinterpret_cast<uintptr_t>(d_roots) % 16)
+        return err(KC_ERR_INVALID, "output buffers must be 16-byte aligned");
     int dev = 0;
     NK(cudaGetDevice(&dev));
     if (dev < 0 || dev >= kMaxDevices) return err(KC_ERR_DEVICE, "device ordinal out of range for the no-alloc path");

@@ -9,10 +9,12 @@
 //   * bucket_of_window() equals the top bits of that canonical key (k <= 64),
 //   * for k = 65..128: window_at4() and canonical4() the same way, and
 //     runs_at_least5() marks exactly the bytes that end k consecutive bases,
+//   * pack_key() writes every k's low.bin record layout,
 //   * nth_set_bit() finds every set bit of random words in order.
 #include <cstdio>
 #include <cstdint>
 #include <cstdlib>
+#include <cstring>
 #include <random>
 #include <vector>
 
@@ -107,6 +109,44 @@ static long check_long_keys(std::mt19937_64& rng) {
     return checks;
 }
 
+// pack_key (low.bin records, widest aligned stores) against the record
+// layout written byte by byte: k/32 whole words little-endian, then the top
+// ceil(2(k%32)/8) bytes of the masked tail word, for every k and records
+// packed back to back from an aligned base.
+static long check_pack_key(std::mt19937_64& rng) {
+    long checks = 0;
+    alignas(16) uint8_t got[40 * 8], want[40 * 8];
+    for (uint32_t k = 1; k <= 128; ++k) {
+        const uint32_t full = k / 32, tail_bits = 2 * (k % 32), tail_bytes = (tail_bits + 7) / 8;
+        const uint32_t P = full * 8 + tail_bytes;
+        const uint64_t tmask = tail_bits ? (~0ull << (64 - tail_bits)) : 0ull;
+        for (int rep = 0; rep < 50; ++rep) {
+            std::memset(got, 0xAB, sizeof got);
+            std::memset(want, 0xAB, sizeof want);
+            for (uint32_t i = 0; i < 8; ++i) {
+                const uint64_t w[4] = {rng(), rng(), rng(), rng()};
+                uint8_t* d = want + i * P;
+                uint32_t q = 0;
+                for (uint32_t f = 0; f < full; ++f)
+                    for (uint32_t b = 0; b < 8; ++b) d[q++] = (uint8_t)(w[f] >> (8 * b));
+                if (tail_bytes) {
+                    const uint64_t tw = (full < 4 ? w[full] : 0ull) & tmask;
+                    for (uint32_t b = 8 - tail_bytes; b < 8; ++b) d[q++] = (uint8_t)(tw >> (8 * b));
+                }
+                if (k <= 32) pack_key<1>(w[0], got + i * P, full, tail_bytes, P, tmask);
+                else if (k <= 64) pack_key<2>(Key2{w[0], w[1]}, got + i * P, full, tail_bytes, P, tmask);
+                else pack_key<4>(Key4{w[0], w[1], w[2], w[3]}, got + i * P, full, tail_bytes, P, tmask);
+            }
+            if (std::memcmp(got, want, sizeof got) != 0) {
+                std::printf("pack_key mismatch k=%u\n", k);
+                std::exit(1);
+            }
+            ++checks;
+        }
+    }
+    return checks;
+}
+
 // nth_set_bit (the export's bitmap walk) against a plain enumeration.
 static long check_nth_set_bit(std::mt19937_64& rng) {
     long checks = 0;
@@ -132,6 +172,7 @@ int main() {
     std::mt19937_64 rng(12345);
     long checks = 0;
     checks += check_nth_set_bit(rng);
+    checks += check_pack_key(rng);
     for (int iter = 0; iter < 20000; ++iter) {
         // three 32-byte segments of codes, byte 0 of each in bits 63..62
         std::vector<int> bases(96);

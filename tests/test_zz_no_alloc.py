@@ -156,6 +156,11 @@ def test_noalloc_allocates_nothing_and_rejects_bad_requests():
     rejected(run(c=kc.default_config(k=65)), "k out of range: 1..64")
     rejected(run(c=kc.default_config(k=k, n_buckets=4096)), "256 buckets only")
     rejected(run(n=data.size - 16, in_ptr=d_in.data_ptr() + 8), "16-byte aligned")
+    off = _native.lib.kc_count_device_noalloc(C.byref(cfg), C.c_void_p(d_in.data_ptr()), data.size,
+                                              C.c_void_p(d_low.data_ptr() + 4), d_low.numel() - 4,
+                                              C.c_void_p(d_roots.data_ptr()), d_roots.numel(), None,
+                                              C.byref(_native.KcStats()))
+    rejected(off, "output buffers must be 16-byte aligned")
     # a call right after the rejections is still exact
     want, K = allocating(data, d_in, k)
     check_noalloc(cfg, data, d_in, want, K)
