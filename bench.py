@@ -804,6 +804,11 @@ def run_ours(args):
         total_ms = float(t.item())
     ms_step = total_ms / args.steps
     _, distinct = counter.histogram(1, 2)  # exact distinct keys (outside the timed region)
+    # the merged count histogram of the device-held result (histogram_tool
+    # precise's output, counts 1..10000), timed on its own after the steps
+    t_h = time.perf_counter()
+    counter.histogram(1, 10000)
+    histogram_ms = (time.perf_counter() - t_h) * 1e3
     stats = st.as_dict()
     stats.pop("root_counts", None)
     gpu_launches = int(sum(stage_launch.values()))
@@ -871,6 +876,7 @@ def run_ours(args):
         "config": workload_config(args, world, n, bases, p.n_reads),
         "distinct_kmers": distinct,
         "distinct_kmers_per_s": distinct * world / (ms_step / 1e3),
+        "histogram_ms": histogram_ms,
         "stats": stats,
         "stages_ms_per_step": {s: v / args.steps for s, v in stage_ms.items()},
         "gpu_launches": gpu_launches,

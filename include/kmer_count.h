@@ -79,6 +79,10 @@ typedef struct kc_config {
                                   * filter and table lines more often in L2; the cost is
                                   * the routed-key buffer, about 3 bytes per FASTQ byte
                                   * for k <= 32 and 6 for k <= 64. */
+    int32_t priority;      /* 1: the context's main stream at the device's highest
+                            * priority, so its kernels are scheduled ahead of work
+                            * already queued on other streams (a sizing prediction
+                            * made beside another context's count); 0 = default */
 } kc_config;
 
 /* Counters of one run.  total_kmers and root_records match the reference's

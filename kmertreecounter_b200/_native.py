@@ -46,6 +46,7 @@ class KcConfig(C.Structure):
         ("n_buckets", C.c_uint32), ("sizing", C.c_uint32), ("device", C.c_int32), ("sort_output", C.c_uint32),
         ("chunk_bytes", C.c_uint64), ("batch_bytes", C.c_uint64), ("bloom_bits", C.c_double),
         ("table_load", C.c_double), ("repeat_ratio", C.c_double), ("device_batch_bytes", C.c_uint64),
+        ("priority", C.c_int32),
     ]
 
 

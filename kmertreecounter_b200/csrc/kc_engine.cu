@@ -323,6 +323,7 @@ int setup_shape(kc_context* c) {
     if (g.batch_bytes < (1ull << 20)) return fail(KC_ERR_INVALID, "batch_bytes must be at least 1 MiB");
     if (g.device_batch_bytes && g.device_batch_bytes < (1ull << 20))
         return fail(KC_ERR_INVALID, "device_batch_bytes must be 0 or at least 1 MiB");
+    if (g.priority != 0 && g.priority != 1) return fail(KC_ERR_INVALID, "priority must be 0 or 1");
     c->nw = g.k <= 32 ? 1 : (g.k <= 64 ? 2 : 4);
     c->n_buckets = g.n_buckets;
     c->bucket_bits = g.n_buckets == 256 ? 8 : 12;
@@ -1456,13 +1457,15 @@ int kc_create(const kc_config* cfg, kc_context** out) {
     }
     c->device = cfg->device;
     cudaDeviceGetAttribute(&c->sm_count, cudaDevAttrMultiProcessorCount, cfg->device);
-    if ((e = cudaSetDevice(c->device)) != cudaSuccess || (e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking)) != cudaSuccess ||
+    int prio_low = 0, prio_high = 0;
+    if ((e = cudaSetDevice(c->device)) != cudaSuccess ||
+        (e = cudaDeviceGetStreamPriorityRange(&prio_low, &prio_high)) != cudaSuccess ||
+        (e = cudaStreamCreateWithPriority(&c->stream, cudaStreamNonBlocking, cfg->priority ? prio_high : 0)) !=
+            cudaSuccess ||
         (e = cudaEventCreate(&c->ev0)) != cudaSuccess || (e = cudaEventCreate(&c->ev1)) != cudaSuccess) {
         delete c;
         return fail(KC_ERR_DEVICE, "stream/event creation failed: %s", cudaGetErrorString(e));
     }
-    int prio_low = 0, prio_high = 0;
-    cudaDeviceGetStreamPriorityRange(&prio_low, &prio_high);
     if ((e = cudaStreamCreateWithFlags(&c->h2d, cudaStreamNonBlocking)) != cudaSuccess ||
         (e = cudaStreamCreateWithFlags(&c->d2h, cudaStreamNonBlocking)) != cudaSuccess ||
         (e = cudaStreamCreateWithPriority(&c->side, cudaStreamNonBlocking, prio_high)) != cudaSuccess ||

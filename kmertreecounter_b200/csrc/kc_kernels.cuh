@@ -163,6 +163,19 @@ __device__ __forceinline__ uint64_t hash_key(const Key4& k) {
     return mix64(k.w0 ^ mix64(k.w1 ^ mix64(k.w2 ^ mix64(k.w3 + 0x9e3779b97f4a7c15ull))));
 }
 
+// Bit 7 of each byte of the result: that byte of x is zero.  Exact per byte:
+// (b & 0x7F) + 0x7F carries into bit 7 unless the low seven bits are zero,
+// and never out of the byte.
+KC_HD uint32_t zero_bytes(uint32_t x) {
+    const uint32_t t = ((x & 0x7F7F7F7Fu) + 0x7F7F7F7Fu) | x;
+    return ~t & 0x80808080u;
+}
+
+// Bit 7 of byte j (j = 0..3) -> bit j of the result: the four flag bits sit
+// at 7, 15, 23, 31; times 2^21 + 2^14 + 2^7 + 1 they meet at bits 28..31
+// (the other products fall below bit 22 or out of the word).
+KC_HD uint32_t gather_bit7(uint32_t f) { return (f * 0x00204081u) >> 28; }
+
 // Reverse the order of the 32 two-bit bases of a word (base p -> 31-p).
 KC_HD uint64_t rev_bases(uint64_t x) {
     x = brev64(x);
@@ -343,7 +356,7 @@ static __global__ void lines_per_tile(const uint8_t* __restrict__ buf, uint64_t 
             const uint4 a = __ldcs(p), b = __ldcs(p + 1);
             const uint32_t w[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
 #pragma unroll
-            for (int i = 0; i < 8; ++i) cnt += __popc(__vcmpeq4(w[i], 0x0A0A0A0Au) & 0x01010101u);
+            for (int i = 0; i < 8; ++i) cnt += __popc(zero_bytes(w[i] ^ 0x0A0A0A0Au));
         } else {
             for (uint32_t j = 0; j < (uint32_t)rem; ++j) cnt += buf[pos + j] == '\n';
         }
@@ -367,7 +380,7 @@ static __global__ void lines_per_set_tile(const uint8_t* __restrict__ buf, const
             const uint4 a = __ldcs(p), b = __ldcs(p + 1);
             const uint32_t w[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
 #pragma unroll
-            for (int i = 0; i < 8; ++i) cnt += __popc(__vcmpeq4(w[i], 0x0A0A0A0Au) & 0x01010101u);
+            for (int i = 0; i < 8; ++i) cnt += __popc(zero_bytes(w[i] ^ 0x0A0A0A0Au));
         } else {
             for (uint32_t j = 0; j < (uint32_t)rem; ++j) cnt += buf[pos + j] == '\n';
         }
@@ -395,28 +408,30 @@ struct Seg {
     uint32_t nls;    // bit j set: byte j is '\n'
 };
 
-// Four bytes at a time: base test by SIMD byte compares, 2-bit code by the
+// Four bytes at a time: base test (A/C/G/T/U after folding case) by the
+// exact zero-byte test of x ^ letter, newline likewise, 2-bit code by the
 // ((c >> 1) ^ (c >> 2)) & 3 identity (A=0 C=1 G=2 T/U=3, either case).
-__device__ __forceinline__ Seg classify(const uint32_t (&w)[8], uint64_t valid_bytes) {
+KC_HD Seg classify(const uint32_t (&w)[8], uint64_t valid_bytes) {
     Seg s{0, 0, 0};
+    uint32_t chi = 0, clo = 0;  // codes of bytes 0..15 (chi) and 16..31 (clo)
 #pragma unroll
     for (int i = 0; i < 8; ++i) {
         const uint32_t x = w[i];
         const uint32_t u = x & 0xDFDFDFDFu;
-        const uint32_t isb = __vcmpeq4(u, 0x41414141u) | __vcmpeq4(u, 0x43434343u) | __vcmpeq4(u, 0x47474747u) |
-                             __vcmpeq4(u, 0x54545454u) | __vcmpeq4(u, 0x55555555u);
-        const uint32_t isn = __vcmpeq4(x, 0x0A0A0A0Au);
+        const uint32_t isb = zero_bytes(u ^ 0x41414141u) | zero_bytes(u ^ 0x43434343u) | zero_bytes(u ^ 0x47474747u) |
+                             zero_bytes(u ^ 0x54545454u) | zero_bytes(u ^ 0x55555555u);
+        const uint32_t isn = zero_bytes(x ^ 0x0A0A0A0Au);
+        s.bases |= gather_bit7(isb) << (4 * i);
+        s.nls |= gather_bit7(isn) << (4 * i);
+        // codes of bytes 4i..4i+3 -> 8 bits, byte 4i in the high pair: the
+        // 2-bit fields at 0, 8, 16, 24 times 2^30 + 2^20 + 2^10 + 1 land at
+        // 30, 28, 26, 24 (the other products fall below bit 22 or out)
         const uint32_t code4 = ((x >> 1) ^ (x >> 2)) & 0x03030303u;
-        // gather one bit per byte (bit 7 of each compare byte) into 4 bits
-        const uint32_t bm = ((isb >> 7) & 1u) | ((isb >> 14) & 2u) | ((isb >> 21) & 4u) | ((isb >> 28) & 8u);
-        const uint32_t nm = ((isn >> 7) & 1u) | ((isn >> 14) & 2u) | ((isn >> 21) & 4u) | ((isn >> 28) & 8u);
-        s.bases |= bm << (4 * i);
-        s.nls |= nm << (4 * i);
-        // codes of bytes 4i..4i+3 -> 8 bits, byte 4i in the high pair
-        const uint32_t c8 = ((code4 & 3u) << 6) | (((code4 >> 8) & 3u) << 4) | (((code4 >> 16) & 3u) << 2) |
-                            ((code4 >> 24) & 3u);
-        s.codes |= (uint64_t)c8 << (56 - 8 * i);
+        const uint32_t c8 = (code4 * 0x40100401u) >> 24;
+        if (i < 4) chi |= c8 << (24 - 8 * i);
+        else clo |= c8 << (24 - 8 * (i - 4));
     }
+    s.codes = ((uint64_t)chi << 32) | clo;
     if (valid_bytes < 32) {
         const uint32_t keep = valid_bytes ? (0xFFFFFFFFu >> (32 - (uint32_t)valid_bytes)) : 0u;
         s.bases &= keep;
@@ -1914,10 +1929,18 @@ __device__ __forceinline__ bool table_find(const typename SlotOf<NW>::T* tab, ui
 
 __device__ __forceinline__ void hist_add(uint32_t* sh, unsigned long long* gh, uint64_t merged, uint32_t lo,
                                          uint32_t hi) {
-    if (merged < lo || merged > hi) return;
+    // the active lanes of the warp that share a shared-memory bin add once
+    // (nearly every low.bin key lands in the bin of count 1, and shared-memory
+    // atomics on one address are serialised)
+    const bool in = merged >= lo && merged <= hi;
     const uint64_t bin = merged - lo;
-    if (bin < HIST_SMEM) atomicAdd(sh + bin, 1u);
-    else atomicAdd(gh + bin, 1ull);
+    const uint32_t key = in && bin < HIST_SMEM ? (uint32_t)bin : 0xFFFFFFFFu;
+    const uint32_t same = __match_any_sync(__activemask(), key);
+    if (key != 0xFFFFFFFFu) {
+        if ((int)(__ffs(same) - 1) == (int)(threadIdx.x & 31)) atomicAdd(sh + key, (uint32_t)__popc(same));
+    } else if (in) {
+        atomicAdd(gh + bin, 1ull);
+    }
 }
 
 template <int NW>

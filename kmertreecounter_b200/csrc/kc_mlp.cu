@@ -314,7 +314,11 @@ int kc_mlp_create(int in, int hid, int out, int max_batch, uint64_t seed, kc_mlp
     m->out = out;
     m->max_batch = max_batch;
     const int dims[4] = {in, hid, hid, out};
-    if (cudaStreamCreateWithFlags(&m->st, cudaStreamNonBlocking) != cudaSuccess) {
+    // the network's kernels at the device's highest priority: a prediction
+    // made beside a count is not held up by the count's queued kernels
+    int prio_low = 0, prio_high = 0;
+    cudaDeviceGetStreamPriorityRange(&prio_low, &prio_high);
+    if (cudaStreamCreateWithPriority(&m->st, cudaStreamNonBlocking, prio_high) != cudaSuccess) {
         delete m;
         g_mlp_err = "stream creation failed";
         return KC_ERR_DEVICE;

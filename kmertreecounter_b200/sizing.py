@@ -276,7 +276,8 @@ class BesideSizing:
     def __init__(self, counter, model, k, read_len, device=0):
         from ._native import Counter
         self.counter, self.model, self.k, self.read_len = counter, model, k, read_len
-        self.helper = Counter(k=k, device=device)
+        # the helper's kernels go ahead of the count's queued extraction
+        self.helper = Counter(k=k, device=device, priority=1)
         self.target = None
         self.last_ms = 0.0
         self.error = None

@@ -10,6 +10,7 @@
 //   * for k = 65..128: window_at4() and canonical4() the same way, and
 //     runs_at_least5() marks exactly the bytes that end k consecutive bases,
 //   * pack_key() writes every k's low.bin record layout,
+//   * classify() flags bases and newlines and codes every byte,
 //   * nth_set_bit() finds every set bit of random words in order.
 #include <cstdio>
 #include <cstdint>
@@ -109,6 +110,40 @@ static long check_long_keys(std::mt19937_64& rng) {
     return checks;
 }
 
+// classify (bases, newlines and 2-bit codes of 32 bytes) against the
+// per-byte definition, for random bytes (all 256 values, and runs of the
+// letters that matter) and every valid length.
+static long check_classify(std::mt19937_64& rng) {
+    long checks = 0;
+    const char* alpha = "ACGTUacgtuNn\n\r@+IJ";
+    for (int iter = 0; iter < 200000; ++iter) {
+        uint8_t b[32];
+        for (int j = 0; j < 32; ++j)
+            b[j] = (iter & 1) ? (uint8_t)alpha[rng() % 20] : (uint8_t)rng();
+        uint32_t w[8];
+        for (int i = 0; i < 8; ++i)
+            w[i] = (uint32_t)b[4 * i] | ((uint32_t)b[4 * i + 1] << 8) | ((uint32_t)b[4 * i + 2] << 16) |
+                   ((uint32_t)b[4 * i + 3] << 24);
+        const uint64_t valid = iter % 7 == 0 ? rng() % 33 : 32;
+        const Seg s = classify(w, valid);
+        uint32_t bases = 0, nls = 0;
+        uint64_t codes = 0;
+        for (int j = 0; j < 32; ++j) {
+            const uint32_t c = b[j], u = c & 0xDF;
+            const bool base = u == 'A' || u == 'C' || u == 'G' || u == 'T' || u == 'U';
+            if (base && (uint64_t)j < valid) bases |= 1u << j;
+            if (c == '\n' && (uint64_t)j < valid) nls |= 1u << j;
+            codes |= (uint64_t)(((c >> 1) ^ (c >> 2)) & 3u) << (62 - 2 * j);
+        }
+        if (s.bases != bases || s.nls != nls || s.codes != codes) {
+            std::printf("classify mismatch at iteration %d\n", iter);
+            std::exit(1);
+        }
+        ++checks;
+    }
+    return checks;
+}
+
 // pack_key (low.bin records, widest aligned stores) against the record
 // layout written byte by byte: k/32 whole words little-endian, then the top
 // ceil(2(k%32)/8) bytes of the masked tail word, for every k and records
@@ -173,6 +208,7 @@ int main() {
     long checks = 0;
     checks += check_nth_set_bit(rng);
     checks += check_pack_key(rng);
+    checks += check_classify(rng);
     for (int iter = 0; iter < 20000; ++iter) {
         // three 32-byte segments of codes, byte 0 of each in bits 63..62
         std::vector<int> bases(96);
