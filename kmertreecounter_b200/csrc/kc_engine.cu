@@ -192,7 +192,7 @@ struct kc_context {
     std::vector<uint64_t> route_counts;
     bool have_route = false;
     DevBuf sort_tmp, sort_hist, sort_offs, sort_sums;
-    DevBuf set_tiles, tile_prefix, set_info;  // multi-set batches
+    DevBuf set_tiles, tile_prefix, set_info, hist_tiles;  // multi-set batches
     std::vector<double> set_pred_distinct, set_pred_table;  // learned rates per (set, root bucket)
     cudaGraphExec_t sets_exec = nullptr;      // the multi-set scatter/gap/count graph, replayed
     int sets_exec_nw = 0, sets_exec_nodes = 0;
@@ -1525,7 +1525,7 @@ void kc_destroy(kc_context* c) {
                       &c->tile_low, &c->tile_fail, &c->tile_low_prefix, &c->scan_sums, &c->scalars, &c->overflow,
                       &c->meta,   &c->bloom,     &c->table,     &c->low_packed,   &c->roots,         &c->chunks,
                       &c->root_count, &c->chunk_pass, &c->chunk_off, &c->sort_tmp, &c->sort_hist, &c->sort_offs, &c->sort_sums,
-                      &c->set_tiles, &c->tile_prefix, &c->set_info, &c->pass_bits, &c->loads, &c->routed2,
+                      &c->set_tiles, &c->tile_prefix, &c->set_info, &c->hist_tiles, &c->pass_bits, &c->loads, &c->routed2,
                       &c->grow_jobs, &c->grow_failed,
                       &c->bucket_win, &c->win_info, &c->win_order, &c->win_count, &c->win_padded, &c->win_start, &c->win_cursor,
                       &c->win_end};
@@ -2207,10 +2207,49 @@ int count_sets_impl(kc_context* c, const uint8_t* buf, const kc_set_desc* sets, 
     a.bucket_count = c->bucket_count.as<unsigned long long>();
     a.bucket_cursor = c->bucket_cursor.as<unsigned long long>();
     a.error = c->scalars.as<uint32_t>() + 12;
+    // Routing regions per (set, bucket).  A set of at least EST_MIN_TILES
+    // tiles is histogrammed on every EST_STRIDE-th of its tiles: its regions
+    // are estimates (x 1.02 + 4 standard deviations + 256 keys) followed by
+    // an overflow area of its own (at least 65536 keys, so one CTA's run of a
+    // bucket always fits), which a CTA's run that does not fit its region
+    // takes whole.  A smaller set is histogrammed on every tile and gets exact
+    // regions.  A pass whose overflow area filled is routed again, exactly.
+    bool exact_only = false;
+route_again:
+    std::vector<uint8_t> sampled(n_sets, 0);
+    std::vector<double> factor(n_sets, 1.0);
+    std::vector<uint32_t> hist_list;
+    bool any_sampled = false;
+    {
+        uint64_t t0 = 0;
+        for (uint32_t s = 0; s < n_sets; ++s) {
+            const uint64_t tn = ceil_div(sets[s].bytes, (uint64_t)kc::EXT_TILE);
+            sampled[s] = !exact_only && tn >= kc::EST_MIN_TILES;
+            uint64_t listed = 0;
+            for (uint64_t q = 0; q < tn; ++q)
+                if (!sampled[s] || q % kc::EST_STRIDE == 0) {
+                    hist_list.push_back((uint32_t)(t0 + q));
+                    ++listed;
+                }
+            if (sampled[s]) {
+                factor[s] = (double)tn / (double)listed;
+                any_sampled = true;
+            }
+            t0 += tn;
+        }
+    }
     CK(cudaMemsetAsync(c->bucket_count.p, 0, nbk * sizeof(uint64_t), c->stream));
     if (nt) {
+        if (any_sampled) {
+            CK(c->hist_tiles.ensure(hist_list.size() * sizeof(uint32_t)));
+            CK(cudaMemcpyAsync(c->hist_tiles.p, hist_list.data(), hist_list.size() * sizeof(uint32_t),
+                               cudaMemcpyHostToDevice, c->stream));
+            a.tile_list = c->hist_tiles.as<uint32_t>();
+        }
         Stage st(c, KC_STAGE_EXTRACT_HIST);
-        kc::extract_kernel<NW, kc::HIST><<<nt, kc::EXT_THREADS, kc::extract_smem_bytes<NW, kc::HIST>(NB), c->stream>>>(a);
+        kc::extract_kernel<NW, kc::HIST><<<any_sampled ? hist_list.size() : nt, kc::EXT_THREADS,
+                                           kc::extract_smem_bytes<NW, kc::HIST>(NB), c->stream>>>(a);
+        a.tile_list = nullptr;
     }
     CK(cudaGetLastError());
     std::vector<uint64_t> cnt(nbk);
@@ -2218,7 +2257,8 @@ int count_sets_impl(kc_context* c, const uint8_t* buf, const kc_set_desc* sets, 
     CK(cudaStreamSynchronize(c->stream));
 
     // layout: each set's routed region starts on a segment boundary
-    std::vector<uint64_t> start(nbk), set_key0(n_sets), set_key1(n_sets), set_next(n_sets), set_seg(n_sets);
+    std::vector<uint64_t> start(nbk), rend(nbk), set_key0(n_sets), set_key1(n_sets), set_next(n_sets), set_seg(n_sets);
+    std::vector<uint64_t> ovf_start(n_sets), ovf_end(n_sets);
     uint64_t pos = 0;
     c->h_meta.assign(nbk, kc::BucketMeta{});
     uint64_t bw = 0, ts = 0, K = 0;
@@ -2232,10 +2272,16 @@ int count_sets_impl(kc_context* c, const uint8_t* buf, const kc_set_desc* sets, 
         pos = ceil_div(pos, SEG) * SEG;
         set_key0[s] = pos;
         set_seg[s] = pos / SEG;
+        uint64_t set_cap = 0;
         for (uint32_t b = 0; b < NB; ++b) {
-            const uint64_t kb = cnt[(uint64_t)s * NB + b];
+            // k-mers of the bucket (estimated for a sampled set) and its region
+            const double e = (double)cnt[(uint64_t)s * NB + b] * factor[s];
+            const uint64_t kb = sampled[s] ? (uint64_t)e : cnt[(uint64_t)s * NB + b];
+            const uint64_t cap = sampled[s] ? (uint64_t)(e * 1.02 + 4.0 * std::sqrt(e) + 256.0) : kb;
             start[(uint64_t)s * NB + b] = pos;
-            pos += kb;
+            pos += cap;
+            rend[(uint64_t)s * NB + b] = pos;
+            set_cap += cap;
             K += kb;
             uint64_t words, slots;
             const uint64_t q = (uint64_t)s * NB + b;
@@ -2252,6 +2298,9 @@ int count_sets_impl(kc_context* c, const uint8_t* buf, const kc_set_desc* sets, 
             bw += words;
             ts += slots;
         }
+        ovf_start[s] = pos;
+        if (sampled[s]) pos += std::max<uint64_t>(1ull << 16, set_cap / 32);
+        ovf_end[s] = pos;
         set_key1[s] = pos;
     }
     const uint64_t n_keys = ceil_div(pos, SEG) * SEG;
@@ -2268,13 +2317,16 @@ int count_sets_impl(kc_context* c, const uint8_t* buf, const kc_set_desc* sets, 
     CK(c->tile_low.ensure(std::max<uint64_t>(nsegs, 1) * sizeof(uint32_t)));
     CK(c->tile_fail.ensure(std::max<uint64_t>(nsegs, 1) * sizeof(uint32_t)));
     CK(c->tile_low_prefix.ensure(std::max<uint64_t>(nsegs, 1) * sizeof(uint64_t)));
-    CK(c->set_info.ensure((size_t)n_sets * 6 * sizeof(uint64_t) + 64));
+    CK(c->set_info.ensure((size_t)n_sets * 9 * sizeof(uint64_t) + 64));
     uint64_t* d_seg = c->set_info.as<uint64_t>();              // set_seg_start[n_sets]
     uint64_t* d_end = d_seg + n_sets;                          // set_key1
     uint64_t* d_next = d_end + n_sets;                         // next set's first key
     uint64_t* d_low = d_next + n_sets;                         // low count per set
     uint64_t* d_lowbase = d_low + n_sets;                      // low byte base per set
-    uint32_t* d_k = reinterpret_cast<uint32_t*>(d_lowbase + n_sets);
+    uint64_t* d_ovs = d_lowbase + n_sets;                      // overflow area per set: start,
+    uint64_t* d_ove = d_ovs + n_sets;                          //   end,
+    uint64_t* d_ovc = d_ove + n_sets;                          //   cursor (end of the set's keys after the scatter)
+    uint32_t* d_k = reinterpret_cast<uint32_t*>(d_ovc + n_sets);
     std::vector<uint32_t> ks(n_sets);
     for (uint32_t s = 0; s < n_sets; ++s) ks[s] = sets[s].k;
     CK(cudaMemcpyAsync(d_seg, set_seg.data(), n_sets * sizeof(uint64_t), cudaMemcpyHostToDevice, c->stream));
@@ -2283,6 +2335,25 @@ int count_sets_impl(kc_context* c, const uint8_t* buf, const kc_set_desc* sets, 
     CK(cudaMemcpyAsync(d_k, ks.data(), n_sets * sizeof(uint32_t), cudaMemcpyHostToDevice, c->stream));
     CK(cudaMemcpyAsync(c->meta.p, c->h_meta.data(), nbk * sizeof(kc::BucketMeta), cudaMemcpyHostToDevice, c->stream));
     CK(cudaMemcpyAsync(c->bucket_cursor.p, start.data(), nbk * sizeof(uint64_t), cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(d_ovs, ovf_start.data(), n_sets * sizeof(uint64_t), cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(d_ove, ovf_end.data(), n_sets * sizeof(uint64_t), cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(d_ovc, ovf_start.data(), n_sets * sizeof(uint64_t), cudaMemcpyHostToDevice, c->stream));
+    if (any_sampled) {
+        CK(c->region_end.ensure(nbk * sizeof(uint64_t)));
+        CK(c->region_fill.ensure(nbk * sizeof(uint64_t)));
+        CK(cudaMemcpyAsync(c->region_end.p, rend.data(), nbk * sizeof(uint64_t), cudaMemcpyHostToDevice, c->stream));
+        CK(cudaMemsetAsync(c->region_fill.p, 0xFF, nbk * sizeof(uint64_t), c->stream));
+        a.region_end = c->region_end.as<unsigned long long>();
+        a.region_fill = c->region_fill.as<unsigned long long>();
+        a.set_ovf_start = d_ovs;
+        a.set_ovf_end = d_ove;
+        a.set_ovf_cursor = reinterpret_cast<unsigned long long*>(d_ovc);
+    } else {
+        a.region_end = nullptr;
+        a.region_fill = nullptr;
+        a.set_ovf_start = a.set_ovf_end = nullptr;
+        a.set_ovf_cursor = nullptr;
+    }
     {
         Stage st(c, KC_STAGE_INIT, 1);
         CK(cudaMemsetAsync(c->bloom.p, 0, bw * sizeof(uint64_t), c->stream));
@@ -2321,13 +2392,19 @@ int count_sets_impl(kc_context* c, const uint8_t* buf, const kc_set_desc* sets, 
         if (nt)
             kc::extract_kernel<NW, kc::SCATTER>
                 <<<nt, kc::EXT_THREADS, kc::extract_smem_bytes<NW, kc::SCATTER>(NB), c->stream>>>(a);
-        kc::fill_set_gaps<NW><<<n_sets, 256, 0, c->stream>>>(c->routed.p, d_end, d_next, n_sets);
+        if (any_sampled)  // EMPTY keys into the unfilled tails of the estimated regions
+            kc::fill_region_gaps<NW><<<nbk, 256, 0, c->stream>>>(
+                c->routed.p, c->bucket_cursor.as<unsigned long long>(), c->region_fill.as<unsigned long long>(),
+                c->region_end.as<unsigned long long>(), (uint32_t)nbk);
+        // and after each set's keys (its overflow area's unused part, the alignment gap)
+        kc::fill_set_gaps<NW><<<n_sets, 256, 0, c->stream>>>(c->routed.p, d_ovc, d_next, n_sets);
         if (cgrid) kc::count_routed<NW><<<cgrid, kc::CNT_THREADS, 0, c->stream>>>(ca);
         const cudaError_t ce = cudaStreamEndCapture(c->stream, &graph);
         if (ce != cudaSuccess) return fail(KC_ERR_DEVICE, "graph capture failed: %s", cudaGetErrorString(ce));
         cudaError_t e = cudaSuccess;
         bool updated = false;
-        if (c->sets_exec && c->sets_exec_nw == NW && c->sets_exec_nodes == (nt ? 3 : 2) + (cgrid ? 0 : -1)) {
+        const int nodes = (nt ? 1 : 0) + (any_sampled ? 1 : 0) + 1 + (cgrid ? 1 : 0);
+        if (c->sets_exec && c->sets_exec_nw == NW && c->sets_exec_nodes == nodes) {
             cudaGraphExecUpdateResultInfo info{};
             updated = cudaGraphExecUpdate(c->sets_exec, graph, &info) == cudaSuccess;
             if (!updated) cudaGetLastError();
@@ -2337,7 +2414,7 @@ int count_sets_impl(kc_context* c, const uint8_t* buf, const kc_set_desc* sets, 
             c->sets_exec = nullptr;
             e = cudaGraphInstantiate(&c->sets_exec, graph, 0);
             c->sets_exec_nw = NW;
-            c->sets_exec_nodes = (nt ? 3 : 2) + (cgrid ? 0 : -1);
+            c->sets_exec_nodes = nodes;
             ++c->sets_instantiations;
         }
         if (e == cudaSuccess) e = cudaGraphLaunch(c->sets_exec, c->stream);
@@ -2347,6 +2424,28 @@ int count_sets_impl(kc_context* c, const uint8_t* buf, const kc_set_desc* sets, 
             c->sets_exec = nullptr;
             return fail(KC_ERR_DEVICE, "graph launch failed: %s", cudaGetErrorString(e));
         }
+    }
+
+    // exact k-mers per (set, bucket): a region's cursor advanced by every run
+    // of its bucket, those sent to the overflow area included
+    std::vector<uint64_t> exact(nbk);
+    {
+        uint32_t flags = 0;
+        CK(cudaMemcpyAsync(exact.data(), c->bucket_cursor.p, nbk * sizeof(uint64_t), cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaMemcpyAsync(&flags, c->scalars.as<uint32_t>() + 12, sizeof flags, cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
+        if (flags & 2u) {  // an overflow area was full: route this pass again, exactly
+            CK(cudaMemsetAsync(c->scalars.as<uint32_t>() + 12, 0, sizeof(uint32_t), c->stream));
+            exact_only = true;
+            ++c->reroutes;
+            goto route_again;
+        }
+        K = 0;
+        for (uint64_t q = 0; q < nbk; ++q) {
+            exact[q] -= start[q];
+            K += exact[q];
+        }
+        c->K = K;
     }
 
     // overflowed tables: grow x4, move, retry only the failed keys
@@ -2427,7 +2526,7 @@ int count_sets_impl(kc_context* c, const uint8_t* buf, const kc_set_desc* sets, 
         std::memset(&r, 0, sizeof r);
         uint64_t km = 0;
         for (uint32_t b = 0; b < NB; ++b) {
-            km += cnt[(uint64_t)s * NB + b];
+            km += exact[(uint64_t)s * NB + b];
             r.root_counts[b] = rc_h[(uint64_t)s * NB + b];
             r.root_records += r.root_counts[b];
         }

@@ -581,6 +581,14 @@ struct ExtractArgs {
     unsigned long long* region_fill;
     unsigned long long* overflow_cursor;
     uint64_t overflow_start, overflow_end;
+    // multi-set batch with estimated regions: per set s an overflow area
+    // [set_ovf_start[s], set_ovf_end[s]) with cursor set_ovf_cursor[s]; the
+    // region arrays are indexed by set x n_buckets + bucket
+    const uint64_t* set_ovf_start;
+    const uint64_t* set_ovf_end;
+    unsigned long long* set_ovf_cursor;
+    // HIST over the listed tiles only (nullptr: every tile_stride-th)
+    const uint32_t* tile_list;
 };
 
 // Bucket of the canonical key of window (hi:lo) without building the key:
@@ -662,17 +670,20 @@ __global__ void __launch_bounds__(EXT_THREADS, EXT_MIN_CTAS) extract_kernel(Extr
     uint16_t* sorder = sbkt + STAGE;                               // one pass: arrival index by bucket order
 
     const int tid = threadIdx.x;
-    const uint64_t tile = (uint64_t)blockIdx.x * (a.tile_stride > 1 ? a.tile_stride : 1u);
+    const uint64_t tile = a.tile_list ? (uint64_t)a.tile_list[blockIdx.x]
+                                      : (uint64_t)blockIdx.x * (a.tile_stride > 1 ? a.tile_stride : 1u);
     uint64_t tile_start = tile * EXT_TILE;
     uint64_t n_end = a.n;
     bool halo_ok = tile_start > 0 || a.has_halo;
     uint32_t k = a.k;
     uint64_t bucket_off = 0;
+    uint32_t set = 0;
     if (a.tiles) {
-        const SetTile t = a.tiles[blockIdx.x];
+        const SetTile t = a.tiles[tile];
         tile_start = t.start;
         n_end = t.end;
-        halo_ok = t.first_tile != blockIdx.x;
+        halo_ok = t.first_tile != tile;
+        set = t.set;
         k = t.k;
         bucket_off = (uint64_t)t.set * a.n_buckets;
     }
@@ -758,18 +769,23 @@ __global__ void __launch_bounds__(EXT_THREADS, EXT_MIN_CTAS) extract_kernel(Extr
             const uint32_t b = tid * per + q;
             if (b < a.n_buckets) {
                 const uint32_t c = hist[b];
-                unsigned long long base = c ? atomicAdd(a.bucket_cursor + bucket_off + b, (unsigned long long)c) : 0ull;
-                if (a.region_end && c && base + c > a.region_end[b]) {
+                const uint64_t rb = bucket_off + b;  // the region (of this set)
+                unsigned long long base = c ? atomicAdd(a.bucket_cursor + rb, (unsigned long long)c) : 0ull;
+                if (a.region_end && c && base + c > a.region_end[rb]) {
                     // the run does not fit the region: it goes whole to the
                     // overflow area.  If that is full too, the batch is routed
                     // again (error bit 1) and the run lands, in bounds, at the
                     // overflow area's start (at least 65536 keys >= one run).
-                    atomicMin(a.region_fill + b, base);
-                    const unsigned long long ob = atomicAdd(a.overflow_cursor, (unsigned long long)c);
-                    if (ob + c <= a.overflow_end) {
+                    atomicMin(a.region_fill + rb, base);
+                    // a multi-set batch has an overflow area per set
+                    unsigned long long* const ocur = a.set_ovf_cursor ? a.set_ovf_cursor + set : a.overflow_cursor;
+                    const uint64_t oend = a.set_ovf_cursor ? a.set_ovf_end[set] : a.overflow_end;
+                    const uint64_t ostart = a.set_ovf_cursor ? a.set_ovf_start[set] : a.overflow_start;
+                    const unsigned long long ob = atomicAdd(ocur, (unsigned long long)c);
+                    if (ob + c <= oend) {
                         base = ob;
                     } else {
-                        base = a.overflow_start;
+                        base = ostart;
                         atomicOr(a.error, 2u);
                     }
                 }

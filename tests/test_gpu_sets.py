@@ -108,3 +108,57 @@ def test_sets_learned_sizing_is_exact(min_prefix):
             assert np.all(tab == -1) and np.all(dist == -1)
         res = c.count_sets(d.data_ptr(), sets)
         check_sets(c, res, sets, datas)
+
+
+def _tiled_sets(specs, seed):
+    """Sets of 8 KiB FASTQ records (one read per extraction tile, so that the
+    routing histogram's sampled tiles can be made unrepresentative): specs
+    is a list of (kinds or None for a small synthetic set, k)."""
+    import test_gpu_routing as tr
+    datas = []
+    for i, (kinds, k) in enumerate(specs):
+        if kinds is None:
+            p = synth.params(seed=seed * 31 + i, genome_len=50_000, n_reads=2000, read_len=(150, 150))
+            datas.append(synth.fastq(p))
+        else:
+            datas.append(tr.tiled_fastq(kinds, seed=seed + i))
+    offs, pos = [], 0
+    for d in datas:
+        offs.append(pos)
+        pos += (d.size + 15) // 16 * 16
+    buf = np.full(pos, ord("\n"), np.uint8)
+    for o, d in zip(offs, datas):
+        buf[o:o + d.size] = d
+    return buf, [(o, d.size, k) for o, d, (_, k) in zip(offs, datas, specs)], datas
+
+
+def test_sets_estimated_regions_overflow_into_the_set_area():
+    """Sets of at least 4096 tiles are routed from a histogram of every 32nd
+    tile: a bucket underestimated by the sample (poly-A reads in unsampled
+    tiles) spills into that set's own overflow area, small sets beside them
+    keep exact regions, and every set's counts are the oracle's."""
+    n = 4160
+    specs = [(["A" if i % 64 == 5 else "R" for i in range(n)], 31), (None, 21),
+             (["R" if i % 64 else "C" for i in range(n)], 31), (None, 31)]
+    buf, sets, datas = _tiled_sets(specs, seed=4)
+    d = torch.from_numpy(buf).cuda()
+    with kc.Counter(k=31) as c:
+        res = c.count_sets(d.data_ptr(), sets)
+        assert c.stats.reroutes == 0
+        check_sets(c, res, sets, datas)
+
+
+def test_sets_full_overflow_area_reroutes_exactly():
+    """A set whose sampled tiles are all poly-A and the rest poly-C: the
+    poly-C bucket is estimated empty and overflows the set's overflow area;
+    the pass is routed again with exact regions and stays exact."""
+    n = 4160
+    specs = [(None, 31), (["A" if i % 32 == 0 else "C" for i in range(n)], 31), (None, 21)]
+    buf, sets, datas = _tiled_sets(specs, seed=6)
+    d = torch.from_numpy(buf).cuda()
+    with kc.Counter(k=31) as c:
+        res = c.count_sets(d.data_ptr(), sets)
+        assert c.stats.reroutes == 1
+        check_sets(c, res, sets, datas)
+        res = c.count_sets(d.data_ptr(), sets)  # the next call routes from the sample again
+        check_sets(c, res, sets, datas)
