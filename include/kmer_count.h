@@ -223,6 +223,9 @@ typedef struct kc_set_result {
 
 int kc_count_sets(kc_context* ctx, const uint8_t* d_fastq, const kc_set_desc* sets, uint32_t n_sets,
                   kc_set_result* results, kc_stats* stats);
+/* Graph instantiations kc_count_sets has made on this context (a diagnostic:
+ * later calls with a shape seen before update and replay its graph). */
+uint64_t kc_sets_graph_instantiations(const kc_context* ctx);
 
 /* Sizes of the last result: packed low.bin bytes, number of root records,
  * and per-root record counts (256 entries, may be NULL). */

@@ -31,6 +31,7 @@ ABI_SYMBOLS = (
     "kc_set_profiling", "kc_stage_times", "kc_stage_name", "kc_count_device_noalloc", "kc_count_host_stream",
     "kc_histogram", "kc_count_sets", "kc_route_device", "kc_copy_routed", "kc_count_keys_device",
     "kc_stage0_rule", "kc_stage0_file", "kc_post_process", "kc_post_process_dir", "kc_routed_keys",
+    "kc_sets_graph_instantiations",
 )
 KC_SINK_LOW = 0
 KC_SINK_ROOT = 1
@@ -140,6 +141,7 @@ def _load():
         "kc_count_host_stream": (i32, [vp, vp, u64, SINK_FN, vp, stp]),
         "kc_histogram": (i32, [vp, u32, u32, C.POINTER(u64), C.POINTER(u64)]),
         "kc_count_sets": (i32, [vp, vp, C.POINTER(KcSetDesc), u32, C.POINTER(KcSetResult), stp]),
+        "kc_sets_graph_instantiations": (u64, [vp]),
         "kc_route_device": (i32, [vp, vp, u64, C.POINTER(u64)]),
         "kc_copy_routed": (i32, [vp, vp, u64]),
         "kc_routed_keys": (i32, [vp, C.POINTER(vp), C.POINTER(u64)]),
@@ -295,6 +297,10 @@ class Counter:
         out = np.empty(nr, dtype=dt)
         check(lib.kc_copy_roots(self._ctx, out.ctypes.data if nr else None, nr * dt.itemsize))
         return out, counts
+
+    def sets_graph_instantiations(self):
+        """Graph instantiations kc_count_sets has made on this context."""
+        return int(lib.kc_sets_graph_instantiations(self._ctx))
 
     def count_sets(self, dptr, sets):
         """Count many read sets in one device buffer in one pass.  `sets` is a

@@ -194,8 +194,12 @@ struct kc_context {
     DevBuf sort_tmp, sort_hist, sort_offs, sort_sums;
     DevBuf set_tiles, tile_prefix, set_info, hist_tiles;  // multi-set batches
     std::vector<double> set_pred_distinct, set_pred_table;  // learned rates per (set, root bucket)
-    cudaGraphExec_t sets_exec = nullptr;      // the multi-set scatter/gap/count graph, replayed
-    int sets_exec_nw = 0, sets_exec_nodes = 0;
+    // the multi-set scatter/gap/count graphs, replayed: one executable per
+    // shape (key width and kernel list; estimated regions add a gap fill)
+    static constexpr int SETS_EXECS = 4;
+    cudaGraphExec_t sets_exec[SETS_EXECS] = {};
+    int sets_exec_key[SETS_EXECS] = {};
+    int sets_exec_next = 0;                   // slot a new shape replaces
     uint64_t sets_instantiations = 0;         // times that graph had to be instantiated
     // windowed count of 64-bit keys (kc_window.cuh): window-grouped keys,
     // per-bucket window ids and per-window counts and key ranges
@@ -1546,7 +1550,8 @@ void kc_destroy(kc_context* c) {
         if (c->ev_ring[i]) cudaEventDestroy(c->ev_ring[i]);
         if (c->ring[i]) cudaFreeHost(c->ring[i]);
     }
-    if (c->sets_exec) cudaGraphExecDestroy(c->sets_exec);
+    for (cudaGraphExec_t& x : c->sets_exec)
+        if (x) cudaGraphExecDestroy(x);
     if (c->ev_pack) cudaEventDestroy(c->ev_pack);
     if (c->ev_mbox) cudaEventDestroy(c->ev_mbox);
     if (c->mbox_h) cudaFreeHost(c->mbox_h);
@@ -2379,11 +2384,12 @@ route_again:
     ca.use_filter = 1;
     const uint64_t cgrid = ceil_div(n_keys, (uint64_t)CT * kc::CNT_SEGS_PER_WARP);
 
-    // scatter -> gap fill -> count as one graph.  The context keeps the
-    // instantiated graph: a later call captures its own launches (the same
-    // three kernels, new arguments and grids) and updates the instantiated
-    // graph in place (cudaGraphExecUpdate), instantiating only when the update
-    // is refused; the replay is one launch of the whole sequence.
+    // scatter -> gap fill(s) -> count as one graph.  The context keeps the
+    // instantiated graph of each shape: a later call captures its own
+    // launches (the same kernels, new arguments and grids) and updates the
+    // instantiated graph of its shape in place (cudaGraphExecUpdate),
+    // instantiating only when the update is refused; the replay is one launch
+    // of the whole sequence.
     {
         Stage st(c, KC_STAGE_COUNT_ROUTED, 3);
         a.routed = c->routed.p;
@@ -2404,24 +2410,31 @@ route_again:
         cudaError_t e = cudaSuccess;
         bool updated = false;
         const int nodes = (nt ? 1 : 0) + (any_sampled ? 1 : 0) + 1 + (cgrid ? 1 : 0);
-        if (c->sets_exec && c->sets_exec_nw == NW && c->sets_exec_nodes == nodes) {
+        const int key = NW * 16 + nodes + (any_sampled ? 8 : 0);
+        int slot = -1;
+        for (int i = 0; i < kc_context::SETS_EXECS; ++i)
+            if (c->sets_exec[i] && c->sets_exec_key[i] == key) slot = i;
+        if (slot >= 0) {
             cudaGraphExecUpdateResultInfo info{};
-            updated = cudaGraphExecUpdate(c->sets_exec, graph, &info) == cudaSuccess;
+            updated = cudaGraphExecUpdate(c->sets_exec[slot], graph, &info) == cudaSuccess;
             if (!updated) cudaGetLastError();
+        } else {
+            slot = c->sets_exec_next;
+            c->sets_exec_next = (c->sets_exec_next + 1) % kc_context::SETS_EXECS;
         }
+        cudaGraphExec_t& ex = c->sets_exec[slot];
         if (!updated) {
-            if (c->sets_exec) cudaGraphExecDestroy(c->sets_exec);
-            c->sets_exec = nullptr;
-            e = cudaGraphInstantiate(&c->sets_exec, graph, 0);
-            c->sets_exec_nw = NW;
-            c->sets_exec_nodes = nodes;
+            if (ex) cudaGraphExecDestroy(ex);
+            ex = nullptr;
+            e = cudaGraphInstantiate(&ex, graph, 0);
+            c->sets_exec_key[slot] = key;
             ++c->sets_instantiations;
         }
-        if (e == cudaSuccess) e = cudaGraphLaunch(c->sets_exec, c->stream);
+        if (e == cudaSuccess) e = cudaGraphLaunch(ex, c->stream);
         cudaGraphDestroy(graph);
         if (e != cudaSuccess) {
-            if (c->sets_exec) cudaGraphExecDestroy(c->sets_exec);
-            c->sets_exec = nullptr;
+            if (ex) cudaGraphExecDestroy(ex);
+            ex = nullptr;
             return fail(KC_ERR_DEVICE, "graph launch failed: %s", cudaGetErrorString(e));
         }
     }
@@ -2650,6 +2663,8 @@ extern "C" int kc_set_prefix_kmers(kc_context* c, const uint8_t* d_fastq, const 
                       : (c->nw == 2 ? set_prefix_kmers_impl<2>(c, d_fastq, sets, n_sets, counts)
                                     : set_prefix_kmers_impl<4>(c, d_fastq, sets, n_sets, counts));
 }
+
+extern "C" uint64_t kc_sets_graph_instantiations(const kc_context* c) { return c ? c->sets_instantiations : 0; }
 
 extern "C" int kc_set_sizing_callback(kc_context* c, kc_sizing_fn fn, void* user) {
     if (!c) return fail(KC_ERR_INVALID, "null context");
