@@ -268,14 +268,27 @@ def time_reference(path, data, k, bases, runs, workdir):
     return out, kind, cores
 
 
-# DRAM traffic (dram__bytes_read.sum + dram__bytes_write.sum) of the count
-# kernel per step of the genome-scale workload, from one ncu capture of the
-# kernel sources whose sha256 is given (the capture and its command are
-# summarised in profiles/count_routed_genome_scale.md).  Reported only while
-# the kernel sources are unchanged since that capture.
+# DRAM traffic (dram__bytes_read.sum + dram__bytes_write.sum) per step of
+# each stage of the genome-scale workload, from one ncu capture of the
+# 10% case's first count (the kernels of kernel sources whose sha256 is
+# given; profiles/launches_genome_scale.md gives the command) scaled to the
+# full step by the units each stage processes: k-mers for extraction,
+# sub-routing and count (x 10.000), first occurrences for packing
+# (x 10.022), table cells for export and initialisation (x 9.781), FASTQ
+# bytes for the line scan (x 10.032).  Reported only while the kernel
+# sources are unchanged since that capture.
+_CAPTURE_SHA = "c3c5fe9e46d3c4d95d90874b4eaaa680d157e678fd0887a45b384a1a487ab048"
 PROFILED_TRAFFIC = {
     # workload: {stage: {"sources_sha256": ..., "bytes_per_step": ...}}
-    "genome_scale": {},
+    "genome_scale": {
+        "extract_scatter": {"sources_sha256": _CAPTURE_SHA, "bytes_per_step": int(2432631808 * 10.000)},
+        "subroute": {"sources_sha256": _CAPTURE_SHA, "bytes_per_step": int(3825624064 * 10.000)},
+        "count": {"sources_sha256": _CAPTURE_SHA, "bytes_per_step": int(4610623360 * 10.000)},
+        "pack_low": {"sources_sha256": _CAPTURE_SHA, "bytes_per_step": int(1244946176 * 10.022)},
+        "export": {"sources_sha256": _CAPTURE_SHA, "bytes_per_step": int(1920999680 * 9.781)},
+        "lines": {"sources_sha256": _CAPTURE_SHA, "bytes_per_step": int(627625472 * 10.032)},
+        "init": {"sources_sha256": _CAPTURE_SHA, "bytes_per_step": int(916664576 * 9.781)},
+    },
 }
 KERNEL_SOURCES = ("kmertreecounter_b200/csrc/kc_kernels.cuh", "kmertreecounter_b200/csrc/kc_window.cuh",
                   "kmertreecounter_b200/csrc/kc_engine.cu")
@@ -311,7 +324,7 @@ STAGE_KERNELS = {
 }
 
 
-def stage_rooflines(stage_ms, stats, F, k, hbm_gbs, P, rec):
+def stage_rooflines(stage_ms, stats, F, k, hbm_gbs, P, rec, traffic=None):
     """Algorithmic bytes per step of every timed stage (the bytes its job has
     to move, counted once) over its device time, against the HBM peak:
 
@@ -349,6 +362,9 @@ def stage_rooflines(stage_ms, stats, F, k, hbm_gbs, P, rec):
         gbs = b / (ms / 1e3) / 1e9
         out[s_] = {"ms": ms, "alg_bytes": b, "rule": rule, "gbs": gbs, "frac": gbs / hbm_gbs,
                    "kernels": STAGE_KERNELS[s_]}
+        if traffic and traffic.get(s_) is not None:  # measured DRAM bytes (profiled, scaled)
+            out[s_]["traffic"] = traffic[s_]
+            out[s_]["traffic_over_alg"] = traffic[s_] / b
     return out
 
 
@@ -854,7 +870,8 @@ def run_ours(args):
     K, L = stats["total_kmers"], stats["low_records"]
     count_ms = stage_ms.get("count", 0.0) / args.steps
     per_stage = stage_rooflines({s_: v / args.steps for s_, v in stage_ms.items()}, stats, n, k, pk["hbm_gbs"],
-                                kc.packed_bytes(k), kc.record_bytes(k))
+                                kc.packed_bytes(k), kc.record_bytes(k),
+                                {s_: profile_traffic(args, s_)[0] for s_ in STAGE_KERNELS})
     dominant = max(per_stage, key=lambda s_: per_stage[s_]["ms"]) if per_stage else None
     roof = pipeline_roofline(dev_peaks, pk, n, K, L, stats["root_records"], kc.packed_bytes(k), kc.record_bytes(k),
                              ms_step, count_ms)
