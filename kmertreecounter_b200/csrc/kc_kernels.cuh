@@ -1943,82 +1943,6 @@ __device__ __forceinline__ bool table_find(const typename SlotOf<NW>::T* tab, ui
     return false;
 }
 
-// Slot s against key: 0 = empty (the key is absent), 1 = the key, 2 = another key.
-template <int NW>
-__device__ __forceinline__ int slot_vs_key(const typename SlotOf<NW>::T& s, const typename KeyOf<NW>::T& key) {
-    if constexpr (NW == 1) {
-        return s.key == EMPTY ? 0 : (s.key == key ? 1 : 2);
-    } else if constexpr (NW == 2) {
-        return (s.w0 == EMPTY && s.w1 == EMPTY) ? 0 : ((s.w0 == key.w0 && s.w1 == key.w1) ? 1 : 2);
-    } else {
-        if (s.state != SLOT_READY) return 0;  // after the count every used slot is ready
-        return (s.w0 == key.w0 && s.w1 == key.w1 && s.w2 == key.w2 && s.w3 == key.w3) ? 1 : 2;
-    }
-}
-
-// The table slots of LOW_BATCH low.bin records r0 + j * step (j < LOW_BATCH,
-// records past n_low skipped): every record's key, then every first probe
-// issued before any is resolved (the loads are independent; one record at a
-// time leaves a thread waiting on one dependent chain), then the rest of each
-// probe sequence.  at[j] = the key's slot in its table (relative to tab[j]),
-// or ~0 when absent.
-// records per thread and batch: as many as the registers of 4 CTAs of 256
-// threads per SM hold (a 256-bit key and its slot take 4x a 64-bit one's)
-template <int NW>
-__host__ __device__ constexpr int low_batch() {
-    return NW == 1 ? 4 : (NW == 2 ? 2 : 1);
-}
-template <int NW, int LOW_BATCH = low_batch<NW>()>
-__device__ __forceinline__ void find_low_batch(const uint8_t* low, uint64_t n_low, uint64_t r0, uint64_t step,
-                                               uint32_t P, uint32_t full, uint32_t tail_bytes,
-                                               const BucketMeta* meta, uint32_t bucket_shift, void* table,
-                                               typename KeyOf<NW>::T (&key)[LOW_BATCH],
-                                               typename SlotOf<NW>::T* (&tab)[LOW_BATCH],
-                                               uint64_t (&at)[LOW_BATCH], bool (&have)[LOW_BATCH]) {
-    using S = typename SlotOf<NW>::T;
-    uint64_t mask[LOW_BATCH], i0[LOW_BATCH];
-#pragma unroll
-    for (int j = 0; j < LOW_BATCH; ++j) {
-        const uint64_t r = r0 + (uint64_t)j * step;
-        have[j] = r < n_low;
-        at[j] = ~0ull;
-        if (!have[j]) continue;
-        key[j] = unpack_low<NW>(low, r, P, full, tail_bytes);
-        const BucketMeta m = meta[key_hi(key[j]) >> bucket_shift];
-        tab[j] = reinterpret_cast<S*>(table) + m.tab_off;
-        mask[j] = m.tab_mask;
-        i0[j] = (hash_key(key[j]) >> 17) & m.tab_mask;
-    }
-    int v0[LOW_BATCH];
-    if constexpr (NW == 1) {
-        uint64_t fk[LOW_BATCH];  // the first probes' keys, all loads in flight at once
-#pragma unroll
-        for (int j = 0; j < LOW_BATCH; ++j)
-            if (have[j]) fk[j] = tab[j][i0[j]].key;
-#pragma unroll
-        for (int j = 0; j < LOW_BATCH; ++j)
-            v0[j] = !have[j] ? 0 : (fk[j] == EMPTY ? 0 : (fk[j] == key[j] ? 1 : 2));
-    } else {
-        S first[LOW_BATCH];
-#pragma unroll
-        for (int j = 0; j < LOW_BATCH; ++j)
-            if (have[j]) first[j] = tab[j][i0[j]];
-#pragma unroll
-        for (int j = 0; j < LOW_BATCH; ++j) v0[j] = have[j] ? slot_vs_key<NW>(first[j], key[j]) : 0;
-    }
-#pragma unroll
-    for (int j = 0; j < LOW_BATCH; ++j) {
-        if (!have[j]) continue;
-        int v = v0[j];
-        if (v == 1) at[j] = i0[j];
-        for (uint64_t p = 1; v == 2 && p <= mask[j]; ++p) {
-            const uint64_t i = (i0[j] + p) & mask[j];
-            v = slot_vs_key<NW>(tab[j][i], key[j]);
-            if (v == 1) at[j] = i;
-        }
-    }
-}
-
 __device__ __forceinline__ void hist_add(uint32_t* sh, unsigned long long* gh, uint64_t merged, uint32_t lo,
                                          uint32_t hi) {
     // the active lanes of the warp that share a shared-memory bin add once
@@ -2047,7 +1971,7 @@ __global__ void hist_clear_marks(void* table, uint64_t n_slots) {
 }
 
 template <int NW>
-__global__ void __launch_bounds__(256, 4) hist_low_pass(const uint8_t* low, uint64_t n_low, uint32_t k, const BucketMeta* meta,
+__global__ void hist_low_pass(const uint8_t* low, uint64_t n_low, uint32_t k, const BucketMeta* meta,
                               uint32_t bucket_shift, void* table, uint32_t lo, uint32_t hi,
                               unsigned long long* gh) {
     using K = typename KeyOf<NW>::T;
@@ -2057,26 +1981,19 @@ __global__ void __launch_bounds__(256, 4) hist_low_pass(const uint8_t* low, uint
     __syncthreads();
     const uint32_t full = k / 32, tail_bits = 2 * (k % 32), tail_bytes = (tail_bits + 7) / 8;
     const uint32_t P = full * 8 + tail_bytes;
-    constexpr int LOW_BATCH = low_batch<NW>();
-    const uint64_t step = (uint64_t)gridDim.x * blockDim.x;
-    for (uint64_t r0 = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; r0 < n_low; r0 += step * LOW_BATCH) {
-        K key[LOW_BATCH];
-        S* tab[LOW_BATCH];
-        uint64_t at[LOW_BATCH];
-        bool have[LOW_BATCH];
-        find_low_batch<NW>(low, n_low, r0, step, P, full, tail_bytes, meta, bucket_shift, table, key, tab, at, have);
-#pragma unroll
-        for (int j = 0; j < LOW_BATCH; ++j) {
-            if (!have[j]) continue;
-            uint64_t merged = 1;
-            if (at[j] != ~0ull) {
-                merged = (uint64_t)tab[j][at[j]].count + 1;
-                if constexpr (NW == 1) tab[j][at[j]].pad = 1;
-                else if constexpr (NW == 2) tab[j][at[j]].pad[0] = 1;
-                else tab[j][at[j]].mark = 1;
-            }
-            hist_add(sh, gh, merged, lo, hi);
+    for (uint64_t r = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; r < n_low; r += (uint64_t)gridDim.x * blockDim.x) {
+        const K key = unpack_low<NW>(low, r, P, full, tail_bytes);
+        const BucketMeta m = meta[key_hi(key) >> bucket_shift];
+        S* tab = reinterpret_cast<S*>(table) + m.tab_off;
+        uint64_t at;
+        uint64_t merged = 1;
+        if (table_find<NW>(tab, m.tab_mask, hash_key(key), key, &at)) {
+            merged = (uint64_t)tab[at].count + 1;
+            if constexpr (NW == 1) tab[at].pad = 1;
+            else if constexpr (NW == 2) tab[at].pad[0] = 1;
+            else tab[at].mark = 1;
         }
+        hist_add(sh, gh, merged, lo, hi);
     }
     __syncthreads();
     for (int i = threadIdx.x; i < HIST_SMEM; i += blockDim.x)
@@ -2130,7 +2047,7 @@ constexpr size_t loads_low_smem() { return KC_LOADS_BINS * (8 + 4); }
 constexpr size_t loads_table_smem() { return KC_LOADS_BINS * (8 + 4 + 4); }
 
 template <int NW>
-__global__ void __launch_bounds__(256, 4) loads_low_pass(const uint8_t* low, uint64_t n_low, uint32_t k, const BucketMeta* meta,
+__global__ void loads_low_pass(const uint8_t* low, uint64_t n_low, uint32_t k, const BucketMeta* meta,
                                uint32_t bucket_shift, void* table, unsigned long long* distinct,
                                unsigned long long* kmers) {
     // per-CTA totals per model bucket in shared memory (consecutive low keys
@@ -2148,28 +2065,21 @@ __global__ void __launch_bounds__(256, 4) loads_low_pass(const uint8_t* low, uin
     using S = typename SlotOf<NW>::T;
     const uint32_t full = k / 32, tail_bits = 2 * (k % 32), tail_bytes = (tail_bits + 7) / 8;
     const uint32_t P = full * 8 + tail_bytes;
-    constexpr int LOW_BATCH = low_batch<NW>();
-    const uint64_t step = (uint64_t)gridDim.x * blockDim.x;
-    for (uint64_t r0 = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; r0 < n_low; r0 += step * LOW_BATCH) {
-        K key[LOW_BATCH];
-        S* tab[LOW_BATCH];
-        uint64_t at[LOW_BATCH];
-        bool have[LOW_BATCH];
-        find_low_batch<NW>(low, n_low, r0, step, P, full, tail_bytes, meta, bucket_shift, table, key, tab, at, have);
-#pragma unroll
-        for (int j = 0; j < LOW_BATCH; ++j) {
-            if (!have[j]) continue;
-            unsigned long long occ = 1;
-            if (at[j] != ~0ull) {
-                occ += tab[j][at[j]].count;
-                if constexpr (NW == 1) tab[j][at[j]].pad = 1;
-                else if constexpr (NW == 2) tab[j][at[j]].pad[0] = 1;
-                else tab[j][at[j]].mark = 1;
-            }
-            const uint32_t bin = (uint32_t)(key_hi(key[j]) >> 52);
-            atomicAdd(s_distinct + bin, 1u);
-            atomicAdd(s_kmers + bin, occ);
+    for (uint64_t r = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; r < n_low; r += (uint64_t)gridDim.x * blockDim.x) {
+        const K key = unpack_low<NW>(low, r, P, full, tail_bytes);
+        const BucketMeta m = meta[key_hi(key) >> bucket_shift];
+        S* tab = reinterpret_cast<S*>(table) + m.tab_off;
+        uint64_t at;
+        unsigned long long occ = 1;
+        if (table_find<NW>(tab, m.tab_mask, hash_key(key), key, &at)) {
+            occ += tab[at].count;
+            if constexpr (NW == 1) tab[at].pad = 1;
+            else if constexpr (NW == 2) tab[at].pad[0] = 1;
+            else tab[at].mark = 1;
         }
+        const uint32_t bin = (uint32_t)(key_hi(key) >> 52);
+        atomicAdd(s_distinct + bin, 1u);
+        atomicAdd(s_kmers + bin, occ);
     }
     __syncthreads();
     for (uint32_t i = threadIdx.x; i < KC_LOADS_BINS; i += blockDim.x) {
