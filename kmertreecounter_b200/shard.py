@@ -184,6 +184,9 @@ def gpu_stages(counter, slice_bytes, device, d_slice=None):
 
     def route():
         d = d_slice if d_slice is not None else torch.from_numpy(np.ascontiguousarray(slice_bytes)).to(device)
+        # the slice was written on torch's stream; the routing kernels run on
+        # the context's own stream
+        torch.cuda.synchronize(device)
         counts = counter.route_device(d.data_ptr(), d.numel())
         return routed_tensor(counter, nw, device), counts
 
