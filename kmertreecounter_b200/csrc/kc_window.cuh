@@ -166,8 +166,8 @@ __global__ void window_bounds(const uint64_t* __restrict__ start, const uint32_t
 }
 
 constexpr int SCAT_THREADS = 512;
-constexpr int SCAT_ITEMS = 16;
-constexpr int SCAT_CHUNK = SCAT_THREADS * SCAT_ITEMS;  // 8192 keys
+constexpr int SCAT_ITEMS = 8;
+constexpr int SCAT_CHUNK = SCAT_THREADS * SCAT_ITEMS;  // 4096 keys
 constexpr int SCAT_BINS = 1024;                         // windows staged in shared memory
 // dynamic shared memory of subroute_scatter
 constexpr size_t scatter_smem_bytes() {
@@ -194,7 +194,7 @@ struct ScatterArgs {
 // window's capacity is reserved in the spill area instead), is staged in
 // shared memory in window order, and leaves as contiguous runs.  Keys of
 // windows outside the chunk's staged span are placed one by one.
-__global__ void __launch_bounds__(SCAT_THREADS, 2) subroute_scatter(ScatterArgs a) {
+__global__ void __launch_bounds__(SCAT_THREADS, 3) subroute_scatter(ScatterArgs a) {
     extern __shared__ __align__(16) uint8_t sc_smem[];
     uint64_t* stage = reinterpret_cast<uint64_t*>(sc_smem);
     uint16_t* stage_bin = reinterpret_cast<uint16_t*>(sc_smem + (size_t)SCAT_CHUNK * 8);
