@@ -337,12 +337,16 @@ def stage_rooflines(stage_ms, stats, F, k, hbm_gbs, P, rec, traffic=None):
                        64 K + 64 (K - L) (global count, no windows) one 32 B filter sector read
                                          + write per k-mer and one table sector per repeat
       pack_low         8N L + P L        first occurrences read, packed low.bin written
-      export           16 cells + rec R  table read, root records written
+      export           S cells + rec R   table read, root records written
       lines            F
-      init             16 cells          table cells written"""
+      init             S cells + 8 W     table cells (and, for keys over 64 bits,
+                                         the separate filter's W words) written
+    with S = the table slot's bytes (16, 32, 48 for 64-, 128-, 256-bit keys)."""
     nw = 1 if k <= 32 else (2 if k <= 64 else 4)
     K, L, R = stats["total_kmers"], stats["low_records"], stats["root_records"]
     cells = stats["table_slots"]
+    S = {1: 16, 2: 32, 4: 48}[nw]
+    W = stats.get("filter_words", 0) if nw > 1 else 0  # 64-bit keys keep the filter in the cells
     windowed = stage_ms.get("subroute", 0.0) > 0
     rules = {
         "extract_scatter": (F + 8 * nw * K, "F + 8N K"),
@@ -350,9 +354,9 @@ def stage_rooflines(stage_ms, stats, F, k, hbm_gbs, P, rec, traffic=None):
         "count": ((8 * nw * K + 8 * nw * L + int(2 * 16 * cells * 9 / 8), "8N K + 8N L + 2 x 16 x cells x 9/8")
                   if windowed else (64 * K + 64 * (K - L), "64 K + 64 (K - L)")),
         "pack_low": (8 * nw * L + P * L, "8N L + P L"),
-        "export": (16 * cells + rec * R, "16 cells + rec R"),
+        "export": (S * cells + rec * R, f"{S} cells + rec R"),
         "lines": (F, "F"),
-        "init": (16 * cells, "16 cells"),
+        "init": (S * cells + 8 * W, f"{S} cells" + (" + 8 filter words" if W else "")),
     }
     out = {}
     for s_, (b, rule) in rules.items():

@@ -58,5 +58,9 @@ def test_stage_rooflines(bench):
     assert r["count"]["alg_bytes"] == 8 * 2_000 + 8 * 600 + int(2 * 16 * 1_000 * 9 / 8)
     assert r["pack_low"]["alg_bytes"] == 8 * 600 + 8 * 600
     assert r["count"]["gbs"] == pytest.approx(r["count"]["alg_bytes"] / 4e-3 / 1e9)
-    r2 = bench.stage_rooflines({"count": 4.0}, stats, 6_000, 63, 1.0, 16, 24)
+    r2 = bench.stage_rooflines({"count": 4.0, "init": 1.0, "export": 1.0}, dict(stats, filter_words=300), 6_000, 63,
+                               1.0, 16, 24)
     assert r2["count"]["alg_bytes"] == 64 * 2_000 + 64 * 1_400 and r2["count"]["rule"].startswith("64 K")
+    # 128-bit keys: 32-byte slots, and a filter of its own to initialise
+    assert r2["init"]["alg_bytes"] == 32 * 1_000 + 8 * 300
+    assert r2["export"]["alg_bytes"] == 32 * 1_000 + 24 * 100
