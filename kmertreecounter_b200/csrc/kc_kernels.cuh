@@ -1520,26 +1520,19 @@ __global__ void grow_move(void* table, const GrowJob* __restrict__ jobs, uint32_
 // Initialise table slots to EMPTY with count 0.
 template <int NW>
 __global__ void init_slots(void* tab, uint64_t n) {
+    // the table as 16-byte words, each lane one coalesced word per step: a
+    // slot is 1, 2 or 3 words, EMPTY keys are all ones, counts, padding,
+    // the 256-bit slot's state (SLOT_EMPTY = 0) and mark are zeros
     using S = typename SlotOf<NW>::T;
-    S* t = reinterpret_cast<S*>(tab);
-    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
-        S s;
-        if constexpr (NW == 1) {
-            s.key = EMPTY;
-            s.count = 0;
-            s.pad = 0;
-        } else if constexpr (NW == 2) {
-            s.w0 = EMPTY;
-            s.w1 = EMPTY;
-            s.count = 0;
-            s.pad[0] = s.pad[1] = s.pad[2] = 0;
-        } else {
-            s.w0 = s.w1 = s.w2 = s.w3 = 0;
-            s.count = 0;
-            s.state = SLOT_EMPTY;
-            s.mark = 0;
-        }
-        t[i] = s;
+    constexpr uint64_t Q = sizeof(S) / 16;
+    static_assert(sizeof(S) % 16 == 0, "slots are whole 16-byte words");
+    uint4* t = reinterpret_cast<uint4*>(tab);
+    const uint64_t n16 = n * Q;
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n16; i += (uint64_t)gridDim.x * blockDim.x) {
+        uint4 v = make_uint4(0u, 0u, 0u, 0u);
+        if constexpr (NW == 1) v = make_uint4(~0u, ~0u, 0u, 0u);           // {key = EMPTY, count, pad}
+        else if constexpr (NW == 2) if ((i & 1) == 0) v = make_uint4(~0u, ~0u, ~0u, ~0u);  // {w0, w1} = EMPTY
+        t[i] = v;
     }
 }
 
