@@ -746,6 +746,50 @@ def file_to_file(args, sample_path, sample_bases, k, ref_sample_gbs, full_path, 
     return out
 
 
+def postprocess_leg(args, k, scale=0.05):
+    """The post-processing row: `bin/Tree` counts a 5% sample of the
+    workload to ./tmp/, then this build's `bin/PostProcess` (device merge)
+    and the reference's own `PostProcess::merge_all` (oracle/_ref, built from
+    its sources; 4 threads as its own main uses) each turn that tmp/ into
+    final_root.bin, final_low.bin and freq_hist.txt; wall clock of each
+    process, and whether their files are byte-identical."""
+    import filecmp
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    tree = os.path.join(ROOT, "kmertreecounter_b200", "bin", "Tree")
+    post = os.path.join(ROOT, "kmertreecounter_b200", "bin", "PostProcess")
+    nw = 1 if k <= 32 else (2 if k <= 64 else 4)
+    out = {"input": f"bin/Tree's tmp/ of the workload at scale {scale}", "method": "wall clock of each process"}
+    with tempfile.TemporaryDirectory() as wd:
+        path, data, _, _, info = cpu_sample(args.workload, scale, wd)
+        r = subprocess.run([tree, path, str(k), "16", "16"], cwd=wd, capture_output=True, text=True,
+                           env=dict(os.environ, KC_STAGE0="0"))
+        if r.returncode:
+            return {"error": f"Tree exit {r.returncode}"}
+        tmp = os.path.join(wd, "tmp") + "/"
+        out["low_bytes"] = os.path.getsize(tmp + "low.bin")
+        dirs = {}
+        for name, cmd in (("ours", [post, tmp, None, str(k)]), ("reference", [oracle.REF_POST, tmp, None, str(nw)])):
+            if name == "reference" and not os.path.exists(oracle.REF_POST):
+                continue
+            d = os.path.join(wd, name) + "/"
+            os.makedirs(d)
+            cmd[2] = d
+            t = time.perf_counter()
+            r = subprocess.run(cmd, capture_output=True, text=True, timeout=300)
+            dt = time.perf_counter() - t
+            out[name] = {"seconds": dt} if r.returncode == 0 else {"error": f"exit {r.returncode}"}
+            dirs[name] = d
+        if "seconds" in out.get("ours", {}) and "seconds" in out.get("reference", {}):
+            files = ("final_root.bin", "final_low.bin", "freq_hist.txt")
+            out["identical"] = all(
+                os.path.exists(dirs["ours"] + f) == os.path.exists(dirs["reference"] + f) and
+                (not os.path.exists(dirs["ours"] + f) or filecmp.cmp(dirs["ours"] + f, dirs["reference"] + f,
+                                                                     shallow=False)) for f in files)
+            out["ratio"] = out["reference"]["seconds"] / out["ours"]["seconds"]
+    return out
+
+
 # --------------------------------------------------------------- our arm
 
 def run_ours(args):
@@ -952,6 +996,10 @@ def run_ours(args):
             if not args.no_file_to_file:
                 line["file_to_file"] = file_to_file(args, path, sbases, kk, best if kind == "reference" else None,
                                                     full_path, bases, stats["total_kmers"])
+                try:
+                    line["postprocess"] = postprocess_leg(args, kk)
+                except (OSError, subprocess.SubprocessError, ValueError) as e:
+                    line["postprocess"] = {"error": str(e)[:200]}
     if ftf_dir is not None:
         ftf_dir.cleanup()
     if world > 1:
