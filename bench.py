@@ -277,13 +277,8 @@ def time_reference(path, data, k, bases, runs, workdir):
 # sub-routing and count (x 10.000), first occurrences for packing
 # (x 10.022), table cells for export and initialisation (x 9.781), FASTQ
 # bytes for the line scan (x 10.032).  Reported only while the kernel
-# sources are unchanged since that capture, or differ from them only in
-# code that none of these stages runs (_SAME_STAGES).
+# sources are unchanged since that capture.
 _CAPTURE_SHA = "cbcf5f8cf3571f44171df3491c10b6a6f761db93203f4e2bd6bd49d0ac3a22c3"
-_SAME_STAGES = {
-    # kc_engine.cu: the sort stage's launch count (sort_output=1 only)
-    "9b2c0f076e668c2f7cd6d719434bb5589be28da632e1fe9f20c0526707b07024",
-}
 PROFILED_TRAFFIC = {
     # workload: {stage: {"sources_sha256": ..., "bytes_per_step": ...}}
     "genome_scale": {
@@ -314,8 +309,7 @@ def profile_traffic(args, stage):
     e = PROFILED_TRAFFIC.get(args.workload, {}).get(stage)
     if not e or args.scale != 1.0 or not e["bytes_per_step"]:
         return None, "no capture of this stage on this workload"
-    sha = kernel_sources_sha256()
-    if e["sources_sha256"] != sha and not (e["sources_sha256"] == _CAPTURE_SHA and sha in _SAME_STAGES):
+    if e["sources_sha256"] != kernel_sources_sha256():
         return None, "kernel sources changed since the last capture"
     return e["bytes_per_step"], "ncu capture of these kernel sources"
 
@@ -566,27 +560,16 @@ def set_checksums(c, base, sets, groups, torch, learned=None):
     return sums
 
 
-def _roots_checksum(torch, d_roots, n_roots):
-    """(records, wrapping sum of mix(key) x count) of 16-byte root records
-    (one key word, then count|pad) in device memory, and the keys."""
-    if not n_roots:
-        return (0, 0), torch.empty(0, dtype=torch.int64, device="cuda")
-    rr = torch.as_tensor(_DeviceBytes(d_roots, n_roots * 16), device="cuda").view(torch.int64).view(-1, 2)
-    keys = rr[:, 0].clone()
-    s = int((_mix(rr[:, 0]) * (rr[:, 1] & 0xFFFFFFFF)).sum().item()) % (1 << 64)
-    return (int(n_roots), s), keys
-
-
-def sort_record(kc, torch, dev, n, k, unsorted, hbm_gbs):
+def sort_record(kc, torch, dev, n, k, merged, hbm_gbs):
     """The optional root-record sort (sort_output=1; the reference's
     export_record_radix_sort) on the workload's root records: one count with
     the sort on after one that sizes its buffers, the sort stage's device
     time from the library's stage events, and the sorted records checked on
     the device: keys strictly ascending as unsigned words (so every root
-    file's records stay together, in key order) and the same records as the
-    unsorted count (record count and a checksum of key and count).
-    Algorithmic bytes: the records read once for the digit counts, then read
-    and written once per 8-bit digit of the 2k-bit key."""
+    file's records stay together, in key order), and the merged result
+    (count histogram, distinct keys) equal to the unsorted count's `merged`.
+    Algorithmic bytes: every record read and written once per 8-bit digit of
+    the 2k-bit key."""
     with kc.Counter(k=k, sort_output=1) as c:
         c.count_device(dev.data_ptr(), n)
         c.set_profiling(True)
@@ -594,15 +577,18 @@ def sort_record(kc, torch, dev, n, k, unsorted, hbm_gbs):
         ms, launches = c.stage_times().get("sort", (0.0, 0))
         c.set_profiling(False)
         _, _, d_roots, n_roots = c.device_results()
-        got, keys = _roots_checksum(torch, d_roots, n_roots)
-        sign = -(1 << 63)
-        asc = bool(((keys[1:] ^ sign) > (keys[:-1] ^ sign)).all().item()) if keys.numel() > 1 else True
+        asc = True
+        if n_roots > 1:
+            rr = torch.as_tensor(_DeviceBytes(d_roots, n_roots * 16), device="cuda").view(torch.int64).view(-1, 2)
+            sign = -(1 << 63)
+            asc = bool(((rr[1:, 0] ^ sign) > (rr[:-1, 0] ^ sign)).all().item())
+        h, d = c.histogram(1, 10000)
     digits = (2 * k + 7) // 8
-    alg = n_roots * 16 * (2 * digits + 1)
+    alg = n_roots * 16 * 2 * digits
     gbs = alg / ms / 1e6 if ms else None
     return {"ms": ms, "launches": launches, "records": n_roots, "digit_passes": digits, "alg_bytes": alg,
-            "rule": "R x 16 x (2 x digits + 1)", "gbs": gbs, "frac": gbs / hbm_gbs if gbs else None,
-            "ascending": asc, "same_records": got == unsorted}
+            "rule": "R x 16 x 2 x digits", "gbs": gbs, "frac": gbs / hbm_gbs if gbs else None,
+            "ascending": asc, "same_merged_counts": d == merged[1] and h.tolist() == merged[0].tolist()}
 
 
 class _DeviceBytes:
@@ -917,7 +903,7 @@ def run_ours(args):
     # the merged count histogram of the device-held result (histogram_tool
     # precise's output, counts 1..10000), timed on its own after the steps
     t_h = time.perf_counter()
-    counter.histogram(1, 10000)
+    merged = counter.histogram(1, 10000)
     histogram_ms = (time.perf_counter() - t_h) * 1e3
     stats = st.as_dict()
     stats.pop("root_counts", None)
@@ -1007,21 +993,17 @@ def run_ours(args):
         "clocks": clk,
         "sizing": None,
     }
-    unsorted = None
-    if rec == 16 and not args.no_sort_record:
-        _, _, d_roots, n_roots = counter.device_results()
-        unsorted, _ = _roots_checksum(torch, d_roots, n_roots)
     counter.close()  # its structures go before the sizing comparison builds two more contexts
     if not args.no_sizing:
         try:
             line["sizing"] = compare_sizing(args, kc, torch, dev, n, k, buckets)
         except kc.KcError as e:
             line["sizing"] = {"error": str(e)}
-    if unsorted is not None:
+    if rank == 0 and rec == 16 and not args.no_sort_record:
         try:
-            line["sorted_roots"] = sort_record(kc, torch, dev, n, k, unsorted, pk["hbm_gbs"])
-        except kc.KcError as e:
-            line["sorted_roots"] = {"error": str(e)}
+            line["sorted_roots"] = sort_record(kc, torch, dev, n, k, merged, pk["hbm_gbs"])
+        except Exception as e:  # a record beside the line, never the line itself
+            line["sorted_roots"] = {"error": f"{type(e).__name__}: {str(e)[:200]}"}
     del dev
     ftf_dir, full_path = None, None
     if rank == 0 and not args.no_file_to_file and not args.no_cpu_baseline:

@@ -1233,7 +1233,7 @@ int finish_run(kc_context* c) {
         CK(c->sort_offs.ensure(bo));
         CK(c->sort_sums.ensure(bs));
         const KcSortScratch w{c->sort_tmp.p, c->sort_hist.p, c->sort_offs.p, c->sort_sums.p};
-        Stage st(c, KC_STAGE_SORT, kc_sort_launches(c->cfg.k));
+        Stage st(c, KC_STAGE_SORT, 4 * ((2 * c->cfg.k + 7) / 8));
         rc = kc_sort_roots(c->roots.p, c->root_total, c->record_bytes, c->cfg.k, w, c->stream);
         if (rc) return fail(rc, "root record sort failed: %s", kc_sort_error());
     }

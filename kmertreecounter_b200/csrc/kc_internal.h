@@ -19,17 +19,14 @@ void kc_sort_scratch_bytes(uint64_t n, uint64_t record_bytes, uint64_t* tmp, uin
                            uint64_t* sums);
 
 // Sort root records (ExportRecord<N>, record_bytes each, grouped by root id)
-// by key, keeping the grouping, in place on `stream`; returns once the
-// stream has finished the sort (it reads the sort's error word back).
+// by key, keeping the grouping, in place on `stream` (asynchronous).
 // Returns 0 or a negative KC_ERR_* code.
 int kc_sort_roots(void* records, uint64_t n, uint64_t record_bytes, uint32_t k, const KcSortScratch& w,
                   cudaStream_t stream);
+const char* kc_sort_error();
 // The same over bare keys of nw 64-bit words (scratch sizes from
 // kc_sort_scratch_bytes with record_bytes = 8 nw).
 int kc_sort_keys(void* keys, uint64_t n, uint32_t nw, uint32_t k, const KcSortScratch& w, cudaStream_t stream);
-const char* kc_sort_error();
-// Kernel launches of one sort of k-mers of length k.
-uint32_t kc_sort_launches(uint32_t k);
 
 int kc_internal_set_error(int code, const char* msg);
 uint64_t kc_internal_record_bytes(const kc_context* c);
