@@ -64,3 +64,28 @@ def test_stage_rooflines(bench):
     # 128-bit keys: 32-byte slots, and a filter of its own to initialise
     assert r2["init"]["alg_bytes"] == 32 * 1_000 + 8 * 300
     assert r2["export"]["alg_bytes"] == 32 * 1_000 + 24 * 100
+
+
+def test_profiled_traffic_keyed_by_kernel_sources(bench):
+    """Measured DRAM traffic is reported only for the genome-scale workload at
+    full size and only while the kernel sources hash to the captured sha256;
+    any other sources give null traffic with the reason."""
+    class A:
+        workload, scale = "genome_scale", 1.0
+    stages = bench.PROFILED_TRAFFIC["genome_scale"]
+    assert set(stages) == set(bench.STAGE_KERNELS)
+    real = bench.kernel_sources_sha256
+    try:
+        bench.kernel_sources_sha256 = lambda: bench._CAPTURE_SHA
+        for s, e in stages.items():
+            b, note = bench.profile_traffic(A, s)
+            assert b == e["bytes_per_step"] > 0 and "capture" in note
+        bench.kernel_sources_sha256 = lambda: "0" * 64
+        assert bench.profile_traffic(A, "count") == (None, "kernel sources changed since the last capture")
+    finally:
+        bench.kernel_sources_sha256 = real
+    A.scale = 0.5
+    assert bench.profile_traffic(A, "count")[0] is None
+    A.scale, A.workload = 1.0, "large_long"
+    assert bench.profile_traffic(A, "count")[0] is None
+
